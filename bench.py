@@ -1,0 +1,344 @@
+#!/usr/bin/env python
+"""Throughput of the 3D Flow Lenia step on B200.
+
+Workload (the headline configuration): one world of 128^3 cells x 4 channels,
+16 kernels of radius 13 (one per channel pair, parameters drawn from the
+seeded sampler), Sobel gradients, RT reintegration (sigma 0.65, dt 0.2), zero
+borders.  A "step" is one full simulation step (spectral growth, flow,
+transport).  Metric: cell-updates/s = cells x channels x steps / s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one process per GPU) every rank advances its own world
+(the single-world step does not shard: replicas, weak scaling); `value` is the
+sum over ranks divided by the slowest rank's time.  `--impl reference` times
+the CPU restatement of the reference's step (oracle, complex-to-complex
+spectral structure like the reference's FFTW path) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s at 128^3x4ch"
+UNIT = "cell-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--width", type=int, default=128)
+    ap.add_argument("--mode", default="rt", choices=["rt", "adv"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(args, rank=0):
+    from lenia_b200 import params as P
+    mode = P.MODE_RT if args.mode == "rt" else P.MODE_ADV
+    return P.config1(seed=1 + rank, width=args.width, mode=mode)
+
+
+def config_dict(args, wl, n):
+    return {
+        "workload": f"single world {wl.desc.width}^3 x {wl.desc.channels}ch, {len(wl.kernels)} kernels "
+                    f"R={wl.kernels[0].radius}, Sobel, {'RT' if args.mode == 'rt' else 'advection'}, zero borders",
+        "grid": [wl.desc.width, wl.desc.height, wl.desc.width],
+        "channels": wl.desc.channels,
+        "kernels": len(wl.kernels),
+        "kernel_radius": wl.kernels[0].radius,
+        "parallelism": f"replicas x{n}" if n > 1 else "single GPU",
+        "l2": "state ~0.7 GB per world, larger than the 126 MB L2 (no flush needed)",
+    }
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", self.gpu_id], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def gpu_uuid(dev: int) -> str:
+    import torch
+    try:
+        u = torch.cuda.get_device_properties(dev).uuid
+        s = str(u)
+        return s if s.startswith("GPU-") else "GPU-" + s
+    except Exception:
+        return str(dev)
+
+
+# ----------------------------------------------------- algorithmic bytes
+def kernel_bytes(wl) -> dict:
+    """Algorithmic HBM bytes per launch of each kernel (each input read once,
+    each output written once; derivation in DESIGN.md)."""
+    d = wl.desc
+    W, H, C = d.width, d.height, d.channels
+    D = W
+    N = W * H * D
+    K = len(wl.kernels)
+    KX = W // 2 + 1
+    HS = KX * D * H  # complex entries of a half spectrum
+    KH = KX * (D // 2 + 1) * (H // 2 + 1)
+    crt = C if d.rt_all_channels else min(C, 3)
+    back = 1 if d.growth_type == 1 else 0
+    return {
+        "fwd_rows": C * N * 4 + C * HS * 8,
+        "planes_fwd": 2 * C * HS * 8,
+        "planes_inv": K * HS * 8 * 2 + K * KH * 4,
+        "growth_rows": K * HS * 8 + back * C * N * 4 + (2 + back) * C * N * 4,
+        "flow": N * 4 + C * N * (4 + 4 + 12 + 12 + 12),
+        "transport": crt * N * 16 + C * N * (4 + 4 + 4) + N * 4,
+    }
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        j = json.load(open(p))
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------- CPU legs
+def cpu_port_rate(wl, steps: int, warmup: int):
+    """The oracle's restatement of the reference step (complex-to-complex
+    spectral path like the reference's FFTW calls), timed on the host."""
+    from oracle.oracle import RestateOracle
+    p, ks = wl.desc.as_dict(), [k.as_dict() for k in wl.kernels]
+    o = RestateOracle(p, ks, fft_mode="c2c")
+    o.set_state(A=wl.A0.ravel())
+    if warmup:
+        o.step(warmup)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    cells = wl.desc.cells * wl.desc.channels
+    return cells * steps / dt, dt
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    n = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    if rank != 0:
+        return 0
+    wl = workload(args)
+    steps = max(1, min(args.steps, 8))
+    warm = 1 if args.warmup > 0 else 0
+    rate, dt = cpu_port_rate(wl, steps, warm)
+    ms = dt * 1000.0 / steps
+    cores = cpu_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": n,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": config_dict(args, wl, 1),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{steps} timed steps (+{warm} warm-up) of the same world on the host, "
+                                   f"C restatement of the reference step with its complex-to-complex FFT "
+                                   f"structure, OpenMP over {cores} threads"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------ GPU arm
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    n = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    dist = None
+    if n > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    from lenia_b200.world import World
+    wl = workload(args, rank)
+    w = World(wl.desc, wl.kernels)
+    stream = torch.cuda.current_stream()
+    w.set_stream(stream.cuda_stream)
+    w.set_state(wl.A0.ravel())
+    C, N = wl.desc.channels, wl.desc.cells
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    w.step(args.warmup)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu_uuid(local)) as clk:
+        barrier()
+        e0.record(stream)
+        w.step(args.steps)
+        e1.record(stream)
+        barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    w.sync()
+    launches = w.launches_per_step * args.steps
+    value = n * N * C * args.steps / (ms / 1000.0)
+
+    # per-kernel device time over a second timed pass (CUDA events around
+    # every launch, on the launching stream)
+    w.set_profiling(True)
+    prof_steps = max(10, min(args.steps, 200))
+    w.step(prof_steps)
+    prof = w.profile_read()
+    w.set_profiling(False)
+    total = sum(v[0] for v in prof.values()) or 1.0
+    kb = kernel_bytes(wl)
+    top = max(prof.items(), key=lambda kv: kv[1][0])
+    top_name, (top_ms, top_n) = top
+    per_launch_ms = top_ms / top_n
+    peak, peak_kind = measured_peaks()
+    achieved = kb.get(top_name, 0) / (per_launch_ms / 1000.0) / 1e9
+    kernels_table = {k: {"ms_per_launch": v[0] / v[1], "share": v[0] / total,
+                         "gbs": kb.get(k, 0) / (v[0] / v[1] / 1000.0) / 1e9 if k in kb else None}
+                     for k, v in prof.items()}
+
+    # end to end through the public API with host buffers: each step uploads
+    # the world state (A, V, GA, SUM) from pinned host memory, steps, and reads
+    # the new state back
+    host = {name: torch.empty(w.field_size(name), dtype=torch.float32).pin_memory()
+            for name in ("A", "V", "GA", "SUM")}
+    for name, t in host.items():
+        w.get(name, out=t.numpy())
+    e2e_steps = max(3, min(args.steps // 10, 50))
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        for name, t in host.items():
+            w.set(name, t.numpy())
+        w.step(1)
+        for name, t in host.items():
+            w.get(name, out=t.numpy())
+    f1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1))
+    h2d = sum(t.numel() * 4 for t in host.values())
+    e2e = {"value": n * N * C * e2e_steps / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": h2d}
+
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": config_dict(args, wl, n),
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "roofline": {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "algorithmic_bytes_per_launch": kb.get(top_name)},
+            "kernels": kernels_table,
+        }
+        if n == 1 and not args.no_cpu_baseline:
+            rate, dt = cpu_port_rate(wl, 2, 1)
+            line["cpu_baseline"] = {
+                "value": rate, "unit": UNIT, "cores": cpu_threads(), "kind": "port",
+                "sample": "2 timed steps (+1 warm-up) of the same world, C restatement of the reference step "
+                          "(complex-to-complex FFT structure), OpenMP over all host threads"}
+    w.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,200 @@
+/*
+ * lenia_b200 — C ABI of the B200-native 3D Flow Lenia step.
+ *
+ * The reference (lostnthought/Lenia) has no library boundary: its step API is
+ * a set of `void stage(TD *t)` functions over process-global arrays
+ * (lenia.h:5-28, reintegration.h:207-240, transposition.h:4-11, mesh.h:7-9),
+ * configured by writing globals (main.cpp:27-66) and driven by a 12-event
+ * state machine (render.cpp:357-604).  This header replaces that surface with
+ * an opaque world handle: the globals become LeniaWorldDesc, the Kernel struct
+ * becomes LeniaKernelParams, the arrays become fields read and written through
+ * lenia_get_field / lenia_set_field, and the event sequence becomes
+ * lenia_step (whole steps) or lenia_step_stage (one stage group).
+ *
+ * Plain C types only; all device work runs on one CUDA stream per world.
+ * Every entry point returns a lenia_status; lenia_last_error() describes the
+ * last failure on a world.  There is no CPU fallback: without a CUDA device
+ * lenia_create fails with LENIA_ERR_NO_DEVICE.
+ */
+#ifndef LENIA_B200_H
+#define LENIA_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LENIA_MAX_CHANNELS 4 /* MAX_CHANNELS, render.h:34 */
+#define LENIA_MAX_BETA 12    /* MAX_BETA, render.h:35 */
+#define LENIA_MAX_KERNELS 64 /* render.h:33 fixes 12; runtime here */
+
+typedef enum lenia_status {
+    LENIA_OK = 0,
+    LENIA_ERR_INVALID_ARG = 1,
+    LENIA_ERR_OOM = 2,
+    LENIA_ERR_CUDA = 3,
+    LENIA_ERR_TIMEOUT = 4,
+    LENIA_ERR_NONFINITE = 5,
+    LENIA_ERR_NO_DEVICE = 6,
+    LENIA_ERR_UNSUPPORTED = 7
+} lenia_status;
+
+/* Enumerations, in the reference's order (render.h:128-223). */
+enum { LENIA_GROWTH_NOGROWTH = 0, LENIA_GROWTH_RT = 1, LENIA_GROWTH_TRANSPOSITION = 2 };
+enum { LENIA_MODE_SRT = 0, LENIA_MODE_RT = 1, LENIA_MODE_ADV = 2 };
+enum { LENIA_BORDER_TORUS = 0, LENIA_BORDER_WALL = 1, LENIA_BORDER_NONE = 2 };
+enum { LENIA_GRADIENT_CENTRAL_DIFF = 0, LENIA_GRADIENT_SOBEL = 1 };
+
+/* The reference's scalar and mode globals (main.cpp:27-56, main.cpp:304,
+ * render.h:125-233) plus the per-channel flags (ChannelData, render.h:486-492).
+ * The grid is width x height x width (x, y, z), GRID_WIDTH/GRID_HEIGHT of
+ * render.h:27-29, here chosen at run time. */
+typedef struct LeniaWorldDesc {
+    int width;
+    int height;
+    int channels;
+    float timestep;
+    float theta_a;
+    float n_alpha;   /* N: accepted, unused (as in the reference) */
+    float s_norm;
+    float gta;
+    float sta;
+    float v_damp;
+    float v_beta;    /* accepted, unused (as in the reference) */
+    float iso_value;
+    float sigma;     /* off_table.sigma */
+    float dd;        /* off_table.dd, truncated to int */
+    int alpha_mode;  /* accepted, no effect (as in the reference) */
+    int growth_type;
+    int mode_type;
+    int sobel_border;
+    int border;
+    int gradient_mode;
+    int adv_vel;
+    int mu_vel;
+    int blur_central_diff;
+    int osc_la;
+    int osc_flow;
+    int osc_div_flow;
+    int osc_vel;
+    float osc_la_amt;
+    float osc_flow_amt;
+    float osc_div_flow_amt;
+    int asymptotic[LENIA_MAX_CHANNELS];
+    int soft_clip[LENIA_MAX_CHANNELS];
+    int rt_all_channels; /* 0 = reference: SRT/RT transport channels 0-2 only */
+    int alpha_index_fix; /* 0 = reference: PREALPHA/GA read at the padded offset */
+} LeniaWorldDesc;
+
+/* One kernel: the parameter part of `Kernel` (render.h:347-361). */
+typedef struct LeniaKernelParams {
+    int radius;
+    int beta_size;
+    float b[LENIA_MAX_BETA];
+    float r_a;
+    float m;
+    float s;
+    float h;
+    int c0; /* source channel */
+    int c1; /* destination channel */
+} LeniaKernelParams;
+
+/* Fields (the reference's arrays, render.h:277-328, lenia.cpp:9-89), each
+ * unpadded, channel-major, x fastest (IDX, render.h:334).  Vector fields are
+ * three blocks x, y, z.  Fields marked (debug) exist only after
+ * lenia_set_debug(w, 1). */
+typedef enum LeniaField {
+    LENIA_FIELD_A = 0,         /* GRID, C*N */
+    LENIA_FIELD_V = 1,         /* V_x,V_y,V_z, 3*C*N */
+    LENIA_FIELD_GA = 2,        /* C*N */
+    LENIA_FIELD_SUM = 3,       /* N */
+    LENIA_FIELD_H = 4,         /* C*N */
+    LENIA_FIELD_U_SUM = 5,     /* C*N */
+    LENIA_FIELD_BACK = 6,      /* C*N */
+    LENIA_FIELD_NA = 7,        /* 3*N (debug) */
+    LENIA_FIELD_NU = 8,        /* 3*C*N (debug) */
+    LENIA_FIELD_PREALPHA = 9,  /* C*N (debug) */
+    LENIA_FIELD_ALPHA = 10,    /* C*N (debug, or with OSC_DIV_FLOW) */
+    LENIA_FIELD_F = 11,        /* 3*C*N (debug, or when advection/oscillators read it) */
+    LENIA_FIELD_MU = 12,       /* 3*C*N */
+    LENIA_FIELD_TT = 13,       /* C*N (debug: TT before the transposition epilogue) */
+    LENIA_FIELD_U_S = 14,      /* C*N (central difference) */
+    LENIA_FIELD_SUM_S = 15,    /* N (central difference) */
+    LENIA_FIELD_U = 16,        /* K*N: u_k = Re(IFFT)/N per kernel (debug) */
+    LENIA_FIELD_H_RB = 17,     /* C*N: H of the previous step */
+    LENIA_FIELD_U_SUM_RB = 18, /* C*N: U_SUM of the previous step */
+    LENIA_FIELD_RBB = 19       /* C*N: grid snapshot for meshing */
+} LeniaField;
+
+/* Stage groups of one step, each a run of the reference's events
+ * (render.h:181-197). */
+typedef enum LeniaStage {
+    LENIA_STAGE_GROWTH = 0,    /* SIM_EVENT_FFT + FFT_MT: u_k, H, U_SUM, BACK */
+    LENIA_STAGE_BLUR = 1,      /* SIM_EVENT_BLUR: U_S, SUM_S */
+    LENIA_STAGE_FLOW = 2,      /* TSB, SOBEL_ONE, SOBEL_TWO, F, MU, TB: V, MU */
+    LENIA_STAGE_TRANSPORT = 3, /* REINTEGRATION + TRM: A, GA, SUM */
+    LENIA_STAGE_SNAPSHOT = 4   /* TMB: RBB */
+} LeniaStage;
+
+typedef struct lenia_world lenia_world;
+
+/* Creates a world on the current CUDA device: validates the description
+ * (width/height in [8,256], multiples of 4, prime factors in {2,3,5,7,11};
+ * channels 1..4; kernels 0..64 with channels in range), allocates device
+ * state, builds the kernels (init_kernel, lenia.cpp:199-261), the growth
+ * table rows (init_bell_lut, lenia.cpp:93-101) and the blur kernel
+ * (precompute_blur_kernel, reintegration.cpp:13-78).  All fields start at 0. */
+lenia_status lenia_create(const LeniaWorldDesc *desc, const LeniaKernelParams *kernels,
+                          int n_kernels, lenia_world **out);
+lenia_status lenia_destroy(lenia_world *w);
+
+/* Replaces scalars and modes (same grid shape and channel count): the
+ * reference's UI edits of the globals (config.cpp:406-520). */
+lenia_status lenia_set_params(lenia_world *w, const LeniaWorldDesc *desc);
+/* Replaces the kernel set (init_kernel per kernel, lenia.cpp:199-261). */
+lenia_status lenia_set_kernels(lenia_world *w, const LeniaKernelParams *kernels, int n_kernels);
+
+/* Copies `count` floats into / out of a field.  `on_device` = 1 means the
+ * pointer is device memory; 0 means host memory (pageable or pinned).
+ * Field sizes are listed at LeniaField; count must match. */
+lenia_status lenia_set_field(lenia_world *w, int field, const float *src, size_t count, int on_device);
+lenia_status lenia_get_field(lenia_world *w, int field, float *dst, size_t count, int on_device);
+/* Number of floats of a field (0 if the field does not exist). */
+size_t lenia_field_size(const lenia_world *w, int field);
+
+/* Advances n_steps full steps (the 12 events FFT..TMB of render.cpp:376-583,
+ * TMB only when snapshots are on).  Stream-ordered; returns when queued. */
+lenia_status lenia_step(lenia_world *w, int n_steps);
+/* Runs one stage group of the current step (per-stage parity hooks). */
+lenia_status lenia_step_stage(lenia_world *w, int stage);
+
+/* Uses `stream` (a cudaStream_t) for all later work of this world. */
+lenia_status lenia_set_stream(lenia_world *w, void *stream);
+/* Waits for the world's stream and reports device-side errors. */
+lenia_status lenia_sync(lenia_world *w);
+/* 1: keep the intermediate fields marked (debug) in LeniaField. */
+lenia_status lenia_set_debug(lenia_world *w, int on);
+/* 1: keep the mesh snapshots H_RB / U_SUM_RB / RBB every step. */
+lenia_status lenia_set_snapshots(lenia_world *w, int on);
+
+/* 1: bracket every kernel launch with CUDA events on the world's stream and
+ * accumulate per-kernel device time (read with lenia_profile_read). */
+lenia_status lenia_set_profiling(lenia_world *w, int on);
+/* Synchronises, then writes per-kernel totals (milliseconds, launches) for
+ * up to `n` kernel ids and clears them; returns the number of kernel ids. */
+int lenia_profile_read(lenia_world *w, double *ms, long long *launches, int n);
+/* Name of kernel id `kid` of lenia_profile_read (NULL past the last). */
+const char *lenia_kernel_name(int kid);
+
+/* Number of kernel launches the last lenia_step issued per step. */
+int lenia_launches_per_step(const lenia_world *w);
+/* Human-readable description of the last failure on w (never NULL). */
+const char *lenia_last_error(const lenia_world *w);
+/* Library version string. */
+const char *lenia_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

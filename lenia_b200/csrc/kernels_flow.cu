@@ -1,0 +1,212 @@
+// Flow stage of the 3D Flow Lenia step, fused into one kernel: the events
+// TSB, SOBEL_ONE, SOBEL_TWO, F, MU and TB of render.cpp:425-548.
+//   gradient of SUM and of each H channel: sum_sobel / h_sobel
+//     (reintegration.cpp:191-259, coefficient tables lenia.h:30-71) or
+//     sum_central_diff / h_central_diff (reintegration.cpp:260-315);
+//   halo faces as the border routines leave them (transposition.cpp:6-665):
+//     torus copies the opposite face, wall the nearest interior cell, none
+//     zero; edge and corner halo cells read 0;
+//   alpha = clamp((A/theta_A)^2, 0, 1) read at the reference's offsets
+//     (lenia.cpp:650-671, compute_f at lenia.cpp:700-712);
+//   F = NU (1 - alpha) - NA alpha (lenia.cpp:679-719);
+//   MU and V: compute_{f,velocity}_mu[_wall] (reintegration.cpp:321-602).
+// Every float operation keeps the reference's order and rounding (this file
+// is compiled with -fmad=false), so outputs match the CPU restatement bit for
+// bit given the same inputs.
+#include "lenia_internal.h"
+
+namespace lenia {
+
+constexpr int kFX = 32, kFY = 8, kFZ = 8;  // output tile
+constexpr int kSX = kFX + 2, kSY = kFY + 2, kSZ = kFZ + 2;
+
+__device__ __forceinline__ float smax(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ float smin(float a, float b) { return a < b ? a : b; }
+
+// Value of a gradient input at (x, y, z), the reference's halo rules.
+__device__ __forceinline__ float gb_read(const float *f, const Dims &d, int x, int y, int z, int border)
+{
+    const int ox = (x < 0) | (x >= d.W), oy = (y < 0) | (y >= d.H), oz = (z < 0) | (z >= d.D);
+    const int no = ox + oy + oz;
+    if (no == 0) return __ldg(f + x + (long long)y * d.W + (long long)z * d.W * d.H);
+    if (no > 1 || border == kBorderNone) return 0.0f;
+    if (border == kBorderTorus) {
+        x = x < 0 ? x + d.W : (x >= d.W ? x - d.W : x);
+        y = y < 0 ? y + d.H : (y >= d.H ? y - d.H : y);
+        z = z < 0 ? z + d.D : (z >= d.D ? z - d.D : z);
+    } else {
+        x = x < 0 ? 0 : (x >= d.W ? d.W - 1 : x);
+        y = y < 0 ? 0 : (y >= d.H ? d.H - 1 : y);
+        z = z < 0 ? 0 : (z >= d.D ? d.D - 1 : z);
+    }
+    return __ldg(f + x + (long long)y * d.W + (long long)z * d.W * d.H);
+}
+
+__device__ __forceinline__ void load_tile(float *tile, const float *f, const Dims &d, int x0, int y0, int z0,
+                                          int border)
+{
+    const int tid = threadIdx.x + threadIdx.y * kFX;
+    for (int e = tid; e < kSX * kSY * kSZ; e += kFX * kFY) {
+        const int lx = e % kSX, ly = (e / kSX) % kSY, lz = e / (kSX * kSY);
+        tile[e] = gb_read(f, d, x0 + lx - 1, y0 + ly - 1, z0 + lz - 1, border);
+    }
+}
+
+__device__ __forceinline__ float sob_w(int dd) { return dd == 0 ? 2.0f : 1.0f; }
+
+// Gradient at tile position (lx, ly, lz) (interior coordinates).
+__device__ __forceinline__ void gradient(const float *tile, int lx, int ly, int lz, int sobel, float &gx, float &gy,
+                                         float &gz)
+{
+    if (sobel) {
+        float ax = 0.0f, ay = 0.0f, az = 0.0f;
+#pragma unroll
+        for (int dz = -1; dz <= 1; dz++)
+#pragma unroll
+            for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+                for (int dx = -1; dx <= 1; dx++) {
+                    const float v = tile[(lx + 1 + dx) + (ly + 1 + dy) * kSX + (lz + 1 + dz) * kSX * kSY];
+                    ax = ax + v * (sob_w(dx) * sob_w(dy) * (float)dz);
+                    ay = ay + v * ((float)dx * sob_w(dy) * sob_w(dz));
+                    az = az + v * (sob_w(dx) * (float)dy * sob_w(dz));
+                }
+        gx = ax;
+        gy = ay;
+        gz = az;
+    } else {
+        const int c = (lx + 1) + (ly + 1) * kSX + (lz + 1) * kSX * kSY;
+        gx = (tile[c + 1] - tile[c - 1]) * 0.5f;
+        gy = (tile[c + kSX] - tile[c - kSX]) * 0.5f;
+        gz = (tile[c + kSX * kSY] - tile[c - kSX * kSY]) * 0.5f;
+    }
+}
+
+__global__ void __launch_bounds__(kFX *kFY) k_flow(StepParams p, FlowBuffers b)
+{
+    __shared__ float tile[kSX * kSY * kSZ];
+    const Dims &d = p.d;
+    const int C = p.C;
+    const long long N = d.N;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int tiles_x = (d.W + kFX - 1) / kFX;
+    const int x0 = (blockIdx.x % tiles_x) * kFX;
+    const int y0 = (blockIdx.x / tiles_x) * kFY;
+    const int z0 = blockIdx.y * kFZ;
+    const int x = x0 + tx, y = y0 + ty;
+    const bool col_in = x < d.W && y < d.H;
+    const int sobel = p.gradient_mode == kGradSobel;
+
+    float na[kFZ][3];
+    load_tile(tile, b.SUM, d, x0, y0, z0, p.sobel_border);
+    __syncthreads();
+#pragma unroll
+    for (int lz = 0; lz < kFZ; lz++) gradient(tile, tx, ty, lz, sobel, na[lz][0], na[lz][1], na[lz][2]);
+    if (b.NA && col_in) {
+#pragma unroll
+        for (int lz = 0; lz < kFZ; lz++) {
+            const int z = z0 + lz;
+            if (z >= d.D) continue;
+            const long long i = x + (long long)y * d.W + (long long)z * d.W * d.H;
+            b.NA[i] = na[lz][0];
+            b.NA[N + i] = na[lz][1];
+            b.NA[2 * N + i] = na[lz][2];
+        }
+    }
+    const float ta = p.theta_a;
+    for (int c = 0; c < C; c++) {
+        __syncthreads();
+        load_tile(tile, b.H + (long long)c * N, d, x0, y0, z0, p.sobel_border);
+        __syncthreads();
+        if (!col_in) continue;
+#pragma unroll
+        for (int lz = 0; lz < kFZ; lz++) {
+            const int z = z0 + lz;
+            if (z >= d.D) continue;
+            const long long i = x + (long long)y * d.W + (long long)z * d.W * d.H;
+            const long long ci = (long long)c * N + i;
+            float nu[3];
+            gradient(tile, tx, ty, lz, sobel, nu[0], nu[1], nu[2]);
+            // alpha: PREALPHA as compute_f reads it (flat index c*N + i), which
+            // sobel_convolve_h wrote from channel f / P, cell f % P (Q20).
+            float alpha;
+            {
+                long long src_c = c, src_i = i;
+                bool valid = true;
+                if (!p.alpha_index_fix) {
+                    const long long f = ci;
+                    src_c = f / d.P;
+                    src_i = f - src_c * d.P;
+                    valid = src_c < C && src_i < N;
+                }
+                if (valid) {
+                    const float g = __ldg(b.A + src_c * N + src_i);
+                    float pg = g / ta;
+                    pg = pg * pg;
+                    alpha = smin(smax(pg, 0.0f), 1.0f);
+                } else {
+                    alpha = 0.0f;
+                }
+            }
+            if (b.PREALPHA) b.PREALPHA[ci] = alpha;
+            if (b.NU) {
+                b.NU[ci] = nu[0];
+                b.NU[(long long)C * N + ci] = nu[1];
+                b.NU[2LL * C * N + ci] = nu[2];
+            }
+            if (b.ALPHA) {
+                // ALPHA = |GRID - GA| with GA read at c*P + i (Q20)
+                // (GA blocks past the last channel are never written: 0)
+                const float g = __ldg(b.A + ci);
+                const long long f = p.alpha_index_fix ? ci : (long long)c * d.P + i;
+                const float ga = f < (long long)C * N ? __ldg(b.GA + f) : 0.0f;
+                b.ALPHA[ci] = fabsf(g - ga);
+            }
+            const float a1 = 1.0f - alpha;
+            float f3[3];
+#pragma unroll
+            for (int q = 0; q < 3; q++) f3[q] = nu[q] * a1 - na[lz][q] * alpha;
+            if (b.F) {
+#pragma unroll
+                for (int q = 0; q < 3; q++) b.F[(long long)q * C * N + ci] = f3[q];
+            }
+            float v3[3];
+#pragma unroll
+            for (int q = 0; q < 3; q++) v3[q] = b.V[(long long)q * C * N + ci];
+            const float pos[3] = {(float)x + 0.5f, (float)y + 0.5f, (float)z + 0.5f};
+            if (p.mu_vel) {
+#pragma unroll
+                for (int q = 0; q < 3; q++) v3[q] = (v3[q] + f3[q]) * p.v_damp;
+            }
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                float m = (p.mu_vel ? v3[q] : f3[q]) * p.timestep;
+                m = smax(m, -p.ma);
+                m = smin(m, p.ma);
+                m = pos[q] + m;
+                if (p.border == kBorderWall) {
+                    m = smax(m, p.sigma);
+                    m = smin(m, q == 1 ? p.ghs : p.gws);
+                }
+                b.MU[(long long)q * C * N + ci] = m;
+            }
+            if (!p.mu_vel) {
+#pragma unroll
+                for (int q = 0; q < 3; q++) v3[q] = (v3[q] + f3[q]) * p.v_damp;
+            }
+#pragma unroll
+            for (int q = 0; q < 3; q++) b.V[(long long)q * C * N + ci] = v3[q];
+        }
+    }
+}
+
+cudaError_t launch_flow(const StepParams &p, const FlowBuffers &b, cudaStream_t st)
+{
+    const int tiles_x = (p.d.W + kFX - 1) / kFX, tiles_y = (p.d.H + kFY - 1) / kFY;
+    dim3 grid(tiles_x * tiles_y, (p.d.D + kFZ - 1) / kFZ);
+    dim3 block(kFX, kFY);
+    k_flow<<<grid, block, 0, st>>>(p, b);
+    return cudaGetLastError();
+}
+
+}  // namespace lenia

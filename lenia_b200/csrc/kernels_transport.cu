@@ -1,0 +1,230 @@
+// Transport stage of the 3D Flow Lenia step, fused into one kernel: the
+// events REINTEGRATION and TRM of render.cpp:550-569.
+//   reintegration_step (lenia.cpp:727-918): srt, rt_border_torus,
+//     rt_border_other, adv_vel, adv_f (reintegration.cpp:607-1410) written as
+//     a destination gather per cell, then the oscillators;
+//   halo cells as transpose_borders leaves them (transposition.cpp:671-876):
+//     (int)dd periodic layers on faces, edges and corners 0;
+//   transpose_to_row_major (lenia.cpp:924-1037): growth or clamp, the moving
+//     averages GA and SUM, the new grid (written to a second buffer: the
+//     gather reads the old one).
+// Float operation order and rounding are the reference's (-fmad=false).
+#include "lenia_internal.h"
+
+namespace lenia {
+
+__device__ __forceinline__ float tmax(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ float tmin(float a, float b) { return a < b ? a : b; }
+
+// Value of a transported field at (x, y, z), the reference's halo rules.
+__device__ __forceinline__ float tb_read(const float *f, const Dims &d, int dd, int x, int y, int z)
+{
+    const int ox = (x < 0) | (x >= d.W), oy = (y < 0) | (y >= d.H), oz = (z < 0) | (z >= d.D);
+    const int no = ox + oy + oz;
+    if (no == 0) return __ldg(f + x + (long long)y * d.W + (long long)z * d.W * d.H);
+    if (no > 1) return 0.0f;
+    if (x < -dd || x >= d.W + dd || y < -dd || y >= d.H + dd || z < -dd || z >= d.D + dd) return 0.0f;
+    x = x < 0 ? x + d.W : (x >= d.W ? x - d.W : x);
+    y = y < 0 ? y + d.H : (y >= d.H ? y - d.H : y);
+    z = z < 0 ? z + d.D : (z >= d.D ? z - d.D : z);
+    return __ldg(f + x + (long long)y * d.W + (long long)z * d.W * d.H);
+}
+
+__device__ __forceinline__ float torus_wrap(float m, int ext)
+{
+    const float half = (float)(ext / 2);
+    if (m > half) m = m - (float)ext;
+    if (m < -half) m = m + (float)ext;
+    return m;
+}
+
+__device__ __forceinline__ float fastexp_dev(float x)
+{
+    const float a0 = 1.0f, a1 = 1.0f, a2 = 1.0f / 2, a3 = 1.0f / 2 / 3, a4 = 1.0f / 2 / 3 / 4,
+                a5 = 1.0f / 2 / 3 / 4 / 5, a6 = 1.0f / 2 / 3 / 4 / 5 / 6, a7 = 1.0f / 2 / 3 / 4 / 5 / 6 / 7;
+    float r = a7 * x + a6;
+    r = r * x + a5;
+    r = r * x + a4;
+    r = r * x + a3;
+    r = r * x + a2;
+    r = r * x + a1;
+    r = r * x + a0;
+    return r;
+}
+
+__global__ void __launch_bounds__(256) k_transport(StepParams p, TransportBuffers b)
+{
+    const Dims &d = p.d;
+    const long long N = d.N;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int C = p.C;
+    const int x = (int)(i % d.W), y = (int)((i / d.W) % d.H), z = (int)(i / ((long long)d.W * d.H));
+    const float px = (float)x + 0.5f, py = (float)y + 0.5f, pz = (float)z + 0.5f;
+    const int dd = p.dd;
+    float tt[kMaxChannels];
+#pragma unroll
+    for (int c = 0; c < kMaxChannels; c++) tt[c] = 0.0f;
+
+    if (p.mode_type == kModeSRT || p.mode_type == kModeRT) {
+        const int crt = p.rt_all_channels ? C : (C < 3 ? C : 3);
+        const bool torus = p.border == kBorderTorus;
+        for (int c = 0; c < crt; c++) {
+            const float *mux = b.MU + (long long)c * N;
+            const float *muy = b.MU + (long long)(C + c) * N;
+            const float *muz = b.MU + (long long)(2 * C + c) * N;
+            const float *arr = b.ARR + (long long)c * N;
+            float acc = 0.0f;
+            if (p.mode_type == kModeSRT) {
+                float mx = fabsf(px - __ldg(mux + i)), my = fabsf(py - __ldg(muy + i)), mz = fabsf(pz - __ldg(muz + i));
+                mx = tmin(tmax(p.si - mx, 0.0f), p.clip);
+                my = tmin(tmax(p.si - my, 0.0f), p.clip);
+                mz = tmin(tmax(p.si - mz, 0.0f), p.clip);
+                float w = __ldg(arr + i) * mx;
+                w = w * my;
+                w = w * mz;
+                w = w * p.sn;
+                acc = acc + w;
+            } else {
+                for (int oz = -dd; oz <= dd; oz++)
+                    for (int oy = -dd; oy <= dd; oy++)
+                        for (int ox = -dd; ox <= dd; ox++) {
+                            const int sx = x + ox, sy = y + oy, sz = z + oz;
+                            float mx = px - tb_read(mux, d, dd, sx, sy, sz);
+                            float my = py - tb_read(muy, d, dd, sx, sy, sz);
+                            float mz = pz - tb_read(muz, d, dd, sx, sy, sz);
+                            if (torus) {
+                                mx = torus_wrap(mx, d.W);
+                                my = torus_wrap(my, d.H);
+                                mz = torus_wrap(mz, d.D);
+                            }
+                            mx = fabsf(mx);
+                            my = fabsf(my);
+                            mz = fabsf(mz);
+                            mx = p.si - mx;
+                            my = p.si - my;
+                            mz = p.si - mz;
+                            mx = tmax(mx, 0.0f);
+                            my = tmax(my, 0.0f);
+                            mz = tmax(mz, 0.0f);
+                            mx = tmin(mx, p.clip);
+                            my = tmin(my, p.clip);
+                            mz = tmin(mz, p.clip);
+                            float w = tb_read(arr, d, dd, sx, sy, sz) * mx;
+                            w = w * my;
+                            w = w * mz;
+                            w = w * p.sn;
+                            acc = acc + w;
+                        }
+            }
+            tt[c] = acc;
+        }
+    } else if (p.mode_type == kModeADV) {
+        const float *vel = p.adv_vel ? b.V : b.F;
+        const float ext[3] = {(float)d.W, (float)d.H, (float)d.W};
+        const float pos[3] = {px, py, pz};
+        for (int c = 0; c < C; c++) {
+            int i0[3];
+            float fr[3];
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                float v = __ldg(vel + (long long)(q * C + c) * N + i) * p.timestep;
+                v = tmin(tmax(v, -p.ma), p.ma);
+                float X = (pos[q] - 0.5f) - v;
+                X = X + ext[q];
+                X = X - floorf(X / ext[q]) * ext[q];
+                const float X0 = floorf(X);
+                i0[q] = (int)X0;
+                fr[q] = X - X0;
+            }
+            const float *arr = b.ARR + (long long)c * N;
+            const float fx = fr[0], fy = fr[1], fz = fr[2];
+            const float nfx = 1.0f - fx, nfy = 1.0f - fy, nfz = 1.0f - fz;
+            const int x0 = i0[0], y0 = i0[1], z0 = i0[2];
+            float s = tb_read(arr, d, dd, x0, y0, z0) * nfx * nfy * nfz;
+            s = s + tb_read(arr, d, dd, x0 + 1, y0, z0) * fx * nfy * nfz;
+            s = s + tb_read(arr, d, dd, x0, y0 + 1, z0) * nfx * fy * nfz;
+            s = s + tb_read(arr, d, dd, x0 + 1, y0 + 1, z0) * fx * fy * nfz;
+            s = s + tb_read(arr, d, dd, x0, y0, z0 + 1) * nfx * nfy * fz;
+            s = s + tb_read(arr, d, dd, x0 + 1, y0, z0 + 1) * fx * nfy * fz;
+            s = s + tb_read(arr, d, dd, x0, y0 + 1, z0 + 1) * nfx * fy * fz;
+            s = s + tb_read(arr, d, dd, x0 + 1, y0 + 1, z0 + 1) * fx * fy * fz;
+            tt[c] = s;
+        }
+    }
+
+    if (p.osc_la || p.osc_flow || p.osc_div_flow) {
+        const float *fl = p.osc_vel ? b.V : b.F;
+        for (int c = 0; c < C; c++) {
+            const float *g = b.A + (long long)c * N;
+            const float fx1 = tb_read(g, d, dd, x + 1, y, z), fx0 = tb_read(g, d, dd, x - 1, y, z);
+            const float fy1 = tb_read(g, d, dd, x, y + 1, z), fy0 = tb_read(g, d, dd, x, y - 1, z);
+            const float fz1 = tb_read(g, d, dd, x, y, z + 1), fz0 = tb_read(g, d, dd, x, y, z - 1);
+            const float dxv = fx1 - fx0, dyv = fy1 - fy0, dzv = fz1 - fz0;
+            float t = tt[c];
+            if (p.osc_la) {
+                const float la = fx1 + fx0 + fy1 + fy0 + fz1 + fz0 - 6 * __ldg(g + i);
+                t = t + la * p.osc_la_amt;
+            }
+            if (p.osc_flow) {
+                const float flow = __ldg(fl + (long long)c * N + i) * dxv + __ldg(fl + (long long)(C + c) * N + i) * dyv +
+                                   __ldg(fl + (long long)(2 * C + c) * N + i) * dzv;
+                t = t + flow * p.osc_flow_amt;
+            }
+            if (p.osc_div_flow) {
+                const float *fxs = fl + (long long)c * N, *fys = fl + (long long)(C + c) * N,
+                            *fzs = fl + (long long)(2 * C + c) * N;
+                const float *al = b.ALPHA + (long long)c * N;
+                const float jx = tb_read(fxs, d, dd, x + 1, y, z) * tb_read(al, d, dd, x + 1, y, z) -
+                                 tb_read(fxs, d, dd, x - 1, y, z) * tb_read(al, d, dd, x - 1, y, z);
+                const float jy = tb_read(fys, d, dd, x, y + 1, z) * tb_read(al, d, dd, x, y + 1, z) -
+                                 tb_read(fys, d, dd, x, y - 1, z) * tb_read(al, d, dd, x, y - 1, z);
+                const float jz = tb_read(fzs, d, dd, x, y, z + 1) * tb_read(al, d, dd, x, y, z + 1) -
+                                 tb_read(fzs, d, dd, x, y, z - 1) * tb_read(al, d, dd, x, y, z - 1);
+                const float divj = jx + jy + jz;
+                t = t + divj * p.osc_div_flow_amt;
+            }
+            tt[c] = t;
+        }
+    }
+    if (b.TT)
+        for (int c = 0; c < C; c++) b.TT[(long long)c * N + i] = tt[c];
+
+    // transpose_to_row_major
+    if (p.growth_type == kGrowthTransposition) {
+        for (int c = 0; c < C; c++) {
+            const long long ci = (long long)c * N + i;
+            const float h = __ldg(b.H + ci);
+            if (p.soft_clip[c]) {
+                float v = __ldg(b.A + ci) + h * p.timestep;
+                v = -4.0f * (v - 0.5f);
+                v = fastexp_dev(v);
+                v = 1.0f + v;
+                v = 1.0f / v;
+                b.BACK[ci] = tmin(tmax(v, 0.0f), 1.0f);
+            } else {
+                tt[c] = tmin(tmax(tt[c] + h * p.timestep, 0.0f), 1.0f);
+            }
+        }
+    } else {
+        for (int c = 0; c < C; c++) tt[c] = tmin(tmax(tt[c], 0.0f), 1.0f);
+    }
+    const float stam = 1.0f - p.sta, stas = p.sta, gtas = p.gta, gtam = 1.0f - p.gta;
+    float ttsum = 0.0f;
+    for (int c = 0; c < C; c++) {
+        const long long ci = (long long)c * N + i;
+        ttsum = ttsum + tt[c];
+        b.GA[ci] = gtam * b.GA[ci] + tt[c] * gtas;
+        b.A_out[ci] = tt[c];
+    }
+    // SUM was cleared at the end of reintegration (lenia.cpp:912-915)
+    b.SUM[i] = stam * 0.0f + ttsum * stas;
+}
+
+cudaError_t launch_transport(const StepParams &p, const TransportBuffers &b, cudaStream_t st)
+{
+    k_transport<<<(unsigned)((p.d.N + 255) / 256), 256, 0, st>>>(p, b);
+    return cudaGetLastError();
+}
+
+}  // namespace lenia

@@ -1,0 +1,938 @@
+// C ABI of the B200 3D Flow Lenia step (include/lenia_b200.h): world
+// lifetime, validation, FFT plans, field I/O and the stream-ordered step.
+//
+// One step issues, in the reference's event order (render.cpp:376-583):
+//   GROWTH     fwd_rows + planes (forward) + planes (inverse, x kernel) +
+//              growth_rows                                   FFT, FFT_MT
+//   BLUR       (central difference with blur) the same chain with the blur
+//              kernel, storing U_S and SUM_S                  BLUR
+//   FLOW       one fused stencil kernel                       TSB .. TB
+//   TRANSPORT  one fused gather kernel                        REINTEGRATION, TRM
+//   SNAPSHOT   (when enabled) grid copy for meshing           TMB
+#include <math.h>
+#include <stdio.h>
+#include <stdarg.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "lenia_internal.h"
+
+using namespace lenia;
+
+namespace lenia {
+int row_tile(const Dims &d, const FftPlan &px);
+bool plane_fits(const Dims &d, const FftPlan &py, const FftPlan &pz);
+
+int fft_factor(int n, int *radix)
+{
+    int k = 0;
+    if (n < 1) return -1;
+    while (n % 8 == 0 && k < kMaxStages) { radix[k++] = 8; n /= 8; }
+    if (n % 4 == 0) { radix[k++] = 4; n /= 4; }
+    if (n % 2 == 0) { radix[k++] = 2; n /= 2; }
+    const int odd[4] = {3, 5, 7, 11};
+    for (int i = 0; i < 4; i++)
+        while (n % odd[i] == 0 && k < kMaxStages) { radix[k++] = odd[i]; n /= odd[i]; }
+    return n == 1 ? k : -1;
+}
+}  // namespace lenia
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+// Twiddles tw[t] = (cos 2 pi t/n, sign sin 2 pi t/n): double, stored as float.
+std::vector<float2> twiddles(int n, int sign)
+{
+    std::vector<float2> t(n);
+    for (int i = 0; i < n; i++) {
+        const double ang = (2.0 * kPi * (double)i) / (double)n;
+        const double c = cos(ang), s = sin(ang);
+        t[i].x = (float)c;
+        t[i].y = (float)(sign < 0 ? -s : s);
+    }
+    return t;
+}
+
+template <typename T>
+T *dalloc(size_t count, cudaError_t &err)
+{
+    T *p = nullptr;
+    if (err != cudaSuccess || count == 0) return nullptr;
+    err = cudaMalloc((void **)&p, count * sizeof(T));
+    if (err == cudaSuccess) err = cudaMemset(p, 0, count * sizeof(T));
+    return err == cudaSuccess ? p : nullptr;
+}
+
+}  // namespace
+
+enum KernelId {
+    KID_FWD_ROWS = 0,
+    KID_PLANES_FWD,
+    KID_PLANES_INV,
+    KID_GROWTH_ROWS,
+    KID_BLUR_FWD_ROWS,
+    KID_BLUR_PLANES_FWD,
+    KID_BLUR_PLANES_INV,
+    KID_BLUR_ROWS,
+    KID_FLOW,
+    KID_TRANSPORT,
+    KID_MAX
+};
+const char *const kKernelNames[KID_MAX] = {"fwd_rows",          "planes_fwd",          "planes_inv",
+                                           "growth_rows",       "blur_fwd_rows",       "blur_planes_fwd",
+                                           "blur_planes_inv",   "blur_rows",           "flow",
+                                           "transport"};
+
+struct ProfRec {
+    int kid;
+    cudaEvent_t a, b;
+};
+
+struct lenia_world {
+    LeniaWorldDesc desc;
+    std::vector<LeniaKernelParams> kernels;
+    Dims d;
+    int C = 0, K = 0;
+    FftPlan px, py;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;  // created by lenia_create
+    int device = 0;
+    bool debug = false, snapshots = false;
+    int launches = 0;
+    std::string err;
+    // device state
+    float *A = nullptr, *A_next = nullptr, *V = nullptr, *GA = nullptr, *SUM = nullptr;
+    float *H = nullptr, *H_RB = nullptr, *U_SUM = nullptr, *U_SUM_RB = nullptr, *BACK = nullptr;
+    float *MU = nullptr, *F = nullptr, *ALPHA = nullptr, *U_S = nullptr, *SUM_S = nullptr, *RBB = nullptr;
+    float *NA = nullptr, *NU = nullptr, *PREALPHA = nullptr, *TT = nullptr, *U = nullptr;
+    float2 *XS = nullptr;   // (C+1) half spectra
+    float2 *S = nullptr;    // max(K, C+1) half spectra
+    float *Kc = nullptr;    // K octant kernel spectra
+    float *blur_hat = nullptr;
+    float *lut_rows = nullptr;
+    int *lut_base = nullptr;
+    float *ksum = nullptr;  // K + 1 normalisation sums
+    LeniaKernelParams *kp_dev = nullptr;
+    float2 *tw_x_fwd = nullptr, *tw_x_inv = nullptr, *tw_y_fwd = nullptr, *tw_y_inv = nullptr;
+    int *err_flag = nullptr;
+    int lut_base_host[kMaxKernels];
+    bool blur_valid = false;  // U_S / SUM_S hold a blur result
+    // profiling
+    bool profile = false;
+    std::vector<ProfRec> prof_pending;
+    std::vector<cudaEvent_t> prof_free;
+    double prof_ms[KID_MAX] = {};
+    long long prof_n[KID_MAX] = {};
+};
+
+namespace {
+
+cudaEvent_t prof_event(lenia_world *w)
+{
+    if (!w->prof_free.empty()) {
+        cudaEvent_t e = w->prof_free.back();
+        w->prof_free.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Brackets the launches issued between prof_begin and prof_end.
+struct ProfScope {
+    lenia_world *w;
+    int kid;
+    cudaEvent_t a = nullptr;
+    ProfScope(lenia_world *w_, int kid_) : w(w_), kid(kid_)
+    {
+        if (w->profile) {
+            a = prof_event(w);
+            cudaEventRecord(a, w->stream);
+        }
+    }
+    ~ProfScope()
+    {
+        if (a) {
+            cudaEvent_t b = prof_event(w);
+            cudaEventRecord(b, w->stream);
+            w->prof_pending.push_back({kid, a, b});
+        }
+    }
+};
+
+lenia_status fail(lenia_world *w, lenia_status s, const char *fmt, ...)
+{
+    if (w) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        w->err = buf;
+    }
+    return s;
+}
+
+lenia_status cuda_fail(lenia_world *w, cudaError_t e, const char *what)
+{
+    if (e == cudaErrorMemoryAllocation) return fail(w, LENIA_ERR_OOM, "%s: %s", what, cudaGetErrorString(e));
+    return fail(w, LENIA_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+bool dim_ok(int n)
+{
+    int r[kMaxStages];
+    return n >= 8 && n <= 256 && n % 4 == 0 && fft_factor(n, r) > 0;
+}
+
+lenia_status validate_desc(lenia_world *w, const LeniaWorldDesc *d)
+{
+    if (!d) return fail(w, LENIA_ERR_INVALID_ARG, "desc is NULL");
+    if (!dim_ok(d->width) || !dim_ok(d->height))
+        return fail(w, LENIA_ERR_INVALID_ARG,
+                    "width/height must be in [8,256], multiples of 4, with prime factors in {2,3,5,7,11} "
+                    "(got %d x %d)", d->width, d->height);
+    if (d->channels < 1 || d->channels > LENIA_MAX_CHANNELS)
+        return fail(w, LENIA_ERR_INVALID_ARG, "channels must be 1..%d", LENIA_MAX_CHANNELS);
+    if (!(d->sigma > 0.0f) || !(d->dd >= 1.0f) || d->dd >= 5.0f)
+        return fail(w, LENIA_ERR_INVALID_ARG, "need sigma > 0 and 1 <= dd < 5 (the reference pads 4 cells)");
+    if (d->growth_type < 0 || d->growth_type > 2 || d->mode_type < 0 || d->mode_type > 2 || d->border < 0 ||
+        d->border > 2 || d->sobel_border < 0 || d->sobel_border > 2 || d->gradient_mode < 0 || d->gradient_mode > 1)
+        return fail(w, LENIA_ERR_INVALID_ARG, "mode enum out of range");
+    return LENIA_OK;
+}
+
+lenia_status validate_kernels(lenia_world *w, const LeniaKernelParams *k, int n, int channels)
+{
+    if (n < 0 || n > LENIA_MAX_KERNELS) return fail(w, LENIA_ERR_INVALID_ARG, "n_kernels must be 0..%d", LENIA_MAX_KERNELS);
+    if (n > 0 && !k) return fail(w, LENIA_ERR_INVALID_ARG, "kernels is NULL");
+    for (int i = 0; i < n; i++) {
+        if (k[i].radius < 1 || k[i].beta_size < 1 || k[i].beta_size > LENIA_MAX_BETA || !(k[i].r_a > 0.0f))
+            return fail(w, LENIA_ERR_INVALID_ARG, "kernel %d: need radius >= 1, 1 <= beta_size <= %d, r_a > 0", i,
+                        LENIA_MAX_BETA);
+        if (k[i].c0 < 0 || k[i].c0 >= channels || k[i].c1 < 0 || k[i].c1 >= channels)
+            return fail(w, LENIA_ERR_INVALID_ARG, "kernel %d: channel out of range", i);
+    }
+    return LENIA_OK;
+}
+
+StepParams step_params(const lenia_world *w)
+{
+    const LeniaWorldDesc &s = w->desc;
+    StepParams p;
+    memset(&p, 0, sizeof(p));
+    p.d = w->d;
+    p.C = w->C;
+    p.timestep = s.timestep;
+    p.theta_a = s.theta_a;
+    p.s_norm = s.s_norm;
+    p.gta = s.gta;
+    p.sta = s.sta;
+    p.v_damp = s.v_damp;
+    p.sigma = s.sigma;
+    p.dd_f = s.dd;
+    p.dd = (int)s.dd;
+    p.growth_type = s.growth_type;
+    p.mode_type = s.mode_type;
+    p.sobel_border = s.sobel_border;
+    p.border = s.border;
+    p.gradient_mode = s.gradient_mode;
+    p.adv_vel = s.adv_vel;
+    p.mu_vel = s.mu_vel;
+    p.blur = s.blur_central_diff;
+    p.osc_la = s.osc_la;
+    p.osc_flow = s.osc_flow;
+    p.osc_div_flow = s.osc_div_flow;
+    p.osc_vel = s.osc_vel;
+    p.osc_la_amt = s.osc_la_amt;
+    p.osc_flow_amt = s.osc_flow_amt;
+    p.osc_div_flow_amt = s.osc_div_flow_amt;
+    for (int c = 0; c < kMaxChannels; c++) {
+        p.asymptotic[c] = s.asymptotic[c];
+        p.soft_clip[c] = s.soft_clip[c];
+    }
+    p.rt_all_channels = s.rt_all_channels;
+    p.alpha_index_fix = s.alpha_index_fix;
+    // off_table.ma (lenia.cpp:143) and the reintegration constants
+    // (lenia.cpp:730-736, reintegration.cpp:610, 328-329), in float.
+    const float sigma = s.sigma;
+    p.ma = s.dd - s.sigma;
+    const float s2 = 1 / (4 * sigma * sigma);
+    const float s23 = 1 / (2 * sigma * sigma * sigma);
+    p.sn = s2 * (1 - s.s_norm) + (s.s_norm * s23);
+    p.clip = 2.0f * sigma < 1.0f ? 2.0f * sigma : 1.0f;
+    p.si = 0.5f + sigma;
+    p.gws = (float)w->d.W - sigma;
+    p.ghs = (float)w->d.H - sigma;
+    return p;
+}
+
+bool needs_F(const LeniaWorldDesc &s)
+{
+    return (s.mode_type == LENIA_MODE_ADV && !s.adv_vel) || ((s.osc_flow || s.osc_div_flow) && !s.osc_vel);
+}
+
+lenia_status ensure_optional(lenia_world *w)
+{
+    cudaError_t e = cudaSuccess;
+    const size_t CN = (size_t)w->C * w->d.N;
+    if ((w->debug || needs_F(w->desc)) && !w->F) w->F = dalloc<float>(3 * CN, e);
+    if ((w->debug || w->desc.osc_div_flow) && !w->ALPHA) w->ALPHA = dalloc<float>(CN, e);
+    if (w->debug) {
+        if (!w->NA) w->NA = dalloc<float>(3 * (size_t)w->d.N, e);
+        if (!w->NU) w->NU = dalloc<float>(3 * CN, e);
+        if (!w->PREALPHA) w->PREALPHA = dalloc<float>(CN, e);
+        if (!w->TT) w->TT = dalloc<float>(CN, e);
+        if (!w->U && w->K > 0) w->U = dalloc<float>((size_t)w->K * w->d.N, e);
+    }
+    if (w->snapshots && !w->RBB) w->RBB = dalloc<float>(CN, e);
+    if (e != cudaSuccess) return cuda_fail(w, e, "allocating optional fields");
+    return LENIA_OK;
+}
+
+// Kernel spectra, growth-table rows and the blur spectrum.
+lenia_status build_kernels(lenia_world *w)
+{
+    cudaError_t e = cudaSuccess;
+    const Dims &d = w->d;
+    const int K = w->K;
+    cudaStream_t st = w->stream;
+    if (K > 0) {
+        e = cudaMemcpyAsync(w->kp_dev, w->kernels.data(), sizeof(LeniaKernelParams) * K, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return cuda_fail(w, e, "copying kernels");
+    }
+    float *grids = nullptr;
+    size_t ng = (size_t)std::max(K, 1) * d.N;
+    e = cudaMallocAsync((void **)&grids, ng * sizeof(float), st);
+    if (e != cudaSuccess) return cuda_fail(w, e, "kernel grid scratch");
+    if ((e = launch_kernel_grids(d, w->kp_dev, K, grids, w->ksum, st)) != cudaSuccess) goto out;
+    for (int k0 = 0; k0 < K; k0 += 2 * kMaxPairs) {
+        FwdRowJobs fj;
+        memset(&fj, 0, sizeof(fj));
+        PlaneJobs pj;
+        memset(&pj, 0, sizeof(pj));
+        for (int k = k0; k < K && k < k0 + 2 * kMaxPairs; k += 2) {
+            const int p = fj.npairs++;
+            fj.in[2 * p] = grids + (size_t)k * d.N;
+            fj.out[2 * p] = w->S + (size_t)k * d.HS;
+            fj.in[2 * p + 1] = k + 1 < K ? grids + (size_t)(k + 1) * d.N : nullptr;
+            fj.out[2 * p + 1] = k + 1 < K ? w->S + (size_t)(k + 1) * d.HS : nullptr;
+        }
+        if ((e = launch_fwd_rows(d, w->px, w->tw_x_fwd, fj, st)) != cudaSuccess) goto out;
+        for (int k = k0; k < K && k < k0 + 2 * kMaxPairs; k++) {
+            if (pj.njobs == kMaxKernels + 8) {
+                if ((e = launch_planes(d, w->py, w->px, w->tw_y_fwd, w->tw_x_fwd, pj, -1, st)) != cudaSuccess) goto out;
+                pj.njobs = 0;
+            }
+            pj.src[pj.njobs] = w->S + (size_t)k * d.HS;
+            pj.dst[pj.njobs] = w->S + (size_t)k * d.HS;
+            pj.kc[pj.njobs] = nullptr;
+            pj.njobs++;
+        }
+        if (pj.njobs && (e = launch_planes(d, w->py, w->px, w->tw_y_fwd, w->tw_x_fwd, pj, -1, st)) != cudaSuccess)
+            goto out;
+    }
+    for (int k = 0; k < K; k++) {
+        const size_t kh = (size_t)d.KX * (d.D / 2 + 1) * (d.H / 2 + 1);
+        if ((e = launch_compress(d, w->S + (size_t)k * d.HS, w->Kc + k * kh, st)) != cudaSuccess) goto out;
+    }
+    // blur kernel (precompute_blur_kernel, reintegration.cpp:13-78)
+    if ((e = launch_blur_grid(d, grids, w->ksum + K, st)) != cudaSuccess) goto out;
+    {
+        FwdRowJobs fj;
+        memset(&fj, 0, sizeof(fj));
+        fj.npairs = 1;
+        fj.in[0] = grids;
+        fj.out[0] = w->S;
+        if ((e = launch_fwd_rows(d, w->px, w->tw_x_fwd, fj, st)) != cudaSuccess) goto out;
+        PlaneJobs pj;
+        memset(&pj, 0, sizeof(pj));
+        pj.njobs = 1;
+        pj.src[0] = w->S;
+        pj.dst[0] = w->S;
+        if ((e = launch_planes(d, w->py, w->px, w->tw_y_fwd, w->tw_x_fwd, pj, -1, st)) != cudaSuccess) goto out;
+        if ((e = launch_compress(d, w->S, w->blur_hat, st)) != cudaSuccess) goto out;
+    }
+    if ((e = launch_lut_rows(w->kp_dev, K, w->lut_rows, w->lut_base, st)) != cudaSuccess) goto out;
+    if (K > 0) {
+        e = cudaMemcpyAsync(w->lut_base_host, w->lut_base, sizeof(int) * K, cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) goto out;
+    }
+out:
+    cudaFreeAsync(grids, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(w, e, "building kernels");
+    return LENIA_OK;
+}
+
+void free_world(lenia_world *w)
+{
+    float *fs[] = {w->A, w->A_next, w->V, w->GA, w->SUM, w->H, w->H_RB, w->U_SUM, w->U_SUM_RB, w->BACK, w->MU,
+                   w->F, w->ALPHA, w->U_S, w->SUM_S, w->RBB, w->NA, w->NU, w->PREALPHA, w->TT, w->U, w->Kc,
+                   w->blur_hat, w->lut_rows, w->ksum};
+    for (float *p : fs)
+        if (p) cudaFree(p);
+    void *vs[] = {w->XS, w->S, w->lut_base, w->kp_dev, w->tw_x_fwd, w->tw_x_inv, w->tw_y_fwd, w->tw_y_inv,
+                  w->err_flag};
+    for (void *p : vs)
+        if (p) cudaFree(p);
+}
+
+// ---------------------------------------------------------------- stages
+
+lenia_status stage_growth(lenia_world *w)
+{
+    const Dims &d = w->d;
+    cudaStream_t st = w->stream;
+    cudaError_t e;
+    if (w->snapshots) {
+        std::swap(w->H, w->H_RB);
+        std::swap(w->U_SUM, w->U_SUM_RB);
+    }
+    // forward transforms of the grid channels, packed in pairs
+    FwdRowJobs fj;
+    memset(&fj, 0, sizeof(fj));
+    for (int c = 0; c < w->C; c += 2) {
+        const int p = fj.npairs++;
+        fj.in[2 * p] = w->A + (size_t)c * d.N;
+        fj.out[2 * p] = w->XS + (size_t)c * d.HS;
+        fj.in[2 * p + 1] = c + 1 < w->C ? w->A + (size_t)(c + 1) * d.N : nullptr;
+        fj.out[2 * p + 1] = c + 1 < w->C ? w->XS + (size_t)(c + 1) * d.HS : nullptr;
+    }
+    {
+        ProfScope ps(w, KID_FWD_ROWS);
+        if ((e = launch_fwd_rows(d, w->px, w->tw_x_fwd, fj, st)) != cudaSuccess) return cuda_fail(w, e, "fwd_rows");
+    }
+    PlaneJobs pj;
+    memset(&pj, 0, sizeof(pj));
+    pj.njobs = w->C;
+    for (int c = 0; c < w->C; c++) {
+        pj.src[c] = w->XS + (size_t)c * d.HS;
+        pj.dst[c] = w->XS + (size_t)c * d.HS;
+        pj.kc[c] = nullptr;
+    }
+    {
+        ProfScope ps(w, KID_PLANES_FWD);
+        if ((e = launch_planes(d, w->py, w->px, w->tw_y_fwd, w->tw_x_fwd, pj, -1, st)) != cudaSuccess)
+            return cuda_fail(w, e, "planes (forward)");
+    }
+    w->launches += 2;
+    if (w->K > 0) {
+        const size_t kh = (size_t)d.KX * (d.D / 2 + 1) * (d.H / 2 + 1);
+        memset(&pj, 0, sizeof(pj));
+        pj.njobs = w->K;
+        for (int k = 0; k < w->K; k++) {
+            pj.src[k] = w->XS + (size_t)w->kernels[k].c0 * d.HS;
+            pj.dst[k] = w->S + (size_t)k * d.HS;
+            pj.kc[k] = w->Kc + k * kh;
+        }
+        ProfScope ps(w, KID_PLANES_INV);
+        if ((e = launch_planes(d, w->py, w->px, w->tw_y_inv, w->tw_x_inv, pj, +1, st)) != cudaSuccess)
+            return cuda_fail(w, e, "planes (inverse)");
+        w->launches++;
+    }
+    GrowthJobs gj;
+    memset(&gj, 0, sizeof(gj));
+    gj.K = w->K;
+    gj.C = w->C;
+    for (int k = 0; k < w->K; k++) {
+        gj.spec[k] = w->S + (size_t)k * d.HS;
+        gj.c1[k] = w->kernels[k].c1;
+        gj.h[k] = w->kernels[k].h;
+        gj.lut_base[k] = w->lut_base_host[k];
+    }
+    for (int c = 0; c < kMaxChannels; c++) {
+        gj.asymptotic[c] = w->desc.asymptotic[c];
+        gj.soft_clip[c] = w->desc.soft_clip[c];
+    }
+    gj.growth_rt = w->desc.growth_type == LENIA_GROWTH_RT;
+    gj.timestep = w->desc.timestep;
+    {
+        ProfScope ps(w, KID_GROWTH_ROWS);
+        if ((e = launch_growth_rows(d, w->px, w->tw_x_inv, gj, w->lut_rows, w->A, w->H, w->U_SUM, w->BACK,
+                                    w->debug ? w->U : nullptr, w->err_flag, st)) != cudaSuccess)
+            return cuda_fail(w, e, "growth_rows");
+    }
+    w->launches++;
+    return LENIA_OK;
+}
+
+lenia_status stage_blur(lenia_world *w)
+{
+    const LeniaWorldDesc &s = w->desc;
+    if (s.gradient_mode != LENIA_GRADIENT_CENTRAL_DIFF || !s.blur_central_diff) {
+        w->blur_valid = false;
+        return LENIA_OK;
+    }
+    const Dims &d = w->d;
+    cudaStream_t st = w->stream;
+    cudaError_t e;
+    const int nf = w->C + 1;  // H_0..H_{C-1}, SUM
+    FwdRowJobs fj;
+    memset(&fj, 0, sizeof(fj));
+    auto field_in = [&](int f) -> const float * { return f < w->C ? w->H + (size_t)f * d.N : w->SUM; };
+    auto field_out = [&](int f) -> float * { return f < w->C ? w->U_S + (size_t)f * d.N : w->SUM_S; };
+    for (int f = 0; f < nf; f += 2) {
+        const int p = fj.npairs++;
+        fj.in[2 * p] = field_in(f);
+        fj.out[2 * p] = w->XS + (size_t)f * d.HS;
+        fj.in[2 * p + 1] = f + 1 < nf ? field_in(f + 1) : nullptr;
+        fj.out[2 * p + 1] = f + 1 < nf ? w->XS + (size_t)(f + 1) * d.HS : nullptr;
+    }
+    {
+        ProfScope ps(w, KID_BLUR_FWD_ROWS);
+        if ((e = launch_fwd_rows(d, w->px, w->tw_x_fwd, fj, st)) != cudaSuccess)
+            return cuda_fail(w, e, "blur fwd_rows");
+    }
+    PlaneJobs pj;
+    memset(&pj, 0, sizeof(pj));
+    pj.njobs = nf;
+    for (int f = 0; f < nf; f++) {
+        pj.src[f] = w->XS + (size_t)f * d.HS;
+        pj.dst[f] = w->XS + (size_t)f * d.HS;
+    }
+    {
+        ProfScope ps(w, KID_BLUR_PLANES_FWD);
+        if ((e = launch_planes(d, w->py, w->px, w->tw_y_fwd, w->tw_x_fwd, pj, -1, st)) != cudaSuccess)
+            return cuda_fail(w, e, "blur planes (forward)");
+    }
+    for (int f = 0; f < nf; f++) {
+        pj.src[f] = w->XS + (size_t)f * d.HS;
+        pj.dst[f] = w->S + (size_t)f * d.HS;
+        pj.kc[f] = w->blur_hat;
+    }
+    {
+        ProfScope ps(w, KID_BLUR_PLANES_INV);
+        if ((e = launch_planes(d, w->py, w->px, w->tw_y_inv, w->tw_x_inv, pj, +1, st)) != cudaSuccess)
+            return cuda_fail(w, e, "blur planes (inverse)");
+    }
+    BlurJobs bj;
+    memset(&bj, 0, sizeof(bj));
+    bj.nfields = nf;
+    for (int f = 0; f < nf; f++) {
+        bj.spec[f] = w->S + (size_t)f * d.HS;
+        bj.out[f] = field_out(f);
+    }
+    {
+        ProfScope ps(w, KID_BLUR_ROWS);
+        if ((e = launch_blur_rows(d, w->px, w->tw_x_inv, bj, st)) != cudaSuccess) return cuda_fail(w, e, "blur rows");
+    }
+    w->launches += 4;
+    w->blur_valid = true;
+    return LENIA_OK;
+}
+
+lenia_status stage_flow(lenia_world *w)
+{
+    lenia_status s = ensure_optional(w);
+    if (s != LENIA_OK) return s;
+    StepParams p = step_params(w);
+    FlowBuffers b;
+    memset(&b, 0, sizeof(b));
+    const bool cd = w->desc.gradient_mode == LENIA_GRADIENT_CENTRAL_DIFF;
+    // Without the blur, U_S and SUM_S are plain copies of H and SUM
+    // (the intended h_sum_blur copy): read H and SUM directly.
+    b.H = (cd && w->blur_valid) ? w->U_S : w->H;
+    b.SUM = (cd && w->blur_valid) ? w->SUM_S : w->SUM;
+    b.A = w->A;
+    b.GA = w->GA;
+    b.V = w->V;
+    b.MU = w->MU;
+    b.F = (w->debug || needs_F(w->desc)) ? w->F : nullptr;
+    b.ALPHA = (w->debug || w->desc.osc_div_flow) ? w->ALPHA : nullptr;
+    if (w->debug) {
+        b.NA = w->NA;
+        b.NU = w->NU;
+        b.PREALPHA = w->PREALPHA;
+    }
+    cudaError_t e;
+    {
+        ProfScope ps(w, KID_FLOW);
+        e = launch_flow(p, b, w->stream);
+    }
+    if (e != cudaSuccess) return cuda_fail(w, e, "flow");
+    w->launches++;
+    return LENIA_OK;
+}
+
+lenia_status stage_transport(lenia_world *w)
+{
+    StepParams p = step_params(w);
+    TransportBuffers b;
+    memset(&b, 0, sizeof(b));
+    const bool use_grid =
+        w->desc.growth_type == LENIA_GROWTH_NOGROWTH || w->desc.growth_type == LENIA_GROWTH_TRANSPOSITION;
+    b.A = w->A;
+    b.A_out = w->A_next;
+    b.ARR = use_grid ? w->A : w->BACK;
+    b.MU = w->MU;
+    b.H = w->H;
+    b.V = w->V;
+    b.F = w->F;
+    b.ALPHA = w->ALPHA;
+    b.GA = w->GA;
+    b.SUM = w->SUM;
+    b.BACK = w->BACK;
+    b.TT = w->debug ? w->TT : nullptr;
+    cudaError_t e;
+    {
+        ProfScope ps(w, KID_TRANSPORT);
+        e = launch_transport(p, b, w->stream);
+    }
+    if (e != cudaSuccess) return cuda_fail(w, e, "transport");
+    std::swap(w->A, w->A_next);
+    w->launches++;
+    return LENIA_OK;
+}
+
+lenia_status stage_snapshot(lenia_world *w)
+{
+    lenia_status s = ensure_optional(w);
+    if (s != LENIA_OK) return s;
+    if (!w->RBB) return LENIA_OK;
+    cudaError_t e = cudaMemcpyAsync(w->RBB, w->A, sizeof(float) * w->C * w->d.N, cudaMemcpyDeviceToDevice, w->stream);
+    if (e != cudaSuccess) return cuda_fail(w, e, "snapshot");
+    return LENIA_OK;
+}
+
+float *field_ptr(lenia_world *w, int field, size_t *count)
+{
+    const size_t N = w->d.N, CN = (size_t)w->C * N;
+    const bool cd_plain = !w->blur_valid;
+    switch (field) {
+    case LENIA_FIELD_A: *count = CN; return w->A;
+    case LENIA_FIELD_V: *count = 3 * CN; return w->V;
+    case LENIA_FIELD_GA: *count = CN; return w->GA;
+    case LENIA_FIELD_SUM: *count = N; return w->SUM;
+    case LENIA_FIELD_H: *count = CN; return w->H;
+    case LENIA_FIELD_U_SUM: *count = CN; return w->U_SUM;
+    case LENIA_FIELD_BACK: *count = CN; return w->BACK;
+    case LENIA_FIELD_NA: *count = 3 * N; return w->NA;
+    case LENIA_FIELD_NU: *count = 3 * CN; return w->NU;
+    case LENIA_FIELD_PREALPHA: *count = CN; return w->PREALPHA;
+    case LENIA_FIELD_ALPHA: *count = CN; return w->ALPHA;
+    case LENIA_FIELD_F: *count = 3 * CN; return w->F;
+    case LENIA_FIELD_MU: *count = 3 * CN; return w->MU;
+    case LENIA_FIELD_TT: *count = CN; return w->TT;
+    case LENIA_FIELD_U_S: *count = CN; return cd_plain ? w->H : w->U_S;
+    case LENIA_FIELD_SUM_S: *count = N; return cd_plain ? w->SUM : w->SUM_S;
+    case LENIA_FIELD_U: *count = (size_t)w->K * N; return w->U;
+    case LENIA_FIELD_H_RB: *count = CN; return w->snapshots ? w->H_RB : nullptr;
+    case LENIA_FIELD_U_SUM_RB: *count = CN; return w->snapshots ? w->U_SUM_RB : nullptr;
+    case LENIA_FIELD_RBB: *count = CN; return w->RBB;
+    default: *count = 0; return nullptr;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *lenia_version(void) { return "lenia_b200 0.1 (sm_100a)"; }
+
+lenia_status lenia_create(const LeniaWorldDesc *desc, const LeniaKernelParams *kernels, int n_kernels,
+                          lenia_world **out)
+{
+    if (!out) return LENIA_ERR_INVALID_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return LENIA_ERR_NO_DEVICE;
+    }
+    lenia_world *w = new lenia_world();
+    lenia_status s = validate_desc(w, desc);
+    if (s == LENIA_OK) s = validate_kernels(w, kernels, n_kernels, desc->channels);
+    if (s != LENIA_OK) {
+        fprintf(stderr, "lenia_create: %s\n", w->err.c_str());
+        delete w;
+        return s;
+    }
+    w->desc = *desc;
+    w->kernels.assign(kernels, kernels + n_kernels);
+    w->C = desc->channels;
+    w->K = n_kernels;
+    Dims &d = w->d;
+    d.W = desc->width;
+    d.H = desc->height;
+    d.D = desc->width;
+    d.N = (long long)d.W * d.H * d.D;
+    d.KX = d.W / 2 + 1;
+    d.HS = (long long)d.KX * d.D * d.H;
+    d.P = (long long)(d.W + 8) * (d.H + 8) * (d.W + 8);
+    w->px.n = d.W;
+    w->px.nstages = fft_factor(d.W, w->px.radix);
+    w->py.n = d.H;
+    w->py.nstages = fft_factor(d.H, w->py.radix);
+    if (row_tile(d, w->px) == 0 || !plane_fits(d, w->py, w->px)) {
+        delete w;
+        return LENIA_ERR_UNSUPPORTED;
+    }
+    cudaGetDevice(&w->device);
+    cudaError_t e = cudaSuccess;
+    const size_t N = d.N, CN = (size_t)w->C * N;
+    w->A = dalloc<float>(CN, e);
+    w->A_next = dalloc<float>(CN, e);
+    w->V = dalloc<float>(3 * CN, e);
+    w->GA = dalloc<float>(CN, e);
+    w->SUM = dalloc<float>(N, e);
+    w->H = dalloc<float>(CN, e);
+    w->H_RB = dalloc<float>(CN, e);
+    w->U_SUM = dalloc<float>(CN, e);
+    w->U_SUM_RB = dalloc<float>(CN, e);
+    w->BACK = dalloc<float>(CN, e);
+    w->MU = dalloc<float>(3 * CN, e);
+    w->U_S = dalloc<float>(CN, e);
+    w->SUM_S = dalloc<float>(N, e);
+    w->XS = dalloc<float2>((size_t)(w->C + 1) * d.HS, e);
+    w->S = dalloc<float2>((size_t)std::max(w->K, w->C + 1) * d.HS, e);
+    const size_t kh = (size_t)d.KX * (d.D / 2 + 1) * (d.H / 2 + 1);
+    w->Kc = dalloc<float>(std::max(w->K, 1) * kh, e);
+    w->blur_hat = dalloc<float>(kh, e);
+    w->lut_rows = dalloc<float>(256 * (size_t)std::max(w->K, 1), e);
+    w->lut_base = dalloc<int>(std::max(w->K, 1), e);
+    w->ksum = dalloc<float>(w->K + 1, e);
+    w->kp_dev = dalloc<LeniaKernelParams>(kMaxKernels, e);
+    w->tw_x_fwd = dalloc<float2>(d.W, e);
+    w->tw_x_inv = dalloc<float2>(d.W, e);
+    w->tw_y_fwd = dalloc<float2>(d.H, e);
+    w->tw_y_inv = dalloc<float2>(d.H, e);
+    w->err_flag = dalloc<int>(1, e);
+    if (e == cudaSuccess) {
+        auto a = twiddles(d.W, -1), b = twiddles(d.W, +1), c = twiddles(d.H, -1), dd = twiddles(d.H, +1);
+        e = cudaMemcpy(w->tw_x_fwd, a.data(), sizeof(float2) * d.W, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(w->tw_x_inv, b.data(), sizeof(float2) * d.W, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(w->tw_y_fwd, c.data(), sizeof(float2) * d.H, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(w->tw_y_inv, dd.data(), sizeof(float2) * d.H, cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&w->own_stream, cudaStreamNonBlocking);
+    w->stream = w->own_stream;
+    if (e != cudaSuccess) {
+        s = e == cudaErrorMemoryAllocation ? LENIA_ERR_OOM : LENIA_ERR_CUDA;
+        fprintf(stderr, "lenia_create: %s\n", cudaGetErrorString(e));
+        free_world(w);
+        delete w;
+        return s;
+    }
+    s = build_kernels(w);
+    if (s != LENIA_OK) {
+        fprintf(stderr, "lenia_create: %s\n", w->err.c_str());
+        free_world(w);
+        delete w;
+        return s;
+    }
+    *out = w;
+    return LENIA_OK;
+}
+
+lenia_status lenia_destroy(lenia_world *w)
+{
+    if (!w) return LENIA_ERR_INVALID_ARG;
+    cudaStreamSynchronize(w->stream);
+    for (const ProfRec &r : w->prof_pending) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (cudaEvent_t e : w->prof_free) cudaEventDestroy(e);
+    free_world(w);
+    if (w->own_stream) cudaStreamDestroy(w->own_stream);
+    delete w;
+    return LENIA_OK;
+}
+
+lenia_status lenia_set_params(lenia_world *w, const LeniaWorldDesc *desc)
+{
+    if (!w) return LENIA_ERR_INVALID_ARG;
+    lenia_status s = validate_desc(w, desc);
+    if (s != LENIA_OK) return s;
+    if (desc->width != w->desc.width || desc->height != w->desc.height || desc->channels != w->desc.channels)
+        return fail(w, LENIA_ERR_INVALID_ARG, "set_params cannot change the grid shape or channel count");
+    w->desc = *desc;
+    return LENIA_OK;
+}
+
+lenia_status lenia_set_kernels(lenia_world *w, const LeniaKernelParams *kernels, int n_kernels)
+{
+    if (!w) return LENIA_ERR_INVALID_ARG;
+    lenia_status s = validate_kernels(w, kernels, n_kernels, w->C);
+    if (s != LENIA_OK) return s;
+    const Dims &d = w->d;
+    cudaError_t e = cudaStreamSynchronize(w->stream);
+    if (e != cudaSuccess) return cuda_fail(w, e, "set_kernels");
+    if (n_kernels > w->K) {
+        // grow the per-kernel buffers
+        const size_t kh = (size_t)d.KX * (d.D / 2 + 1) * (d.H / 2 + 1);
+        cudaFree(w->S);
+        cudaFree(w->Kc);
+        cudaFree(w->lut_rows);
+        cudaFree(w->lut_base);
+        cudaFree(w->ksum);
+        if (w->U) { cudaFree(w->U); w->U = nullptr; }
+        e = cudaSuccess;
+        w->S = dalloc<float2>((size_t)std::max(n_kernels, w->C + 1) * d.HS, e);
+        w->Kc = dalloc<float>(n_kernels * kh, e);
+        w->lut_rows = dalloc<float>(256 * (size_t)n_kernels, e);
+        w->lut_base = dalloc<int>(n_kernels, e);
+        w->ksum = dalloc<float>(n_kernels + 1, e);
+        if (e != cudaSuccess) return cuda_fail(w, e, "set_kernels");
+    }
+    w->kernels.assign(kernels, kernels + n_kernels);
+    w->K = n_kernels;
+    return build_kernels(w);
+}
+
+size_t lenia_field_size(const lenia_world *w, int field)
+{
+    if (!w) return 0;
+    size_t n = 0;
+    field_ptr(const_cast<lenia_world *>(w), field, &n);
+    return n;
+}
+
+lenia_status lenia_set_field(lenia_world *w, int field, const float *src, size_t count, int on_device)
+{
+    if (!w || !src) return LENIA_ERR_INVALID_ARG;
+    if (field == LENIA_FIELD_U_S || field == LENIA_FIELD_SUM_S) {
+        // the blur stage owns these; writing them selects them as flow inputs
+        w->blur_valid = true;
+    }
+    if (field == LENIA_FIELD_H_RB || field == LENIA_FIELD_U_SUM_RB || field == LENIA_FIELD_RBB) {
+        w->snapshots = true;
+    }
+    lenia_status s = ensure_optional(w);
+    if (s != LENIA_OK) return s;
+    size_t n = 0;
+    float *p = field_ptr(w, field, &n);
+    if (!p) return fail(w, LENIA_ERR_INVALID_ARG, "field %d is not available (enable debug?)", field);
+    if (count != n) return fail(w, LENIA_ERR_INVALID_ARG, "field %d holds %zu floats, got %zu", field, n, count);
+    cudaError_t e = cudaMemcpyAsync(p, src, count * sizeof(float),
+                                    on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, w->stream);
+    if (e == cudaSuccess && !on_device) e = cudaStreamSynchronize(w->stream);
+    if (e != cudaSuccess) return cuda_fail(w, e, "set_field");
+    return LENIA_OK;
+}
+
+lenia_status lenia_get_field(lenia_world *w, int field, float *dst, size_t count, int on_device)
+{
+    if (!w || !dst) return LENIA_ERR_INVALID_ARG;
+    size_t n = 0;
+    float *p = field_ptr(w, field, &n);
+    if (!p) return fail(w, LENIA_ERR_INVALID_ARG, "field %d is not available (enable debug?)", field);
+    if (count != n) return fail(w, LENIA_ERR_INVALID_ARG, "field %d holds %zu floats, got %zu", field, n, count);
+    cudaError_t e = cudaMemcpyAsync(dst, p, count * sizeof(float),
+                                    on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, w->stream);
+    if (e == cudaSuccess && !on_device) e = cudaStreamSynchronize(w->stream);
+    if (e != cudaSuccess) return cuda_fail(w, e, "get_field");
+    return LENIA_OK;
+}
+
+lenia_status lenia_step_stage(lenia_world *w, int stage)
+{
+    if (!w) return LENIA_ERR_INVALID_ARG;
+    switch (stage) {
+    case LENIA_STAGE_GROWTH: return stage_growth(w);
+    case LENIA_STAGE_BLUR: return stage_blur(w);
+    case LENIA_STAGE_FLOW: return stage_flow(w);
+    case LENIA_STAGE_TRANSPORT: return stage_transport(w);
+    case LENIA_STAGE_SNAPSHOT: return stage_snapshot(w);
+    default: return fail(w, LENIA_ERR_INVALID_ARG, "unknown stage %d", stage);
+    }
+}
+
+lenia_status lenia_step(lenia_world *w, int n_steps)
+{
+    if (!w || n_steps < 0) return LENIA_ERR_INVALID_ARG;
+    lenia_status s = ensure_optional(w);
+    if (s != LENIA_OK) return s;
+    for (int i = 0; i < n_steps; i++) {
+        w->launches = 0;
+        if ((s = stage_growth(w)) != LENIA_OK) return s;
+        if ((s = stage_blur(w)) != LENIA_OK) return s;
+        if ((s = stage_flow(w)) != LENIA_OK) return s;
+        if ((s = stage_transport(w)) != LENIA_OK) return s;
+        if (w->snapshots && (s = stage_snapshot(w)) != LENIA_OK) return s;
+    }
+    return LENIA_OK;
+}
+
+lenia_status lenia_set_stream(lenia_world *w, void *stream)
+{
+    if (!w) return LENIA_ERR_INVALID_ARG;
+    cudaError_t e = cudaStreamSynchronize(w->stream);
+    if (e != cudaSuccess) return cuda_fail(w, e, "set_stream");
+    w->stream = (cudaStream_t)stream;
+    return LENIA_OK;
+}
+
+lenia_status lenia_sync(lenia_world *w)
+{
+    if (!w) return LENIA_ERR_INVALID_ARG;
+    cudaError_t e = cudaStreamSynchronize(w->stream);
+    if (e != cudaSuccess) return cuda_fail(w, e, "sync");
+    int flag = 0;
+    e = cudaMemcpy(&flag, w->err_flag, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(w, e, "sync");
+    if (flag) {
+        cudaMemset(w->err_flag, 0, sizeof(int));
+        return fail(w, LENIA_ERR_NONFINITE, "non-finite u met in the growth table lookup");
+    }
+    return LENIA_OK;
+}
+
+lenia_status lenia_set_debug(lenia_world *w, int on)
+{
+    if (!w) return LENIA_ERR_INVALID_ARG;
+    w->debug = on != 0;
+    return ensure_optional(w);
+}
+
+lenia_status lenia_set_snapshots(lenia_world *w, int on)
+{
+    if (!w) return LENIA_ERR_INVALID_ARG;
+    w->snapshots = on != 0;
+    return ensure_optional(w);
+}
+
+lenia_status lenia_set_profiling(lenia_world *w, int on)
+{
+    if (!w) return LENIA_ERR_INVALID_ARG;
+    w->profile = on != 0;
+    return LENIA_OK;
+}
+
+int lenia_profile_read(lenia_world *w, double *ms, long long *launches, int n)
+{
+    if (!w) return -1;
+    cudaStreamSynchronize(w->stream);
+    for (const ProfRec &r : w->prof_pending) {
+        float t = 0.0f;
+        if (cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) {
+            w->prof_ms[r.kid] += t;
+            w->prof_n[r.kid] += 1;
+        }
+        w->prof_free.push_back(r.a);
+        w->prof_free.push_back(r.b);
+    }
+    w->prof_pending.clear();
+    for (int k = 0; k < KID_MAX && k < n; k++) {
+        if (ms) ms[k] = w->prof_ms[k];
+        if (launches) launches[k] = w->prof_n[k];
+        w->prof_ms[k] = 0.0;
+        w->prof_n[k] = 0;
+    }
+    return KID_MAX;
+}
+
+const char *lenia_kernel_name(int kid) { return kid >= 0 && kid < KID_MAX ? kKernelNames[kid] : nullptr; }
+
+int lenia_launches_per_step(const lenia_world *w) { return w ? w->launches : 0; }
+
+const char *lenia_last_error(const lenia_world *w) { return w ? w->err.c_str() : "null world"; }
+
+}  // extern "C"

@@ -1,0 +1,135 @@
+// Internal declarations shared by the host code (lenia_api.cu) and the CUDA
+// kernels of the 3D Flow Lenia step.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/lenia_b200.h"
+#include "lfft_device.cuh"
+
+namespace lenia {
+
+constexpr int kMaxKernels = 64;
+constexpr int kMaxChannels = 4;
+constexpr int kMaxPairs = 40;       // packed real-field pairs in one forward launch
+constexpr int kPlaneThreads = 512;  // block size of the plane transform
+constexpr int kPlaneCap = 32;       // values per thread in the plane transform
+constexpr int kRowThreads = 256;    // block size of the row transforms
+constexpr int kRowCap = 32;
+
+enum { kBorderTorus = 0, kBorderWall = 1, kBorderNone = 2 };
+enum { kGrowthNone = 0, kGrowthRT = 1, kGrowthTransposition = 2 };
+enum { kModeSRT = 0, kModeRT = 1, kModeADV = 2 };
+enum { kGradCentralDiff = 0, kGradSobel = 1 };
+
+struct Dims {
+    int W, H, D;  // x, y, z extents (D == W)
+    long long N;  // cells
+    int KX;       // W/2 + 1
+    long long HS; // KX * D * H complex entries of a half spectrum
+    long long P;  // (W+8)(H+8)(W+8): the reference's padded block (Q20)
+};
+
+// Forward row pass: up to kMaxPairs pairs of real fields -> half spectra.
+struct FwdRowJobs {
+    const float *in[2 * kMaxPairs];
+    float2 *out[2 * kMaxPairs];
+    int npairs;
+};
+
+// Plane pass: one job per (array); a job transforms every kx plane of it.
+struct PlaneJobs {
+    const float2 *src[kMaxKernels + 8];
+    float2 *dst[kMaxKernels + 8];
+    const float *kc[kMaxKernels + 8];  // octant kernel spectrum, or null
+    int njobs;
+};
+
+// Inverse row pass with the growth epilogue.
+struct GrowthJobs {
+    const float2 *spec[kMaxKernels];
+    int c1[kMaxKernels];
+    float h[kMaxKernels];
+    int lut_base[kMaxKernels];
+    int K;
+    int C;
+    int asymptotic[kMaxChannels];
+    int soft_clip[kMaxChannels];
+    int growth_rt;  // write BACK
+    float timestep;
+};
+
+// Inverse row pass storing field/N (the blur).
+struct BlurJobs {
+    const float2 *spec[2 * kMaxChannels + 2];
+    float *out[2 * kMaxChannels + 2];
+    int nfields;
+};
+
+// Everything the flow and transport kernels read, by value.
+struct StepParams {
+    Dims d;
+    int C;
+    float timestep, theta_a, s_norm, gta, sta, v_damp, sigma, dd_f;
+    int dd;
+    int growth_type, mode_type, sobel_border, border, gradient_mode;
+    int adv_vel, mu_vel, blur;
+    int osc_la, osc_flow, osc_div_flow, osc_vel;
+    float osc_la_amt, osc_flow_amt, osc_div_flow_amt;
+    int asymptotic[kMaxChannels], soft_clip[kMaxChannels];
+    int rt_all_channels, alpha_index_fix;
+    // derived (computed on the host in the reference's float expressions)
+    float ma, sn, clip, si, gws, ghs;
+};
+
+struct FlowBuffers {
+    const float *H;      // H (Sobel) or U_S (central difference), C*N
+    const float *SUM;    // SUM (Sobel) or SUM_S, N
+    const float *A;      // C*N
+    const float *GA;     // C*N (ALPHA only)
+    float *V;            // 3*C*N, updated in place
+    float *MU;           // 3*C*N
+    float *F;            // 3*C*N or null
+    float *ALPHA;        // C*N or null
+    float *NA, *NU, *PREALPHA;  // debug outputs or null (PREALPHA: 4*N flat)
+};
+
+struct TransportBuffers {
+    const float *A;      // current grid, C*N
+    float *A_out;        // new grid, C*N
+    const float *ARR;    // GRID or BACK, C*N
+    const float *MU;     // 3*C*N
+    const float *H;      // C*N (growth by transposition)
+    const float *V;      // 3*C*N (advection, oscillators)
+    const float *F;      // 3*C*N or null
+    const float *ALPHA;  // C*N or null
+    float *GA;           // C*N, updated in place
+    float *SUM;          // N
+    float *BACK;         // C*N (transposition soft clip)
+    float *TT;           // debug: pre-clamp TT, or null
+};
+
+// Launch wrappers (kernels_*.cu); all are asynchronous on `st`.
+cudaError_t launch_fwd_rows(const Dims &d, const FftPlan &px, const float2 *tw_x, const FwdRowJobs &jobs,
+                            cudaStream_t st);
+cudaError_t launch_planes(const Dims &d, const FftPlan &py, const FftPlan &pz, const float2 *tw_y,
+                          const float2 *tw_z, const PlaneJobs &jobs, int sign, cudaStream_t st);
+cudaError_t launch_growth_rows(const Dims &d, const FftPlan &px, const float2 *tw_x_inv, const GrowthJobs &jobs,
+                               const float *lut_rows, const float *A, float *H, float *U_SUM, float *BACK,
+                               float *U_dbg, int *err_flag, cudaStream_t st);
+cudaError_t launch_blur_rows(const Dims &d, const FftPlan &px, const float2 *tw_x_inv, const BlurJobs &jobs,
+                             cudaStream_t st);
+cudaError_t launch_kernel_grids(const Dims &d, const LeniaKernelParams *kp_dev, int K, float *grids,
+                                float *ksum, cudaStream_t st);
+cudaError_t launch_blur_grid(const Dims &d, float *grid, float *ksum, cudaStream_t st);
+cudaError_t launch_compress(const Dims &d, const float2 *spec, float *kc, cudaStream_t st);
+cudaError_t launch_lut_rows(const LeniaKernelParams *kp_dev, int K, float *lut_rows, int *lut_base,
+                            cudaStream_t st);
+cudaError_t launch_flow(const StepParams &p, const FlowBuffers &b, cudaStream_t st);
+cudaError_t launch_transport(const StepParams &p, const TransportBuffers &b, cudaStream_t st);
+
+// Host FFT plans and twiddle tables (lenia_api.cu).
+int fft_factor(int n, int *radix);
+
+}  // namespace lenia

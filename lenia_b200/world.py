@@ -1,0 +1,149 @@
+"""Host-side mirror of the reference's step API over the C ABI.
+
+`World` owns one simulated grid on the GPU.  Its methods follow the
+reference's interface for the step: the parameter globals become a
+`WorldDesc`, the Kernel structs a list of `KernelParams`, the arrays are
+fields (`get` / `set`), and the event sequence of render.cpp:357-604 is
+`step()` (whole steps) or `stage()` (one stage group).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from .params import KernelParams, WorldDesc
+
+
+class World:
+    def __init__(self, desc: WorldDesc, kernels: Sequence[KernelParams]):
+        self._lib = _lib.load()
+        self.desc = desc
+        self.kernels = list(kernels)
+        self._cdesc = _lib.to_c_desc(desc)
+        self._ckern = _lib.to_c_kernels(self.kernels)
+        h = ctypes.c_void_p()
+        st = self._lib.lenia_create(ctypes.byref(self._cdesc), self._ckern, len(self.kernels), ctypes.byref(h))
+        if st != _lib.LENIA_OK:
+            raise _lib.LeniaError(st, "lenia_create failed")
+        self._h = h
+
+    # -------------------------------------------------------------- helpers
+    def _check(self, st: int):
+        if st != _lib.LENIA_OK:
+            msg = self._lib.lenia_last_error(self._h).decode()
+            raise _lib.LeniaError(st, msg)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.lenia_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    @property
+    def C(self) -> int:
+        return self.desc.channels
+
+    @property
+    def N(self) -> int:
+        return self.desc.cells
+
+    def field_size(self, name: str) -> int:
+        return int(self._lib.lenia_field_size(self._h, _lib.FIELD[name]))
+
+    # --------------------------------------------------------------- fields
+    def set(self, name: str, value) -> None:
+        """Writes a field from a numpy array (host) or a CUDA torch tensor."""
+        n = self.field_size(name) if name not in ("U_S", "SUM_S") else None
+        if hasattr(value, "is_cuda") and value.is_cuda:
+            t = value.contiguous()
+            self._check(self._lib.lenia_set_field(self._h, _lib.FIELD[name], ctypes.c_void_p(t.data_ptr()),
+                                                  t.numel(), 1))
+            return
+        a = np.ascontiguousarray(value, dtype=np.float32).ravel()
+        self._check(self._lib.lenia_set_field(self._h, _lib.FIELD[name], a.ctypes.data_as(ctypes.c_void_p),
+                                              a.size, 0))
+        del n
+
+    def get(self, name: str, out=None):
+        """Reads a field into a new numpy array, or into `out` (numpy or CUDA tensor)."""
+        n = self.field_size(name)
+        if n == 0:
+            raise _lib.LeniaError(1, f"field {name} is not available (enable debug or snapshots)")
+        if out is not None and hasattr(out, "is_cuda") and out.is_cuda:
+            self._check(self._lib.lenia_get_field(self._h, _lib.FIELD[name], ctypes.c_void_p(out.data_ptr()),
+                                                  out.numel(), 1))
+            return out
+        a = np.empty(n, dtype=np.float32) if out is None else out
+        self._check(self._lib.lenia_get_field(self._h, _lib.FIELD[name], a.ctypes.data_as(ctypes.c_void_p),
+                                              a.size, 0))
+        return a
+
+    def set_state(self, A: np.ndarray, V: Optional[np.ndarray] = None, GA: Optional[np.ndarray] = None,
+                  SUM: Optional[np.ndarray] = None) -> None:
+        """A new world state (the reference's reseed: every field zero, then A)."""
+        C, N = self.C, self.N
+        self.set("A", A)
+        self.set("V", np.zeros(3 * C * N, np.float32) if V is None else V)
+        self.set("GA", np.zeros(C * N, np.float32) if GA is None else GA)
+        self.set("SUM", np.zeros(N, np.float32) if SUM is None else SUM)
+
+    # ---------------------------------------------------------------- steps
+    def step(self, n: int = 1) -> None:
+        self._check(self._lib.lenia_step(self._h, int(n)))
+
+    def stage(self, name: str) -> None:
+        self._check(self._lib.lenia_step_stage(self._h, _lib.STAGE[name]))
+
+    def sync(self) -> None:
+        self._check(self._lib.lenia_sync(self._h))
+
+    def set_debug(self, on: bool = True) -> None:
+        self._check(self._lib.lenia_set_debug(self._h, int(on)))
+
+    def set_snapshots(self, on: bool = True) -> None:
+        self._check(self._lib.lenia_set_snapshots(self._h, int(on)))
+
+    def set_stream(self, stream_ptr: int) -> None:
+        self._check(self._lib.lenia_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def set_params(self, desc: WorldDesc) -> None:
+        self._cdesc = _lib.to_c_desc(desc)
+        self._check(self._lib.lenia_set_params(self._h, ctypes.byref(self._cdesc)))
+        self.desc = desc
+
+    def set_kernels(self, kernels: Sequence[KernelParams]) -> None:
+        self.kernels = list(kernels)
+        self._ckern = _lib.to_c_kernels(self.kernels)
+        self._check(self._lib.lenia_set_kernels(self._h, self._ckern, len(self.kernels)))
+
+    def set_profiling(self, on: bool = True) -> None:
+        self._check(self._lib.lenia_set_profiling(self._h, int(on)))
+
+    def profile_read(self) -> dict:
+        """Per-kernel device time since the last read: {name: (ms, launches)}."""
+        n = 32
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_longlong * n)()
+        k = self._lib.lenia_profile_read(self._h, ms, cnt, n)
+        out = {}
+        for i in range(max(k, 0)):
+            name = self._lib.lenia_kernel_name(i).decode()
+            if cnt[i]:
+                out[name] = (float(ms[i]), int(cnt[i]))
+        return out
+
+    @property
+    def launches_per_step(self) -> int:
+        return int(self._lib.lenia_launches_per_step(self._h))

@@ -184,15 +184,22 @@ void lfft_3d_c2c(lcf *x, int w, int h, int d, int sign)
     lfft_plan_init(&pd, d);
     int mx = w > h ? w : h;
     if (d > mx) mx = d;
-    lcf *work = (lcf *)malloc(sizeof(lcf) * 2 * (size_t)mx);
     const long plane = (long)w * h;
-    for (int z = 0; z < d; z++)
-        for (int y = 0; y < h; y++) lfft_1d(&pw, x + z * plane + (long)y * w, 1, sign, work);
-    for (int z = 0; z < d; z++)
-        for (int xx = 0; xx < w; xx++) lfft_1d(&ph, x + z * plane + xx, w, sign, work);
-    for (int y = 0; y < h; y++)
-        for (int xx = 0; xx < w; xx++) lfft_1d(&pd, x + (long)y * w + xx, plane, sign, work);
-    free(work);
+    /* lines are independent: any thread order gives the same bits */
+#pragma omp parallel
+    {
+        lcf *work = (lcf *)malloc(sizeof(lcf) * 2 * (size_t)mx);
+#pragma omp for schedule(static)
+        for (long zy = 0; zy < (long)d * h; zy++)
+            lfft_1d(&pw, x + (zy / h) * plane + (zy % h) * w, 1, sign, work);
+#pragma omp for schedule(static)
+        for (long zx = 0; zx < (long)d * w; zx++)
+            lfft_1d(&ph, x + (zx / w) * plane + (zx % w), w, sign, work);
+#pragma omp for schedule(static)
+        for (long yx = 0; yx < (long)h * w; yx++)
+            lfft_1d(&pd, x + (yx / w) * w + (yx % w), plane, sign, work);
+        free(work);
+    }
     lfft_plan_free(&pw);
     lfft_plan_free(&ph);
     lfft_plan_free(&pd);

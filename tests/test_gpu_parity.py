@@ -1,0 +1,132 @@
+"""Parity of the CUDA step with the CPU restatement (oracle/restate).
+
+The restatement runs in its half-spectrum mode, which performs the CUDA
+library's convolution arithmetic; every other stage is the reference's
+arithmetic (pinned bit for bit to the reference's own code by
+test_oracle_pin.py).  So the bar is bit-exact equality: after every stage
+group of every step, every field, in every mode.
+"""
+import numpy as np
+import pytest
+
+from lenia_cases import VARIANTS, as_oracle, diff_report, four_channels, two_channel_div_flow, variant
+from lenia_b200 import params as P
+from oracle.oracle import RestateOracle
+
+pytestmark = pytest.mark.gpu
+
+GROWTH_EVENTS = ["FFT", "FFT_MT"]
+FLOW_EVENTS = ["TSB", "SOBEL_ONE", "SOBEL_TWO", "F", "MU", "TB"]
+
+
+def make_pair(wl, debug=True):
+    from lenia_b200.world import World
+    p, ks = as_oracle(wl)
+    ora = RestateOracle(p, ks, fft_mode="half")
+    ora.set_state(A=wl.A0.ravel())
+    gpu = World(wl.desc, wl.kernels)
+    if debug:
+        gpu.set_debug(True)
+    gpu.set_state(wl.A0.ravel())
+    return ora, gpu
+
+
+def compare(ora, gpu, names, tag, problems):
+    for n in names:
+        r = diff_report(n, ora.get(n), gpu.get(n))
+        if r:
+            problems.append(f"{tag} {r}")
+
+
+def staged_step(ora, gpu, desc, tag, problems):
+    for ev in GROWTH_EVENTS:
+        ora.run_event(ev)
+    gpu.stage("GROWTH")
+    names = ["U", "H", "U_SUM"] + (["BACK"] if desc.growth_type == P.GROWTH_RT else [])
+    compare(ora, gpu, names, f"{tag} GROWTH", problems)
+    ora.run_event("BLUR")
+    gpu.stage("BLUR")
+    if desc.gradient_mode == P.GRADIENT_CENTRAL_DIFF:
+        compare(ora, gpu, ["U_S", "SUM_S"], f"{tag} BLUR", problems)
+    for ev in FLOW_EVENTS:
+        ora.run_event(ev)
+    gpu.stage("FLOW")
+    compare(ora, gpu, ["NA", "NU", "PREALPHA", "ALPHA", "F", "MU", "V"], f"{tag} FLOW", problems)
+    ora.run_event("REINTEGRATION")
+    gpu.stage("TRANSPORT")
+    compare(ora, gpu, ["TT"], f"{tag} REINTEGRATION", problems)
+    ora.run_event("TRM")
+    ora.run_event("TMB")
+    names = ["A", "GA", "SUM"]
+    if desc.growth_type == P.GROWTH_TRANSPOSITION and any(desc.soft_clip[:desc.channels]):
+        names.append("BACK")
+    compare(ora, gpu, names, f"{tag} TRANSPORT", problems)
+
+
+def run_staged(wl, steps=2):
+    ora, gpu = make_pair(wl)
+    problems = []
+    for s in range(steps):
+        staged_step(ora, gpu, wl.desc, f"step {s}", problems)
+    gpu.sync()
+    gpu.close()
+    return problems
+
+
+@pytest.mark.parametrize("name", sorted(VARIANTS))
+def test_stages_bit_exact(cuda_lib, oracle_built, name):
+    problems = run_staged(variant(name))
+    assert not problems, "\n".join(problems[:12])
+
+
+def test_stages_bit_exact_div_flow(cuda_lib, oracle_built):
+    problems = run_staged(two_channel_div_flow())
+    assert not problems, "\n".join(problems[:12])
+
+
+def test_stages_bit_exact_four_channels(cuda_lib, oracle_built):
+    problems = run_staged(four_channels())
+    assert not problems, "\n".join(problems[:12])
+
+
+@pytest.mark.parametrize("width", [24, 36, 44, 48])
+def test_stages_bit_exact_mixed_radix(cuda_lib, oracle_built, width):
+    """Grid sizes whose transforms use radices 3 and 11."""
+    problems = run_staged(variant("sobel_torus", seed=width, width=width), steps=1)
+    assert not problems, "\n".join(problems[:12])
+
+
+def test_trajectory_bit_exact_cfg0(cuda_lib, oracle_built):
+    """Whole steps (the production path, no debug outputs) stay bit-exact over
+    100 steps of the 32^3 plain-step configuration."""
+    from lenia_b200.world import World
+    wl = P.config0(seed=0)
+    p, ks = as_oracle(wl)
+    ora = RestateOracle(p, ks, fft_mode="half")
+    ora.set_state(A=wl.A0.ravel())
+    gpu = World(wl.desc, wl.kernels)
+    gpu.set_state(wl.A0.ravel())
+    for chunk in range(10):
+        ora.step(10)
+        gpu.step(10)
+        for n in ("A", "V", "GA", "SUM"):
+            r = diff_report(n, ora.get(n), gpu.get(n))
+            assert not r, f"after {10 * (chunk + 1)} steps: {r}"
+    gpu.sync()
+
+
+def test_config1_step_bit_exact(cuda_lib, oracle_built):
+    """One full step of the 128^3 x 4 channel, 16-kernel configuration."""
+    from lenia_b200.world import World
+    wl = P.config1(seed=1)
+    p, ks = as_oracle(wl)
+    ora = RestateOracle(p, ks, fft_mode="half")
+    ora.set_state(A=wl.A0.ravel())
+    gpu = World(wl.desc, wl.kernels)
+    gpu.set_state(wl.A0.ravel())
+    ora.step(1)
+    gpu.step(1)
+    for n in ("A", "V", "GA", "SUM", "H", "U_SUM", "BACK", "MU"):
+        r = diff_report(n, ora.get(n), gpu.get(n))
+        assert not r, r
+    gpu.sync()
