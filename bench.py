@@ -83,6 +83,11 @@ class ClockSampler:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
                  "-i", self.gpu_id], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            # wait for the first sample so that nvidia-smi's start-up does not
+            # overlap the timed region
+            t0 = time.time()
+            while time.time() - t0 < 20 and os.path.getsize(self.path) == 0 and self.proc.poll() is None:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
         return self
@@ -247,10 +252,9 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    w.step(args.warmup)
-    barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(gpu_uuid(local)) as clk:
+        w.step(args.warmup)
         barrier()
         e0.record(stream)
         w.step(args.steps)

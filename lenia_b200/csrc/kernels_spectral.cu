@@ -17,6 +17,7 @@
 // The same arrangement is written out on the CPU (oracle/restate) so results
 // can be compared bit for bit.
 #include "lenia_internal.h"
+#include "growth_common.cuh"
 
 namespace lenia {
 
@@ -99,21 +100,6 @@ __global__ void __launch_bounds__(kPlaneThreads) k_planes(Dims d, FftPlan py, Ff
 }
 
 // ------------------------------------------------- inverse rows: growth
-
-__device__ __forceinline__ float bell_dev(float x, float m, float s)
-{
-    const float qf = (x - m) / s;
-    const double q = (double)qf;
-    return (float)exp(-(q * q) / 2.0);
-}
-
-// Entry f of the reference's 256^3 growth table (lenia.cpp:93-101).
-__device__ float lut_flat_dev(long long f)
-{
-    if (f < 0 || f >= 256LL * 256 * 256) return 0.0f;
-    const int m = (int)(f >> 16), s = (int)((f >> 8) & 255), u = (int)(f & 255);
-    return bell_dev((float)u / 255, (float)m / 255, (float)s / 255);
-}
 
 // Builds the packed row spectrum of kernels (s0, s1) for one row tile.
 __device__ __forceinline__ void load_packed_rows(float2 *buf, const Dims &d, const float2 *s0, const float2 *s1,
@@ -199,28 +185,7 @@ __global__ void __launch_bounds__(kRowThreads) k_growth_rows(Dims d, FftPlan px,
             const float hv = hacc[c * T + e];
             Hout[o] = hv;
             Uout[o] = uacc[c * T + e];
-            if (jobs.growth_rt) {
-                // mt_fft_step early growth (lenia.cpp:542-592)
-                float v = A[o] + hv * jobs.timestep;
-                if (jobs.soft_clip[c]) {
-                    v = -4.0f * (v - 0.5f);
-                    const float a0 = 1.0f, a1 = 1.0f, a2 = 1.0f / 2, a3 = 1.0f / 2 / 3, a4 = 1.0f / 2 / 3 / 4,
-                                a5 = 1.0f / 2 / 3 / 4 / 5, a6 = 1.0f / 2 / 3 / 4 / 5 / 6,
-                                a7 = 1.0f / 2 / 3 / 4 / 5 / 6 / 7;
-                    float r = a7 * v + a6;
-                    r = r * v + a5;
-                    r = r * v + a4;
-                    r = r * v + a3;
-                    r = r * v + a2;
-                    r = r * v + a1;
-                    r = r * v + a0;
-                    v = 1.0f + r;
-                    v = 1.0f / v;
-                }
-                v = v > 0.0f ? v : 0.0f;
-                v = v < 1.0f ? v : 1.0f;
-                BACK[o] = v;
-            }
+            if (jobs.growth_rt) BACK[o] = early_growth(A[o], hv, jobs.timestep, jobs.soft_clip[c]);
         }
     }
     if (bad && err_flag) atomicOr(err_flag, 1);
@@ -410,6 +375,7 @@ static cudaError_t set_smem(const void *fn, size_t bytes)
 cudaError_t launch_fwd_rows(const Dims &d, const FftPlan &px, const float2 *tw_x, const FwdRowJobs &jobs,
                             cudaStream_t st)
 {
+    if (fast_supported(d)) return launch_fwd_rows_fast(d, tw_x, jobs, st);
     const int TY = row_tile(d, px);
     if (TY == 0) return cudaErrorInvalidValue;
     const size_t smem = (size_t)(d.W + TY * d.W) * sizeof(float2);
@@ -423,6 +389,7 @@ cudaError_t launch_fwd_rows(const Dims &d, const FftPlan &px, const float2 *tw_x
 cudaError_t launch_planes(const Dims &d, const FftPlan &py, const FftPlan &pz, const float2 *tw_y,
                           const float2 *tw_z, const PlaneJobs &jobs, int sign, cudaStream_t st)
 {
+    if (fast_supported(d)) return launch_planes_fast(d, tw_y, tw_z, jobs, sign, st);
     if (!plane_fits(d, py, pz)) return cudaErrorInvalidValue;
     const size_t smem = (size_t)(d.H + d.D + (long long)d.D * d.H) * sizeof(float2);
     cudaError_t e = set_smem((const void *)k_planes, smem);
@@ -436,6 +403,8 @@ cudaError_t launch_growth_rows(const Dims &d, const FftPlan &px, const float2 *t
                                const float *lut_rows, const float *A, float *H, float *U_SUM, float *BACK,
                                float *U_dbg, int *err_flag, cudaStream_t st)
 {
+    if (fast_supported(d))
+        return launch_growth_rows_fast(d, tw_x_inv, jobs, lut_rows, A, H, U_SUM, BACK, U_dbg, err_flag, st);
     int TY = row_tile(d, px);
     if (TY == 0) return cudaErrorInvalidValue;
     auto smem_for = [&](int ty) {
@@ -455,6 +424,7 @@ cudaError_t launch_growth_rows(const Dims &d, const FftPlan &px, const float2 *t
 cudaError_t launch_blur_rows(const Dims &d, const FftPlan &px, const float2 *tw_x_inv, const BlurJobs &jobs,
                              cudaStream_t st)
 {
+    if (fast_supported(d)) return launch_blur_rows_fast(d, tw_x_inv, jobs, st);
     const int TY = row_tile(d, px);
     if (TY == 0) return cudaErrorInvalidValue;
     const size_t smem = (size_t)(d.W + TY * d.W) * sizeof(float2);

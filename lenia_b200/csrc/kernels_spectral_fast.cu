@@ -1,0 +1,354 @@
+// Size-specialised spectral kernels for cubic grids (W = H = D in
+// {24, 32, 36, 44, 48, 64, 96, 128}): the same transforms and epilogues as
+// kernels_spectral.cu, with compile-time radix plans, padded conflict-free
+// shared memory and the growth accumulators held in registers.  Results are
+// bit-identical to the generic kernels (same float operations in the same
+// order); only the schedule differs.
+#include "lenia_internal.h"
+#include "lfft_static.cuh"
+#include "growth_common.cuh"
+
+namespace lenia {
+
+namespace {
+
+constexpr int kFastRowThreads = 256;
+constexpr int kFastPlaneThreads = 512;
+
+template <int W>
+struct RowShape {
+    static constexpr int TY = row_tile_for(W);
+    static constexpr int T = TY * W;                       // cells of a tile
+    static constexpr int NCELL = (T + kFastRowThreads - 1) / kFastRowThreads;
+    using PM = PadMat<W>;
+};
+
+template <int W>
+__global__ void __launch_bounds__(kFastRowThreads) k_fwd_rows_s(FwdRowJobs jobs, const float2 *__restrict__ tw_x)
+{
+    using S = RowShape<W>;
+    constexpr int H = W, D = W, TY = S::TY, KX = W / 2 + 1;
+    extern __shared__ float2 smem[];
+    float2 *tw = smem;
+    float2 *buf = smem + W;
+    const int z = blockIdx.x / (H / TY);
+    const int y0 = (blockIdx.x % (H / TY)) * TY;
+    const int pair = blockIdx.y;
+    const float *fa = jobs.in[2 * pair];
+    const float *fb = jobs.in[2 * pair + 1];
+    float2 *oa = jobs.out[2 * pair];
+    float2 *ob = jobs.out[2 * pair + 1];
+    for (int i = threadIdx.x; i < W; i += kFastRowThreads) tw[i] = tw_x[i];
+    const long long base = ((long long)z * H + y0) * W;
+    for (int e = threadIdx.x; e < TY * W; e += kFastRowThreads) {
+        const int ty = e / W, x = e % W;
+        const float a = __ldg(fa + base + e);
+        const float b = fb ? __ldg(fb + base + e) : 0.0f;
+        buf[S::PM::at(ty, x)] = make_float2(a, b);
+    }
+    __syncthreads();
+    static_fft<W, TY, false, W, kFastRowThreads>(buf, tw, -1);
+    for (int e = threadIdx.x; e < TY * KX; e += kFastRowThreads) {
+        const int ty = e % TY, kx = e / TY;
+        const float2 p = buf[S::PM::at(ty, kx)];
+        const float2 q = buf[S::PM::at(ty, (W - kx) % W)];
+        const long long o = ((long long)kx * D + z) * H + y0 + ty;
+        oa[o] = make_float2((p.x + q.x) * 0.5f, (p.y - q.y) * 0.5f);
+        if (ob) ob[o] = make_float2((p.y + q.y) * 0.5f, (q.x - p.x) * 0.5f);
+    }
+}
+
+template <int W>
+__global__ void __launch_bounds__(kFastPlaneThreads) k_planes_s(PlaneJobs jobs, const float2 *__restrict__ tw_y,
+                                                                const float2 *__restrict__ tw_z, int sign)
+{
+    constexpr int H = W, D = W;
+    using PM = PadMat<H>;
+    extern __shared__ float2 smem[];
+    float2 *twy = smem;
+    float2 *twz = smem + H;
+    float2 *buf = smem + H + D;
+    const int kx = blockIdx.x;
+    const int job = blockIdx.y;
+    const float4 *src = reinterpret_cast<const float4 *>(jobs.src[job] + (long long)kx * D * H);
+    float4 *dst = reinterpret_cast<float4 *>(jobs.dst[job] + (long long)kx * D * H);
+    const float *kc = jobs.kc[job];
+    for (int i = threadIdx.x; i < H; i += kFastPlaneThreads) twy[i] = tw_y[i];
+    for (int i = threadIdx.x; i < D; i += kFastPlaneThreads) twz[i] = tw_z[i];
+    constexpr int KZ = D / 2 + 1, KY = H / 2 + 1;
+    if (kc) {
+        const float *kp = kc + (long long)kx * KZ * KY;
+        for (int e = threadIdx.x; e < D * H / 2; e += kFastPlaneThreads) {
+            const int z = (2 * e) / H, y = (2 * e) % H;
+            const int oz = z <= D - z ? z : D - z;
+            const int oy0 = y <= H - y ? y : H - y;
+            const int oy1 = (y + 1) <= H - (y + 1) ? (y + 1) : H - (y + 1);
+            const float k0 = __ldg(kp + oz * KY + oy0);
+            const float k1 = __ldg(kp + oz * KY + oy1);
+            const float4 t = __ldg(src + e);
+            buf[PM::at(z, y)] = make_float2(t.x * k0, t.y * k0);
+            buf[PM::at(z, y + 1)] = make_float2(t.z * k1, t.w * k1);
+        }
+    } else {
+        for (int e = threadIdx.x; e < D * H / 2; e += kFastPlaneThreads) {
+            const int z = (2 * e) / H, y = (2 * e) % H;
+            const float4 t = __ldg(src + e);
+            buf[PM::at(z, y)] = make_float2(t.x, t.y);
+            buf[PM::at(z, y + 1)] = make_float2(t.z, t.w);
+        }
+    }
+    __syncthreads();
+    static_fft<H, D, false, H, kFastPlaneThreads>(buf, twy, sign);
+    static_fft<D, H, true, H, kFastPlaneThreads>(buf, twz, sign);
+    for (int e = threadIdx.x; e < D * H / 2; e += kFastPlaneThreads) {
+        const int z = (2 * e) / H, y = (2 * e) % H;
+        const float2 a = buf[PM::at(z, y)], b = buf[PM::at(z, y + 1)];
+        dst[e] = make_float4(a.x, a.y, b.x, b.y);
+    }
+}
+
+// Packed row spectrum of two kernels (or fields) for one tile: kx < W/2+1
+// from the stored half spectra, the rest by Hermitian symmetry.
+template <int W>
+__device__ __forceinline__ void load_packed_rows_s(float2 *buf, const float2 *s0, const float2 *s1, int z, int y0)
+{
+    using S = RowShape<W>;
+    constexpr int H = W, D = W, TY = S::TY, KX = W / 2 + 1;
+    for (int e = threadIdx.x; e < TY * W; e += kFastRowThreads) {
+        const int ty = e % TY, kx = e / TY;
+        const int m = kx < KX ? kx : W - kx;
+        const long long o = ((long long)m * D + z) * H + y0 + ty;
+        const float2 a = __ldg(s0 + o);
+        const float2 b = s1 ? __ldg(s1 + o) : make_float2(0.0f, 0.0f);
+        float2 r;
+        if (kx < KX) r = make_float2(a.x - b.y, a.y + b.x);
+        else r = make_float2(a.x + b.y, b.x - a.y);
+        buf[S::PM::at(ty, kx)] = r;
+    }
+}
+
+template <int W>
+__global__ void __launch_bounds__(kFastRowThreads) k_growth_rows_s(GrowthJobs jobs, const float2 *__restrict__ tw_x,
+                                                                   const float *__restrict__ lut_rows,
+                                                                   const float *__restrict__ A,
+                                                                   float *__restrict__ Hout, float *__restrict__ Uout,
+                                                                   float *__restrict__ BACK, float *__restrict__ Udbg,
+                                                                   int *err_flag)
+{
+    using S = RowShape<W>;
+    constexpr int H = W, TY = S::TY, T = S::T, NCELL = S::NCELL;
+    constexpr long long N = (long long)W * W * W;
+    extern __shared__ float2 smem[];
+    float2 *tw = smem;
+    float2 *buf = tw + W;
+    float *lut = reinterpret_cast<float *>(buf + S::PM::size(TY));
+    const int C = jobs.C, K = jobs.K;
+    const int z = blockIdx.x / (H / TY);
+    const int y0 = (blockIdx.x % (H / TY)) * TY;
+    const long long base = ((long long)z * H + y0) * W;
+    const float nf = (float)N;
+    for (int i = threadIdx.x; i < W; i += kFastRowThreads) tw[i] = tw_x[i];
+    for (int i = threadIdx.x; i < 256 * K; i += kFastRowThreads) lut[i] = lut_rows[i];
+
+    float hacc[NCELL][kMaxChannels], uacc[NCELL][kMaxChannels];
+#pragma unroll
+    for (int i = 0; i < NCELL; i++)
+#pragma unroll
+        for (int c = 0; c < kMaxChannels; c++) {
+            hacc[i][c] = 0.0f;
+            uacc[i][c] = 0.0f;
+        }
+    int bad = 0;
+    for (int k0 = 0; k0 < K; k0 += 2) {
+        const int k1 = k0 + 1 < K ? k0 + 1 : -1;
+        load_packed_rows_s<W>(buf, jobs.spec[k0], k1 >= 0 ? jobs.spec[k1] : nullptr, z, y0);
+        __syncthreads();
+        static_fft<W, TY, false, W, kFastRowThreads>(buf, tw, +1);
+#pragma unroll
+        for (int i = 0; i < NCELL; i++) {
+            const int e = threadIdx.x + i * kFastRowThreads;
+            if (T % kFastRowThreads != 0 && e >= T) continue;
+            const float2 zz = buf[S::PM::at(e / W, e % W)];
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const int k = q == 0 ? k0 : k1;
+                if (k < 0) continue;
+                const float u = (q == 0 ? zz.x : zz.y) / nf;
+                const int c1 = jobs.c1[k];
+                const float h = jobs.h[k];
+                const int ui = (int)(u * 255);
+                float l;
+                if (ui >= 0 && ui < 256) l = lut[k * 256 + ui];
+                else {
+                    if (!(u == u)) bad = 1;
+                    l = lut_flat_dev((long long)jobs.lut_base[k] + ui);
+                }
+#pragma unroll
+                for (int c = 0; c < kMaxChannels; c++) {
+                    if (c == c1) {
+                        uacc[i][c] = uacc[i][c] + u;
+                        const float g =
+                            jobs.asymptotic[c] ? (l - __ldg(A + (long long)c * N + base + e)) * h : l * h;
+                        hacc[i][c] = hacc[i][c] + g;
+                    }
+                }
+                if (Udbg) Udbg[(long long)k * N + base + e] = u;
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < NCELL; i++) {
+        const int e = threadIdx.x + i * kFastRowThreads;
+        if (T % kFastRowThreads != 0 && e >= T) continue;
+#pragma unroll
+        for (int c = 0; c < kMaxChannels; c++) {
+            if (c >= C) continue;
+            const long long o = (long long)c * N + base + e;
+            const float hv = hacc[i][c];
+            Hout[o] = hv;
+            Uout[o] = uacc[i][c];
+            if (jobs.growth_rt) BACK[o] = early_growth(__ldg(A + o), hv, jobs.timestep, jobs.soft_clip[c]);
+        }
+    }
+    if (bad && err_flag) atomicOr(err_flag, 1);
+}
+
+template <int W>
+__global__ void __launch_bounds__(kFastRowThreads) k_blur_rows_s(BlurJobs jobs, const float2 *__restrict__ tw_x)
+{
+    using S = RowShape<W>;
+    constexpr int H = W, TY = S::TY, T = S::T;
+    constexpr long long N = (long long)W * W * W;
+    extern __shared__ float2 smem[];
+    float2 *tw = smem;
+    float2 *buf = tw + W;
+    const int z = blockIdx.x / (H / TY);
+    const int y0 = (blockIdx.x % (H / TY)) * TY;
+    const int pair = blockIdx.y;
+    const long long base = ((long long)z * H + y0) * W;
+    const float nf = (float)N;
+    for (int i = threadIdx.x; i < W; i += kFastRowThreads) tw[i] = tw_x[i];
+    const int f0 = 2 * pair, f1 = 2 * pair + 1 < jobs.nfields ? 2 * pair + 1 : -1;
+    load_packed_rows_s<W>(buf, jobs.spec[f0], f1 >= 0 ? jobs.spec[f1] : nullptr, z, y0);
+    __syncthreads();
+    static_fft<W, TY, false, W, kFastRowThreads>(buf, tw, +1);
+    for (int e = threadIdx.x; e < T; e += kFastRowThreads) {
+        const float2 zz = buf[S::PM::at(e / W, e % W)];
+        jobs.out[f0][base + e] = zz.x / nf;
+        if (f1 >= 0) jobs.out[f1][base + e] = zz.y / nf;
+    }
+}
+
+cudaError_t smem_attr(const void *fn, size_t bytes)
+{
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <int W>
+cudaError_t fwd_rows_w(const Dims &d, const float2 *tw, const FwdRowJobs &jobs, cudaStream_t st)
+{
+    using S = RowShape<W>;
+    const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2);
+    cudaError_t e = smem_attr((const void *)k_fwd_rows_s<W>, smem);
+    if (e != cudaSuccess) return e;
+    k_fwd_rows_s<W><<<dim3(W * (W / S::TY), jobs.npairs), kFastRowThreads, smem, st>>>(jobs, tw);
+    return cudaGetLastError();
+}
+
+template <int W>
+cudaError_t planes_w(const Dims &d, const float2 *twy, const float2 *twz, const PlaneJobs &jobs, int sign,
+                     cudaStream_t st)
+{
+    const size_t smem = (size_t)(2 * W + PadMat<W>::size(W)) * sizeof(float2);
+    cudaError_t e = smem_attr((const void *)k_planes_s<W>, smem);
+    if (e != cudaSuccess) return e;
+    k_planes_s<W><<<dim3(W / 2 + 1, jobs.njobs), kFastPlaneThreads, smem, st>>>(jobs, twy, twz, sign);
+    return cudaGetLastError();
+}
+
+template <int W>
+cudaError_t growth_rows_w(const float2 *tw, const GrowthJobs &jobs, const float *lut, const float *A, float *H,
+                          float *U, float *BACK, float *Udbg, int *err, cudaStream_t st)
+{
+    using S = RowShape<W>;
+    const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2) + (size_t)256 * jobs.K * sizeof(float);
+    cudaError_t e = smem_attr((const void *)k_growth_rows_s<W>, smem);
+    if (e != cudaSuccess) return e;
+    k_growth_rows_s<W><<<W * (W / S::TY), kFastRowThreads, smem, st>>>(jobs, tw, lut, A, H, U, BACK, Udbg, err);
+    return cudaGetLastError();
+}
+
+template <int W>
+cudaError_t blur_rows_w(const float2 *tw, const BlurJobs &jobs, cudaStream_t st)
+{
+    using S = RowShape<W>;
+    const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2);
+    cudaError_t e = smem_attr((const void *)k_blur_rows_s<W>, smem);
+    if (e != cudaSuccess) return e;
+    k_blur_rows_s<W><<<dim3(W * (W / S::TY), (jobs.nfields + 1) / 2), kFastRowThreads, smem, st>>>(jobs, tw);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+#define LENIA_FAST_SIZES(X) X(24) X(32) X(36) X(44) X(48) X(64) X(96) X(128)
+
+bool fast_supported(const Dims &d)
+{
+    if (d.W != d.H) return false;
+    switch (d.W) {
+#define CASE(n) case n:
+        LENIA_FAST_SIZES(CASE)
+#undef CASE
+        return true;
+    default: return false;
+    }
+}
+
+cudaError_t launch_fwd_rows_fast(const Dims &d, const float2 *tw_x, const FwdRowJobs &jobs, cudaStream_t st)
+{
+    switch (d.W) {
+#define CASE(n) case n: return fwd_rows_w<n>(d, tw_x, jobs, st);
+        LENIA_FAST_SIZES(CASE)
+#undef CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_planes_fast(const Dims &d, const float2 *tw_y, const float2 *tw_z, const PlaneJobs &jobs, int sign,
+                               cudaStream_t st)
+{
+    switch (d.W) {
+#define CASE(n) case n: return planes_w<n>(d, tw_y, tw_z, jobs, sign, st);
+        LENIA_FAST_SIZES(CASE)
+#undef CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_growth_rows_fast(const Dims &d, const float2 *tw_x_inv, const GrowthJobs &jobs,
+                                    const float *lut_rows, const float *A, float *H, float *U_SUM, float *BACK,
+                                    float *U_dbg, int *err_flag, cudaStream_t st)
+{
+    switch (d.W) {
+#define CASE(n) \
+    case n: return growth_rows_w<n>(tw_x_inv, jobs, lut_rows, A, H, U_SUM, BACK, U_dbg, err_flag, st);
+        LENIA_FAST_SIZES(CASE)
+#undef CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_blur_rows_fast(const Dims &d, const float2 *tw_x_inv, const BlurJobs &jobs, cudaStream_t st)
+{
+    switch (d.W) {
+#define CASE(n) case n: return blur_rows_w<n>(tw_x_inv, jobs, st);
+        LENIA_FAST_SIZES(CASE)
+#undef CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace lenia

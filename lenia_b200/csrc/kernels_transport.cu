@@ -10,6 +10,7 @@
 //     gather reads the old one).
 // Float operation order and rounding are the reference's (-fmad=false).
 #include "lenia_internal.h"
+#include "growth_common.cuh"
 
 namespace lenia {
 
@@ -38,18 +39,92 @@ __device__ __forceinline__ float torus_wrap(float m, int ext)
     return m;
 }
 
-__device__ __forceinline__ float fastexp_dev(float x)
+// Oscillators (lenia.cpp:803-911) and transpose_to_row_major
+// (lenia.cpp:924-1037) for one destination cell; tt holds its reintegrated
+// mass per channel.
+__device__ __forceinline__ void transport_epilogue(const StepParams &p, const TransportBuffers &b, float *tt, int x,
+                                                   int y, int z, long long i)
 {
-    const float a0 = 1.0f, a1 = 1.0f, a2 = 1.0f / 2, a3 = 1.0f / 2 / 3, a4 = 1.0f / 2 / 3 / 4,
-                a5 = 1.0f / 2 / 3 / 4 / 5, a6 = 1.0f / 2 / 3 / 4 / 5 / 6, a7 = 1.0f / 2 / 3 / 4 / 5 / 6 / 7;
-    float r = a7 * x + a6;
-    r = r * x + a5;
-    r = r * x + a4;
-    r = r * x + a3;
-    r = r * x + a2;
-    r = r * x + a1;
-    r = r * x + a0;
-    return r;
+    const Dims &d = p.d;
+    const long long N = d.N;
+    const int C = p.C;
+    const int dd = p.dd;
+    if (p.osc_la || p.osc_flow || p.osc_div_flow) {
+        const float *fl = p.osc_vel ? b.V : b.F;
+#pragma unroll
+        for (int c = 0; c < kMaxChannels; c++) {
+            if (c >= C) continue;
+            const float *g = b.A + (long long)c * N;
+            const float fx1 = tb_read(g, d, dd, x + 1, y, z), fx0 = tb_read(g, d, dd, x - 1, y, z);
+            const float fy1 = tb_read(g, d, dd, x, y + 1, z), fy0 = tb_read(g, d, dd, x, y - 1, z);
+            const float fz1 = tb_read(g, d, dd, x, y, z + 1), fz0 = tb_read(g, d, dd, x, y, z - 1);
+            const float dxv = fx1 - fx0, dyv = fy1 - fy0, dzv = fz1 - fz0;
+            float t = tt[c];
+            if (p.osc_la) {
+                const float la = fx1 + fx0 + fy1 + fy0 + fz1 + fz0 - 6 * __ldg(g + i);
+                t = t + la * p.osc_la_amt;
+            }
+            if (p.osc_flow) {
+                const float flow = __ldg(fl + (long long)c * N + i) * dxv + __ldg(fl + (long long)(C + c) * N + i) * dyv +
+                                   __ldg(fl + (long long)(2 * C + c) * N + i) * dzv;
+                t = t + flow * p.osc_flow_amt;
+            }
+            if (p.osc_div_flow) {
+                const float *fxs = fl + (long long)c * N, *fys = fl + (long long)(C + c) * N,
+                            *fzs = fl + (long long)(2 * C + c) * N;
+                const float *al = b.ALPHA + (long long)c * N;
+                const float jx = tb_read(fxs, d, dd, x + 1, y, z) * tb_read(al, d, dd, x + 1, y, z) -
+                                 tb_read(fxs, d, dd, x - 1, y, z) * tb_read(al, d, dd, x - 1, y, z);
+                const float jy = tb_read(fys, d, dd, x, y + 1, z) * tb_read(al, d, dd, x, y + 1, z) -
+                                 tb_read(fys, d, dd, x, y - 1, z) * tb_read(al, d, dd, x, y - 1, z);
+                const float jz = tb_read(fzs, d, dd, x, y, z + 1) * tb_read(al, d, dd, x, y, z + 1) -
+                                 tb_read(fzs, d, dd, x, y, z - 1) * tb_read(al, d, dd, x, y, z - 1);
+                const float divj = jx + jy + jz;
+                t = t + divj * p.osc_div_flow_amt;
+            }
+            tt[c] = t;
+        }
+    }
+    if (b.TT)
+#pragma unroll
+        for (int c = 0; c < kMaxChannels; c++)
+            if (c < C) b.TT[(long long)c * N + i] = tt[c];
+
+    // transpose_to_row_major
+    if (p.growth_type == kGrowthTransposition) {
+#pragma unroll
+        for (int c = 0; c < kMaxChannels; c++) {
+            if (c >= C) continue;
+            const long long ci = (long long)c * N + i;
+            const float h = __ldg(b.H + ci);
+            if (p.soft_clip[c]) {
+                float v = __ldg(b.A + ci) + h * p.timestep;
+                v = -4.0f * (v - 0.5f);
+                v = fastexp_dev(v);
+                v = 1.0f + v;
+                v = 1.0f / v;
+                b.BACK[ci] = tmin(tmax(v, 0.0f), 1.0f);
+            } else {
+                tt[c] = tmin(tmax(tt[c] + h * p.timestep, 0.0f), 1.0f);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < kMaxChannels; c++)
+            if (c < C) tt[c] = tmin(tmax(tt[c], 0.0f), 1.0f);
+    }
+    const float stam = 1.0f - p.sta, stas = p.sta, gtas = p.gta, gtam = 1.0f - p.gta;
+    float ttsum = 0.0f;
+#pragma unroll
+    for (int c = 0; c < kMaxChannels; c++) {
+        if (c >= C) continue;
+        const long long ci = (long long)c * N + i;
+        ttsum = ttsum + tt[c];
+        b.GA[ci] = gtam * b.GA[ci] + tt[c] * gtas;
+        b.A_out[ci] = tt[c];
+    }
+    // SUM was cleared at the end of reintegration (lenia.cpp:912-915)
+    b.SUM[i] = stam * 0.0f + ttsum * stas;
 }
 
 __global__ void __launch_bounds__(256) k_transport(StepParams p, TransportBuffers b)
@@ -153,76 +228,161 @@ __global__ void __launch_bounds__(256) k_transport(StepParams p, TransportBuffer
         }
     }
 
-    if (p.osc_la || p.osc_flow || p.osc_div_flow) {
-        const float *fl = p.osc_vel ? b.V : b.F;
-        for (int c = 0; c < C; c++) {
-            const float *g = b.A + (long long)c * N;
-            const float fx1 = tb_read(g, d, dd, x + 1, y, z), fx0 = tb_read(g, d, dd, x - 1, y, z);
-            const float fy1 = tb_read(g, d, dd, x, y + 1, z), fy0 = tb_read(g, d, dd, x, y - 1, z);
-            const float fz1 = tb_read(g, d, dd, x, y, z + 1), fz0 = tb_read(g, d, dd, x, y, z - 1);
-            const float dxv = fx1 - fx0, dyv = fy1 - fy0, dzv = fz1 - fz0;
-            float t = tt[c];
-            if (p.osc_la) {
-                const float la = fx1 + fx0 + fy1 + fy0 + fz1 + fz0 - 6 * __ldg(g + i);
-                t = t + la * p.osc_la_amt;
-            }
-            if (p.osc_flow) {
-                const float flow = __ldg(fl + (long long)c * N + i) * dxv + __ldg(fl + (long long)(C + c) * N + i) * dyv +
-                                   __ldg(fl + (long long)(2 * C + c) * N + i) * dzv;
-                t = t + flow * p.osc_flow_amt;
-            }
-            if (p.osc_div_flow) {
-                const float *fxs = fl + (long long)c * N, *fys = fl + (long long)(C + c) * N,
-                            *fzs = fl + (long long)(2 * C + c) * N;
-                const float *al = b.ALPHA + (long long)c * N;
-                const float jx = tb_read(fxs, d, dd, x + 1, y, z) * tb_read(al, d, dd, x + 1, y, z) -
-                                 tb_read(fxs, d, dd, x - 1, y, z) * tb_read(al, d, dd, x - 1, y, z);
-                const float jy = tb_read(fys, d, dd, x, y + 1, z) * tb_read(al, d, dd, x, y + 1, z) -
-                                 tb_read(fys, d, dd, x, y - 1, z) * tb_read(al, d, dd, x, y - 1, z);
-                const float jz = tb_read(fzs, d, dd, x, y, z + 1) * tb_read(al, d, dd, x, y, z + 1) -
-                                 tb_read(fzs, d, dd, x, y, z - 1) * tb_read(al, d, dd, x, y, z - 1);
-                const float divj = jx + jy + jz;
-                t = t + divj * p.osc_div_flow_amt;
-            }
-            tt[c] = t;
-        }
-    }
-    if (b.TT)
-        for (int c = 0; c < C; c++) b.TT[(long long)c * N + i] = tt[c];
+    transport_epilogue(p, b, tt, x, y, z, i);
+}
 
-    // transpose_to_row_major
-    if (p.growth_type == kGrowthTransposition) {
-        for (int c = 0; c < C; c++) {
-            const long long ci = (long long)c * N + i;
-            const float h = __ldg(b.H + ci);
-            if (p.soft_clip[c]) {
-                float v = __ldg(b.A + ci) + h * p.timestep;
-                v = -4.0f * (v - 0.5f);
-                v = fastexp_dev(v);
-                v = 1.0f + v;
-                v = 1.0f / v;
-                b.BACK[ci] = tmin(tmax(v, 0.0f), 1.0f);
-            } else {
-                tt[c] = tmin(tmax(tt[c] + h * p.timestep, 0.0f), 1.0f);
+// ------------------------------------------------------------------
+// RT / SRT as a tiled destination gather.  A block owns 32 x 8 x TZ cells
+// (thread = one x, y column of TZ cells).  Per channel the block stages MU and
+// ARR of its cells plus a DD-cell halo (the reference's halo rules applied at
+// load time) in shared memory, then walks the source layers z' upward: the x
+// and y overlap factors of a source depend only on the thread's column, so
+// they are computed once and reused for the (up to 2 DD + 1) destinations of
+// the column that the source reaches.  Each destination still receives its
+// contributions in the reference's (dz, dy, dx) order, with the reference's
+// float operations, so the result is bit-identical.
+constexpr int kTX = 32, kTY = 8, kTZ = 8;
+
+__device__ __forceinline__ float overlap(float d, float si, float clip, bool torus, int ext)
+{
+    if (torus) d = torus_wrap(d, ext);
+    d = fabsf(d);
+    d = si - d;
+    d = tmax(d, 0.0f);
+    d = tmin(d, clip);
+    return d;
+}
+
+template <int DD>
+__global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, TransportBuffers b)
+{
+    constexpr int SX = kTX + 2 * DD, SY = kTY + 2 * DD, SZ = kTZ + 2 * DD, SV = SX * SY * SZ;
+    extern __shared__ float tiles[];
+    float *tmx = tiles, *tmy = tiles + SV, *tmz = tiles + 2 * SV, *tar = tiles + 3 * SV;
+    const Dims &d = p.d;
+    const long long N = d.N;
+    const int C = p.C;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int tiles_x = (d.W + kTX - 1) / kTX;
+    const int x0 = (blockIdx.x % tiles_x) * kTX;
+    const int y0 = (blockIdx.x / tiles_x) * kTY;
+    const int z0 = blockIdx.y * kTZ;
+    const int x = x0 + tx, y = y0 + ty;
+    const float px = (float)x + 0.5f, py = (float)y + 0.5f;
+    const bool torus = p.border == kBorderTorus;
+    const bool srt = p.mode_type == kModeSRT;
+    const int crt = p.rt_all_channels ? C : (C < 3 ? C : 3);
+    const int tid = tx + ty * kTX;
+
+    float tt[kMaxChannels][kTZ];
+#pragma unroll
+    for (int c = 0; c < kMaxChannels; c++)
+#pragma unroll
+        for (int j = 0; j < kTZ; j++) tt[c][j] = 0.0f;
+
+    for (int c = 0; c < crt; c++) {
+        const float *mux = b.MU + (long long)c * N;
+        const float *muy = b.MU + (long long)(C + c) * N;
+        const float *muz = b.MU + (long long)(2 * C + c) * N;
+        const float *arr = b.ARR + (long long)c * N;
+        __syncthreads();
+        for (int e = tid; e < SV; e += kTX * kTY) {
+            const int lx = e % SX, ly = (e / SX) % SY, lz = e / (SX * SY);
+            const int gx = x0 + lx - DD, gy = y0 + ly - DD, gz = z0 + lz - DD;
+            tmx[e] = tb_read(mux, d, p.dd, gx, gy, gz);
+            tmy[e] = tb_read(muy, d, p.dd, gx, gy, gz);
+            tmz[e] = tb_read(muz, d, p.dd, gx, gy, gz);
+            tar[e] = tb_read(arr, d, p.dd, gx, gy, gz);
+        }
+        __syncthreads();
+        float acc[kTZ];
+#pragma unroll
+        for (int j = 0; j < kTZ; j++) acc[j] = 0.0f;
+        if (srt) {
+#pragma unroll
+            for (int j = 0; j < kTZ; j++) {
+                const int e = (tx + DD) + (ty + DD) * SX + (j + DD) * SX * SY;
+                const float pz = (float)(z0 + j) + 0.5f;
+                float mx = fabsf(px - tmx[e]), my = fabsf(py - tmy[e]), mz = fabsf(pz - tmz[e]);
+                mx = tmin(tmax(p.si - mx, 0.0f), p.clip);
+                my = tmin(tmax(p.si - my, 0.0f), p.clip);
+                mz = tmin(tmax(p.si - mz, 0.0f), p.clip);
+                float w = tar[e] * mx;
+                w = w * my;
+                w = w * mz;
+                w = w * p.sn;
+                acc[j] = acc[j] + w;
+            }
+        } else {
+#pragma unroll
+            for (int lz = 0; lz < SZ; lz++) {          // source layer z' = z0 + lz - DD
+#pragma unroll
+                for (int oy = -DD; oy <= DD; oy++) {
+#pragma unroll
+                    for (int ox = -DD; ox <= DD; ox++) {
+                        const int e = (tx + DD + ox) + (ty + DD + oy) * SX + lz * SX * SY;
+                        const float mx = overlap(px - tmx[e], p.si, p.clip, torus, d.W);
+                        const float my = overlap(py - tmy[e], p.si, p.clip, torus, d.H);
+                        const float am = tar[e] * mx;
+                        const float amy = am * my;
+                        const float smz = tmz[e];
+#pragma unroll
+                        for (int oz = -DD; oz <= DD; oz++) {
+                            const int j = lz - DD - oz;  // destination whose offset to this source is oz
+                            if (j < 0 || j >= kTZ) continue;
+                            const float pz = (float)(z0 + j) + 0.5f;
+                            const float mz = overlap(pz - smz, p.si, p.clip, torus, d.D);
+                            float w = amy * mz;
+                            w = w * p.sn;
+                            acc[j] = acc[j] + w;
+                        }
+                    }
+                }
             }
         }
-    } else {
-        for (int c = 0; c < C; c++) tt[c] = tmin(tmax(tt[c], 0.0f), 1.0f);
+#pragma unroll
+        for (int cc = 0; cc < kMaxChannels; cc++)
+            if (cc == c)
+#pragma unroll
+                for (int j = 0; j < kTZ; j++) tt[cc][j] = acc[j];
     }
-    const float stam = 1.0f - p.sta, stas = p.sta, gtas = p.gta, gtam = 1.0f - p.gta;
-    float ttsum = 0.0f;
-    for (int c = 0; c < C; c++) {
-        const long long ci = (long long)c * N + i;
-        ttsum = ttsum + tt[c];
-        b.GA[ci] = gtam * b.GA[ci] + tt[c] * gtas;
-        b.A_out[ci] = tt[c];
+    if (x >= d.W || y >= d.H) return;
+
+    // oscillators and transpose_to_row_major, per destination cell
+#pragma unroll
+    for (int j = 0; j < kTZ; j++) {
+        const int z = z0 + j;
+        if (z >= d.D) continue;
+        const long long i = x + (long long)y * d.W + (long long)z * d.W * d.H;
+        float t4[kMaxChannels];
+#pragma unroll
+        for (int c = 0; c < kMaxChannels; c++) t4[c] = tt[c][j];
+        transport_epilogue(p, b, t4, x, y, z, i);
     }
-    // SUM was cleared at the end of reintegration (lenia.cpp:912-915)
-    b.SUM[i] = stam * 0.0f + ttsum * stas;
 }
 
 cudaError_t launch_transport(const StepParams &p, const TransportBuffers &b, cudaStream_t st)
 {
+    if ((p.mode_type == kModeRT || p.mode_type == kModeSRT) && p.dd >= 1 && p.dd <= 2) {
+        const int tiles_x = (p.d.W + kTX - 1) / kTX, tiles_y = (p.d.H + kTY - 1) / kTY;
+        dim3 grid(tiles_x * tiles_y, (p.d.D + kTZ - 1) / kTZ), block(kTX, kTY);
+        if (p.dd == 1) {
+            constexpr int SV = (kTX + 2) * (kTY + 2) * (kTZ + 2);
+            const size_t smem = 4 * SV * sizeof(float);
+            cudaError_t e = cudaFuncSetAttribute(k_transport_tiled<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+            k_transport_tiled<1><<<grid, block, smem, st>>>(p, b);
+        } else {
+            constexpr int SV = (kTX + 4) * (kTY + 4) * (kTZ + 4);
+            const size_t smem = 4 * SV * sizeof(float);
+            cudaError_t e = cudaFuncSetAttribute(k_transport_tiled<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+            k_transport_tiled<2><<<grid, block, smem, st>>>(p, b);
+        }
+        return cudaGetLastError();
+    }
     k_transport<<<(unsigned)((p.d.N + 255) / 256), 256, 0, st>>>(p, b);
     return cudaGetLastError();
 }

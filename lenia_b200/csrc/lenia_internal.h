@@ -129,6 +129,17 @@ cudaError_t launch_lut_rows(const LeniaKernelParams *kp_dev, int K, float *lut_r
 cudaError_t launch_flow(const StepParams &p, const FlowBuffers &b, cudaStream_t st);
 cudaError_t launch_transport(const StepParams &p, const TransportBuffers &b, cudaStream_t st);
 
+// Size-specialised spectral kernels (kernels_spectral_fast.cu) for cubic
+// grids of the sizes they are instantiated for.
+bool fast_supported(const Dims &d);
+cudaError_t launch_fwd_rows_fast(const Dims &d, const float2 *tw_x, const FwdRowJobs &jobs, cudaStream_t st);
+cudaError_t launch_planes_fast(const Dims &d, const float2 *tw_y, const float2 *tw_z, const PlaneJobs &jobs, int sign,
+                               cudaStream_t st);
+cudaError_t launch_growth_rows_fast(const Dims &d, const float2 *tw_x_inv, const GrowthJobs &jobs,
+                                    const float *lut_rows, const float *A, float *H, float *U_SUM, float *BACK,
+                                    float *U_dbg, int *err_flag, cudaStream_t st);
+cudaError_t launch_blur_rows_fast(const Dims &d, const float2 *tw_x_inv, const BlurJobs &jobs, cudaStream_t st);
+
 // Host FFT plans and twiddle tables (lenia_api.cu).
 int fft_factor(int n, int *radix);
 

@@ -96,6 +96,19 @@ def test_stages_bit_exact_mixed_radix(cuda_lib, oracle_built, width):
     assert not problems, "\n".join(problems[:12])
 
 
+@pytest.mark.parametrize("shape", [(32, 24), (24, 40)])
+def test_stages_bit_exact_non_cubic(cuda_lib, oracle_built, shape):
+    """Width != height runs the runtime-sized kernels (the size-specialised
+    ones cover cubic grids)."""
+    w, h = shape
+    wl = variant("sobel_torus", seed=w + h, width=w)
+    wl.desc.height = h
+    rng = np.random.default_rng(w * h)
+    wl.A0 = P.seed_cube(rng, wl.desc, min(w, h) // 2)
+    problems = run_staged(wl, steps=1)
+    assert not problems, "\n".join(problems[:12])
+
+
 def test_trajectory_bit_exact_cfg0(cuda_lib, oracle_built):
     """Whole steps (the production path, no debug outputs) stay bit-exact over
     100 steps of the 32^3 plain-step configuration."""
