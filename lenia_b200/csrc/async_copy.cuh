@@ -1,0 +1,23 @@
+// Asynchronous global -> shared copies (cp.async, sm_80+ and sm_100a).  A copy
+// with `valid` false writes zero, which is how halo cells that the reference
+// never writes (edges and corners) are filled.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace lenia {
+
+__device__ __forceinline__ void cp_async_f32(float *smem_dst, const float *gmem_src, bool valid)
+{
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    const int n = valid ? 4 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(gmem_src), "r"(n) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+}  // namespace lenia

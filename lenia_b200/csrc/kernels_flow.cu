@@ -14,6 +14,7 @@
 // is compiled with -fmad=false), so outputs match the CPU restatement bit for
 // bit given the same inputs.
 #include "lenia_internal.h"
+#include "async_copy.cuh"
 
 namespace lenia {
 
@@ -23,13 +24,14 @@ constexpr int kSX = kFX + 2, kSY = kFY + 2, kSZ = kFZ + 2;
 __device__ __forceinline__ float smax(float a, float b) { return a > b ? a : b; }
 __device__ __forceinline__ float smin(float a, float b) { return a < b ? a : b; }
 
-// Value of a gradient input at (x, y, z), the reference's halo rules.
-__device__ __forceinline__ float gb_read(const float *f, const Dims &d, int x, int y, int z, int border)
+// Source of tile cell (x, y, z) under the gradient halo rules; false when
+// the cell reads 0 (edges, corners, zero faces).
+__device__ __forceinline__ bool gb_source(const Dims &d, int border, int &x, int &y, int &z)
 {
     const int ox = (x < 0) | (x >= d.W), oy = (y < 0) | (y >= d.H), oz = (z < 0) | (z >= d.D);
     const int no = ox + oy + oz;
-    if (no == 0) return __ldg(f + x + (long long)y * d.W + (long long)z * d.W * d.H);
-    if (no > 1 || border == kBorderNone) return 0.0f;
+    if (no == 0) return true;
+    if (no > 1 || border == kBorderNone) return false;
     if (border == kBorderTorus) {
         x = x < 0 ? x + d.W : (x >= d.W ? x - d.W : x);
         y = y < 0 ? y + d.H : (y >= d.H ? y - d.H : y);
@@ -39,24 +41,41 @@ __device__ __forceinline__ float gb_read(const float *f, const Dims &d, int x, i
         y = y < 0 ? 0 : (y >= d.H ? d.H - 1 : y);
         z = z < 0 ? 0 : (z >= d.D ? d.D - 1 : z);
     }
-    return __ldg(f + x + (long long)y * d.W + (long long)z * d.W * d.H);
+    return true;
 }
 
-__device__ __forceinline__ void load_tile(float *tile, const float *f, const Dims &d, int x0, int y0, int z0,
-                                          int border)
+// Queues the asynchronous copy of one field's tile (with its one-cell halo).
+__device__ __forceinline__ void issue_tile(float *tile, const float *f, const Dims &d, int x0, int y0, int z0,
+                                           int border)
 {
     const int tid = threadIdx.x + threadIdx.y * kFX;
     for (int e = tid; e < kSX * kSY * kSZ; e += kFX * kFY) {
         const int lx = e % kSX, ly = (e / kSX) % kSY, lz = e / (kSX * kSY);
-        tile[e] = gb_read(f, d, x0 + lx - 1, y0 + ly - 1, z0 + lz - 1, border);
+        int x = x0 + lx - 1, y = y0 + ly - 1, z = z0 + lz - 1;
+        const bool ok = gb_source(d, border, x, y, z);
+        const float *src = ok ? f + x + (long long)y * d.W + (long long)z * d.W * d.H : f;
+        cp_async_f32(tile + e, src, ok);
     }
+    cp_async_commit();
+}
+
+// True when any value of the tile is infinite or NaN (block-wide).
+__device__ __forceinline__ bool tile_nonfinite(const float *tile)
+{
+    const int tid = threadIdx.x + threadIdx.y * kFX;
+    int bad = 0;
+    for (int e = tid; e < kSX * kSY * kSZ; e += kFX * kFY) bad |= !isfinite(tile[e]);
+    return __syncthreads_or(bad) != 0;
 }
 
 __device__ __forceinline__ float sob_w(int dd) { return dd == 0 ? 2.0f : 1.0f; }
 
-// Gradient at tile position (lx, ly, lz) (interior coordinates).
-__device__ __forceinline__ void gradient(const float *tile, int lx, int ly, int lz, int sobel, float &gx, float &gy,
-                                         float &gz)
+// Gradient at tile position (lx, ly, lz) (interior coordinates).  With
+// `all_taps` false the zero-coefficient taps of the Sobel tables are skipped:
+// for finite inputs adding v*0 leaves the running sum unchanged (the sum
+// starts at +0 and can never become -0), so the result is identical.
+__device__ __forceinline__ void gradient(const float *tile, int lx, int ly, int lz, int sobel, bool all_taps,
+                                         float &gx, float &gy, float &gz)
 {
     if (sobel) {
         float ax = 0.0f, ay = 0.0f, az = 0.0f;
@@ -67,9 +86,9 @@ __device__ __forceinline__ void gradient(const float *tile, int lx, int ly, int 
 #pragma unroll
                 for (int dx = -1; dx <= 1; dx++) {
                     const float v = tile[(lx + 1 + dx) + (ly + 1 + dy) * kSX + (lz + 1 + dz) * kSX * kSY];
-                    ax = ax + v * (sob_w(dx) * sob_w(dy) * (float)dz);
-                    ay = ay + v * ((float)dx * sob_w(dy) * sob_w(dz));
-                    az = az + v * (sob_w(dx) * (float)dy * sob_w(dz));
+                    if (all_taps || dz != 0) ax = ax + v * (sob_w(dx) * sob_w(dy) * (float)dz);
+                    if (all_taps || dx != 0) ay = ay + v * ((float)dx * sob_w(dy) * sob_w(dz));
+                    if (all_taps || dy != 0) az = az + v * (sob_w(dx) * (float)dy * sob_w(dz));
                 }
         gx = ax;
         gy = ay;
@@ -84,7 +103,7 @@ __device__ __forceinline__ void gradient(const float *tile, int lx, int ly, int 
 
 __global__ void __launch_bounds__(kFX *kFY) k_flow(StepParams p, FlowBuffers b)
 {
-    __shared__ float tile[kSX * kSY * kSZ];
+    __shared__ float tiles[2][kSX * kSY * kSZ];
     const Dims &d = p.d;
     const int C = p.C;
     const long long N = d.N;
@@ -96,107 +115,127 @@ __global__ void __launch_bounds__(kFX *kFY) k_flow(StepParams p, FlowBuffers b)
     const int x = x0 + tx, y = y0 + ty;
     const bool col_in = x < d.W && y < d.H;
     const int sobel = p.gradient_mode == kGradSobel;
+    const float ta = p.theta_a;
 
     float na[kFZ][3];
-    load_tile(tile, b.SUM, d, x0, y0, z0, p.sobel_border);
-    __syncthreads();
+    // field 0 is SUM, field 1 + c is H channel c; field f+1 loads while f computes
+    issue_tile(tiles[0], b.SUM, d, x0, y0, z0, p.sobel_border);
+    for (int f = 0; f <= C; f++) {
+        float *tile = tiles[f & 1];
+        if (f < C) issue_tile(tiles[(f + 1) & 1], b.H + (long long)f * N, d, x0, y0, z0, p.sobel_border);
+        // per-cell inputs of this channel, loaded while the tile lands
+        float v3[3][kFZ], gal[kFZ];
+        unsigned gvalid = 0;  // bit lz: the alpha source of cell lz was written
+        const int c = f - 1;
+        if (f > 0 && col_in) {
 #pragma unroll
-    for (int lz = 0; lz < kFZ; lz++) gradient(tile, tx, ty, lz, sobel, na[lz][0], na[lz][1], na[lz][2]);
-    if (b.NA && col_in) {
+            for (int lz = 0; lz < kFZ; lz++) {
+                const int z = z0 + lz;
+                if (z >= d.D) continue;
+                const long long i = x + (long long)y * d.W + (long long)z * d.W * d.H;
+                const long long ci = (long long)c * N + i;
 #pragma unroll
-        for (int lz = 0; lz < kFZ; lz++) {
-            const int z = z0 + lz;
-            if (z >= d.D) continue;
-            const long long i = x + (long long)y * d.W + (long long)z * d.W * d.H;
-            b.NA[i] = na[lz][0];
-            b.NA[N + i] = na[lz][1];
-            b.NA[2 * N + i] = na[lz][2];
-        }
-    }
-    const float ta = p.theta_a;
-    for (int c = 0; c < C; c++) {
-        __syncthreads();
-        load_tile(tile, b.H + (long long)c * N, d, x0, y0, z0, p.sobel_border);
-        __syncthreads();
-        if (!col_in) continue;
-#pragma unroll
-        for (int lz = 0; lz < kFZ; lz++) {
-            const int z = z0 + lz;
-            if (z >= d.D) continue;
-            const long long i = x + (long long)y * d.W + (long long)z * d.W * d.H;
-            const long long ci = (long long)c * N + i;
-            float nu[3];
-            gradient(tile, tx, ty, lz, sobel, nu[0], nu[1], nu[2]);
-            // alpha: PREALPHA as compute_f reads it (flat index c*N + i), which
-            // sobel_convolve_h wrote from channel f / P, cell f % P (Q20).
-            float alpha;
-            {
+                for (int q = 0; q < 3; q++) v3[q][lz] = b.V[(long long)q * C * N + ci];
+                // alpha source: PREALPHA as compute_f reads it (flat c*N + i),
+                // written by sobel_convolve_h from channel f / P, cell f % P (Q20)
                 long long src_c = c, src_i = i;
                 bool valid = true;
                 if (!p.alpha_index_fix) {
-                    const long long f = ci;
-                    src_c = f / d.P;
-                    src_i = f - src_c * d.P;
+                    src_c = ci / d.P;
+                    src_i = ci - src_c * d.P;
                     valid = src_c < C && src_i < N;
                 }
-                if (valid) {
-                    const float g = __ldg(b.A + src_c * N + src_i);
-                    float pg = g / ta;
-                    pg = pg * pg;
-                    alpha = smin(smax(pg, 0.0f), 1.0f);
-                } else {
-                    alpha = 0.0f;
-                }
+                gal[lz] = valid ? __ldg(b.A + src_c * N + src_i) : 0.0f;
+                gvalid |= (valid ? 1u : 0u) << lz;
             }
-            if (b.PREALPHA) b.PREALPHA[ci] = alpha;
-            if (b.NU) {
-                b.NU[ci] = nu[0];
-                b.NU[(long long)C * N + ci] = nu[1];
-                b.NU[2LL * C * N + ci] = nu[2];
-            }
-            if (b.ALPHA) {
-                // ALPHA = |GRID - GA| with GA read at c*P + i (Q20)
-                // (GA blocks past the last channel are never written: 0)
-                const float g = __ldg(b.A + ci);
-                const long long f = p.alpha_index_fix ? ci : (long long)c * d.P + i;
-                const float ga = f < (long long)C * N ? __ldg(b.GA + f) : 0.0f;
-                b.ALPHA[ci] = fabsf(g - ga);
-            }
-            const float a1 = 1.0f - alpha;
-            float f3[3];
-#pragma unroll
-            for (int q = 0; q < 3; q++) f3[q] = nu[q] * a1 - na[lz][q] * alpha;
-            if (b.F) {
-#pragma unroll
-                for (int q = 0; q < 3; q++) b.F[(long long)q * C * N + ci] = f3[q];
-            }
-            float v3[3];
-#pragma unroll
-            for (int q = 0; q < 3; q++) v3[q] = b.V[(long long)q * C * N + ci];
-            const float pos[3] = {(float)x + 0.5f, (float)y + 0.5f, (float)z + 0.5f};
-            if (p.mu_vel) {
-#pragma unroll
-                for (int q = 0; q < 3; q++) v3[q] = (v3[q] + f3[q]) * p.v_damp;
-            }
-#pragma unroll
-            for (int q = 0; q < 3; q++) {
-                float m = (p.mu_vel ? v3[q] : f3[q]) * p.timestep;
-                m = smax(m, -p.ma);
-                m = smin(m, p.ma);
-                m = pos[q] + m;
-                if (p.border == kBorderWall) {
-                    m = smax(m, p.sigma);
-                    m = smin(m, q == 1 ? p.ghs : p.gws);
-                }
-                b.MU[(long long)q * C * N + ci] = m;
-            }
-            if (!p.mu_vel) {
-#pragma unroll
-                for (int q = 0; q < 3; q++) v3[q] = (v3[q] + f3[q]) * p.v_damp;
-            }
-#pragma unroll
-            for (int q = 0; q < 3; q++) b.V[(long long)q * C * N + ci] = v3[q];
         }
+        if (f < C) cp_async_wait<1>();
+        else cp_async_wait<0>();
+        __syncthreads();
+        const bool all_taps = sobel && tile_nonfinite(tile);
+        if (f == 0) {
+#pragma unroll
+            for (int lz = 0; lz < kFZ; lz++) gradient(tile, tx, ty, lz, sobel, all_taps, na[lz][0], na[lz][1], na[lz][2]);
+            if (b.NA && col_in) {
+#pragma unroll
+                for (int lz = 0; lz < kFZ; lz++) {
+                    const int z = z0 + lz;
+                    if (z >= d.D) continue;
+                    const long long i = x + (long long)y * d.W + (long long)z * d.W * d.H;
+                    b.NA[i] = na[lz][0];
+                    b.NA[N + i] = na[lz][1];
+                    b.NA[2 * N + i] = na[lz][2];
+                }
+            }
+        } else if (col_in) {
+#pragma unroll
+            for (int lz = 0; lz < kFZ; lz++) {
+                const int z = z0 + lz;
+                if (z >= d.D) continue;
+                const long long i = x + (long long)y * d.W + (long long)z * d.W * d.H;
+                const long long ci = (long long)c * N + i;
+                float nu[3];
+                gradient(tile, tx, ty, lz, sobel, all_taps, nu[0], nu[1], nu[2]);
+                float alpha;
+                {
+                    const float g = gal[lz];
+                    if (!((gvalid >> lz) & 1u)) {
+                        alpha = 0.0f;
+                    } else {
+                        float pg = g / ta;
+                        pg = pg * pg;
+                        alpha = smin(smax(pg, 0.0f), 1.0f);
+                    }
+                }
+                if (b.PREALPHA) b.PREALPHA[ci] = alpha;
+                if (b.NU) {
+                    b.NU[ci] = nu[0];
+                    b.NU[(long long)C * N + ci] = nu[1];
+                    b.NU[2LL * C * N + ci] = nu[2];
+                }
+                if (b.ALPHA) {
+                    // ALPHA = |GRID - GA| with GA read at c*P + i (Q20)
+                    // (GA blocks past the last channel are never written: 0)
+                    const float g = __ldg(b.A + ci);
+                    const long long fi = p.alpha_index_fix ? ci : (long long)c * d.P + i;
+                    const float ga = fi < (long long)C * N ? __ldg(b.GA + fi) : 0.0f;
+                    b.ALPHA[ci] = fabsf(g - ga);
+                }
+                const float a1 = 1.0f - alpha;
+                float f3[3];
+#pragma unroll
+                for (int q = 0; q < 3; q++) f3[q] = nu[q] * a1 - na[lz][q] * alpha;
+                if (b.F) {
+#pragma unroll
+                    for (int q = 0; q < 3; q++) b.F[(long long)q * C * N + ci] = f3[q];
+                }
+                float vv[3] = {v3[0][lz], v3[1][lz], v3[2][lz]};
+                const float pos[3] = {(float)x + 0.5f, (float)y + 0.5f, (float)z + 0.5f};
+                if (p.mu_vel) {
+#pragma unroll
+                    for (int q = 0; q < 3; q++) vv[q] = (vv[q] + f3[q]) * p.v_damp;
+                }
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    float m = (p.mu_vel ? vv[q] : f3[q]) * p.timestep;
+                    m = smax(m, -p.ma);
+                    m = smin(m, p.ma);
+                    m = pos[q] + m;
+                    if (p.border == kBorderWall) {
+                        m = smax(m, p.sigma);
+                        m = smin(m, q == 1 ? p.ghs : p.gws);
+                    }
+                    b.MU[(long long)q * C * N + ci] = m;
+                }
+                if (!p.mu_vel) {
+#pragma unroll
+                    for (int q = 0; q < 3; q++) vv[q] = (vv[q] + f3[q]) * p.v_damp;
+                }
+#pragma unroll
+                for (int q = 0; q < 3; q++) b.V[(long long)q * C * N + ci] = vv[q];
+            }
+        }
+        __syncthreads();
     }
 }
 

@@ -15,11 +15,20 @@ namespace {
 constexpr int kFastRowThreads = 256;
 constexpr int kFastPlaneThreads = 512;
 
-template <int W>
+// Rows per tile of the growth pass: at most 8 (the accumulators live in
+// registers, so smaller tiles keep more blocks resident).
+constexpr int growth_tile_for(int n)
+{
+    for (int t = 8; t > 1; t--)
+        if (n % t == 0) return t;
+    return 1;
+}
+
+template <int W, bool GROWTH = false>
 struct RowShape {
-    static constexpr int TY = row_tile_for(W);
+    static constexpr int TY = GROWTH ? growth_tile_for(W) : row_tile_for(W);
     static constexpr int T = TY * W;                       // cells of a tile
-    static constexpr int NCELL = (T + kFastRowThreads - 1) / kFastRowThreads;
+    static constexpr int NCELL = (T + kFastRowThreads - 1) / kFastRowThreads;  // cells per thread
     using PM = PadMat<W>;
 };
 
@@ -135,8 +144,8 @@ __global__ void __launch_bounds__(kFastRowThreads) k_growth_rows_s(GrowthJobs jo
                                                                    float *__restrict__ BACK, float *__restrict__ Udbg,
                                                                    int *err_flag)
 {
-    using S = RowShape<W>;
-    constexpr int H = W, TY = S::TY, T = S::T, NCELL = S::NCELL;
+    using S = RowShape<W, true>;
+    constexpr int H = W, D = W, TY = S::TY, T = S::T, NCELL = S::NCELL, KX = W / 2 + 1;
     constexpr long long N = (long long)W * W * W;
     extern __shared__ float2 smem[];
     float2 *tw = smem;
@@ -150,6 +159,25 @@ __global__ void __launch_bounds__(kFastRowThreads) k_growth_rows_s(GrowthJobs jo
     for (int i = threadIdx.x; i < W; i += kFastRowThreads) tw[i] = tw_x[i];
     for (int i = threadIdx.x; i < 256 * K; i += kFastRowThreads) lut[i] = lut_rows[i];
 
+    // The packed row spectrum of a kernel pair: element e of the tile is
+    // (ty = e % TY, kx = e / TY); its half-spectrum values are prefetched into
+    // registers one pair ahead so the loads overlap the current transform.
+    float2 pa[NCELL], pb[NCELL];
+    auto prefetch = [&](int k0) {
+        const float2 *s0 = jobs.spec[k0];
+        const float2 *s1 = k0 + 1 < K ? jobs.spec[k0 + 1] : nullptr;
+#pragma unroll
+        for (int i = 0; i < NCELL; i++) {
+            const int e = threadIdx.x + i * kFastRowThreads;
+            if (T % kFastRowThreads != 0 && e >= T) continue;
+            const int ty = e % TY, kx = e / TY;
+            const int m = kx < KX ? kx : W - kx;
+            const long long o = ((long long)m * D + z) * H + y0 + ty;
+            pa[i] = __ldg(s0 + o);
+            pb[i] = s1 ? __ldg(s1 + o) : make_float2(0.0f, 0.0f);
+        }
+    };
+
     float hacc[NCELL][kMaxChannels], uacc[NCELL][kMaxChannels];
 #pragma unroll
     for (int i = 0; i < NCELL; i++)
@@ -159,10 +187,22 @@ __global__ void __launch_bounds__(kFastRowThreads) k_growth_rows_s(GrowthJobs jo
             uacc[i][c] = 0.0f;
         }
     int bad = 0;
+    if (K > 0) prefetch(0);
     for (int k0 = 0; k0 < K; k0 += 2) {
         const int k1 = k0 + 1 < K ? k0 + 1 : -1;
-        load_packed_rows_s<W>(buf, jobs.spec[k0], k1 >= 0 ? jobs.spec[k1] : nullptr, z, y0);
+#pragma unroll
+        for (int i = 0; i < NCELL; i++) {
+            const int e = threadIdx.x + i * kFastRowThreads;
+            if (T % kFastRowThreads != 0 && e >= T) continue;
+            const int ty = e % TY, kx = e / TY;
+            const float2 a = pa[i], b = pb[i];
+            float2 r;
+            if (kx < KX) r = make_float2(a.x - b.y, a.y + b.x);
+            else r = make_float2(a.x + b.y, b.x - a.y);
+            buf[S::PM::at(ty, kx)] = r;
+        }
         __syncthreads();
+        if (k0 + 2 < K) prefetch(k0 + 2);
         static_fft<W, TY, false, W, kFastRowThreads>(buf, tw, +1);
 #pragma unroll
         for (int i = 0; i < NCELL; i++) {
@@ -272,7 +312,7 @@ template <int W>
 cudaError_t growth_rows_w(const float2 *tw, const GrowthJobs &jobs, const float *lut, const float *A, float *H,
                           float *U, float *BACK, float *Udbg, int *err, cudaStream_t st)
 {
-    using S = RowShape<W>;
+    using S = RowShape<W, true>;
     const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2) + (size_t)256 * jobs.K * sizeof(float);
     cudaError_t e = smem_attr((const void *)k_growth_rows_s<W>, smem);
     if (e != cudaSuccess) return e;

@@ -11,6 +11,7 @@
 // Float operation order and rounding are the reference's (-fmad=false).
 #include "lenia_internal.h"
 #include "growth_common.cuh"
+#include "async_copy.cuh"
 
 namespace lenia {
 
@@ -253,12 +254,26 @@ __device__ __forceinline__ float overlap(float d, float si, float clip, bool tor
     return d;
 }
 
+// Source of a halo cell under the transported-field rules; false when the
+// cell reads 0 (edges, corners, layers past dd).
+__device__ __forceinline__ bool tb_source(const Dims &d, int dd, int &x, int &y, int &z)
+{
+    const int ox = (x < 0) | (x >= d.W), oy = (y < 0) | (y >= d.H), oz = (z < 0) | (z >= d.D);
+    const int no = ox + oy + oz;
+    if (no == 0) return true;
+    if (no > 1) return false;
+    if (x < -dd || x >= d.W + dd || y < -dd || y >= d.H + dd || z < -dd || z >= d.D + dd) return false;
+    x = x < 0 ? x + d.W : (x >= d.W ? x - d.W : x);
+    y = y < 0 ? y + d.H : (y >= d.H ? y - d.H : y);
+    z = z < 0 ? z + d.D : (z >= d.D ? z - d.D : z);
+    return true;
+}
+
 template <int DD>
 __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, TransportBuffers b)
 {
     constexpr int SX = kTX + 2 * DD, SY = kTY + 2 * DD, SZ = kTZ + 2 * DD, SV = SX * SY * SZ;
-    extern __shared__ float tiles[];
-    float *tmx = tiles, *tmy = tiles + SV, *tmz = tiles + 2 * SV, *tar = tiles + 3 * SV;
+    extern __shared__ float tiles[];  // [2 buffers][MU_x, MU_y, MU_z, ARR][SV]
     const Dims &d = p.d;
     const long long N = d.N;
     const int C = p.C;
@@ -274,27 +289,42 @@ __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, Tran
     const int crt = p.rt_all_channels ? C : (C < 3 ? C : 3);
     const int tid = tx + ty * kTX;
 
+    // queues channel c's MU and ARR tiles (cells plus a DD halo) into buffer c & 1
+    auto issue = [&](int c) {
+        float *buf = tiles + (c & 1) * 4 * SV;
+        const float *mux = b.MU + (long long)c * N;
+        const float *muy = b.MU + (long long)(C + c) * N;
+        const float *muz = b.MU + (long long)(2 * C + c) * N;
+        const float *arr = b.ARR + (long long)c * N;
+        for (int e = tid; e < SV; e += kTX * kTY) {
+            const int lx = e % SX, ly = (e / SX) % SY, lz = e / (SX * SY);
+            int gx = x0 + lx - DD, gy = y0 + ly - DD, gz = z0 + lz - DD;
+            const bool ok = tb_source(d, p.dd, gx, gy, gz);
+            const long long o = ok ? gx + (long long)gy * d.W + (long long)gz * d.W * d.H : 0;
+            cp_async_f32(buf + e, mux + o, ok);
+            cp_async_f32(buf + SV + e, muy + o, ok);
+            cp_async_f32(buf + 2 * SV + e, muz + o, ok);
+            cp_async_f32(buf + 3 * SV + e, arr + o, ok);
+        }
+        cp_async_commit();
+    };
+
     float tt[kMaxChannels][kTZ];
 #pragma unroll
     for (int c = 0; c < kMaxChannels; c++)
 #pragma unroll
         for (int j = 0; j < kTZ; j++) tt[c][j] = 0.0f;
 
+    if (crt > 0) issue(0);
     for (int c = 0; c < crt; c++) {
-        const float *mux = b.MU + (long long)c * N;
-        const float *muy = b.MU + (long long)(C + c) * N;
-        const float *muz = b.MU + (long long)(2 * C + c) * N;
-        const float *arr = b.ARR + (long long)c * N;
-        __syncthreads();
-        for (int e = tid; e < SV; e += kTX * kTY) {
-            const int lx = e % SX, ly = (e / SX) % SY, lz = e / (SX * SY);
-            const int gx = x0 + lx - DD, gy = y0 + ly - DD, gz = z0 + lz - DD;
-            tmx[e] = tb_read(mux, d, p.dd, gx, gy, gz);
-            tmy[e] = tb_read(muy, d, p.dd, gx, gy, gz);
-            tmz[e] = tb_read(muz, d, p.dd, gx, gy, gz);
-            tar[e] = tb_read(arr, d, p.dd, gx, gy, gz);
+        if (c + 1 < crt) {
+            issue(c + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
+        const float *tmx = tiles + (c & 1) * 4 * SV, *tmy = tmx + SV, *tmz = tmx + 2 * SV, *tar = tmx + 3 * SV;
         float acc[kTZ];
 #pragma unroll
         for (int j = 0; j < kTZ; j++) acc[j] = 0.0f;
@@ -345,6 +375,7 @@ __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, Tran
             if (cc == c)
 #pragma unroll
                 for (int j = 0; j < kTZ; j++) tt[cc][j] = acc[j];
+        __syncthreads();  // buffer c & 1 is refilled by issue(c + 2)
     }
     if (x >= d.W || y >= d.H) return;
 
@@ -368,14 +399,14 @@ cudaError_t launch_transport(const StepParams &p, const TransportBuffers &b, cud
         dim3 grid(tiles_x * tiles_y, (p.d.D + kTZ - 1) / kTZ), block(kTX, kTY);
         if (p.dd == 1) {
             constexpr int SV = (kTX + 2) * (kTY + 2) * (kTZ + 2);
-            const size_t smem = 4 * SV * sizeof(float);
+            const size_t smem = 2 * 4 * SV * sizeof(float);
             cudaError_t e = cudaFuncSetAttribute(k_transport_tiled<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)smem);
             if (e != cudaSuccess) return e;
             k_transport_tiled<1><<<grid, block, smem, st>>>(p, b);
         } else {
             constexpr int SV = (kTX + 4) * (kTY + 4) * (kTZ + 4);
-            const size_t smem = 4 * SV * sizeof(float);
+            const size_t smem = 2 * 4 * SV * sizeof(float);
             cudaError_t e = cudaFuncSetAttribute(k_transport_tiled<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)smem);
             if (e != cudaSuccess) return e;
