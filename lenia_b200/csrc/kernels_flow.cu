@@ -18,7 +18,7 @@
 
 namespace lenia {
 
-constexpr int kFX = 32, kFY = 8, kFZ = 8;  // output tile
+constexpr int kFX = 32, kFY = 8, kFZ = 4;  // output tile
 constexpr int kSX = kFX + 2, kSY = kFY + 2, kSZ = kFZ + 2;
 
 __device__ __forceinline__ float smax(float a, float b) { return a > b ? a : b; }
@@ -59,22 +59,26 @@ __device__ __forceinline__ void issue_tile(float *tile, const float *f, const Di
     cp_async_commit();
 }
 
-// True when any value of the tile is infinite or NaN (block-wide).
-__device__ __forceinline__ bool tile_nonfinite(const float *tile)
+// True when any value of the tile is infinite, NaN or so large that a
+// Sobel product could overflow (block-wide); such blocks take the literal
+// 27-tap multiply-then-add path.
+__device__ __forceinline__ bool tile_unsafe(const float *tile)
 {
     const int tid = threadIdx.x + threadIdx.y * kFX;
     int bad = 0;
-    for (int e = tid; e < kSX * kSY * kSZ; e += kFX * kFY) bad |= !isfinite(tile[e]);
+    for (int e = tid; e < kSX * kSY * kSZ; e += kFX * kFY) bad |= !(fabsf(tile[e]) < 1.0e30f);
     return __syncthreads_or(bad) != 0;
 }
 
 __device__ __forceinline__ float sob_w(int dd) { return dd == 0 ? 2.0f : 1.0f; }
 
-// Gradient at tile position (lx, ly, lz) (interior coordinates).  With
-// `all_taps` false the zero-coefficient taps of the Sobel tables are skipped:
-// for finite inputs adding v*0 leaves the running sum unchanged (the sum
-// starts at +0 and can never become -0), so the result is identical.
-__device__ __forceinline__ void gradient(const float *tile, int lx, int ly, int lz, int sobel, bool all_taps,
+// Gradient at tile position (lx, ly, lz) (interior coordinates).
+// Literal path (`literal`): every tap as the reference writes it,
+// acc = acc + v * coef.  Fast path: the coefficients are 0, +-1, +-2, +-4, so
+// for finite v of moderate size v * coef is exact and acc + v * coef rounds
+// exactly like fma(v, coef, acc); zero taps leave acc unchanged (acc starts at
+// +0 and never becomes -0).  Both paths give the same bits.
+__device__ __forceinline__ void gradient(const float *tile, int lx, int ly, int lz, int sobel, bool literal,
                                          float &gx, float &gy, float &gz)
 {
     if (sobel) {
@@ -86,9 +90,18 @@ __device__ __forceinline__ void gradient(const float *tile, int lx, int ly, int 
 #pragma unroll
                 for (int dx = -1; dx <= 1; dx++) {
                     const float v = tile[(lx + 1 + dx) + (ly + 1 + dy) * kSX + (lz + 1 + dz) * kSX * kSY];
-                    if (all_taps || dz != 0) ax = ax + v * (sob_w(dx) * sob_w(dy) * (float)dz);
-                    if (all_taps || dx != 0) ay = ay + v * ((float)dx * sob_w(dy) * sob_w(dz));
-                    if (all_taps || dy != 0) az = az + v * (sob_w(dx) * (float)dy * sob_w(dz));
+                    const float cx = sob_w(dx) * sob_w(dy) * (float)dz;
+                    const float cy = (float)dx * sob_w(dy) * sob_w(dz);
+                    const float cz = sob_w(dx) * (float)dy * sob_w(dz);
+                    if (literal) {
+                        ax = ax + v * cx;
+                        ay = ay + v * cy;
+                        az = az + v * cz;
+                    } else {
+                        if (dz != 0) ax = __fmaf_rn(v, cx, ax);
+                        if (dx != 0) ay = __fmaf_rn(v, cy, ay);
+                        if (dy != 0) az = __fmaf_rn(v, cz, az);
+                    }
                 }
         gx = ax;
         gy = ay;
@@ -152,10 +165,10 @@ __global__ void __launch_bounds__(kFX *kFY) k_flow(StepParams p, FlowBuffers b)
         if (f < C) cp_async_wait<1>();
         else cp_async_wait<0>();
         __syncthreads();
-        const bool all_taps = sobel && tile_nonfinite(tile);
+        const bool literal = sobel && tile_unsafe(tile);
         if (f == 0) {
 #pragma unroll
-            for (int lz = 0; lz < kFZ; lz++) gradient(tile, tx, ty, lz, sobel, all_taps, na[lz][0], na[lz][1], na[lz][2]);
+            for (int lz = 0; lz < kFZ; lz++) gradient(tile, tx, ty, lz, sobel, literal, na[lz][0], na[lz][1], na[lz][2]);
             if (b.NA && col_in) {
 #pragma unroll
                 for (int lz = 0; lz < kFZ; lz++) {
@@ -175,7 +188,7 @@ __global__ void __launch_bounds__(kFX *kFY) k_flow(StepParams p, FlowBuffers b)
                 const long long i = x + (long long)y * d.W + (long long)z * d.W * d.H;
                 const long long ci = (long long)c * N + i;
                 float nu[3];
-                gradient(tile, tx, ty, lz, sobel, all_taps, nu[0], nu[1], nu[2]);
+                gradient(tile, tx, ty, lz, sobel, literal, nu[0], nu[1], nu[2]);
                 float alpha;
                 {
                     const float g = gal[lz];
