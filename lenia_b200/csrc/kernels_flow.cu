@@ -78,34 +78,46 @@ __device__ __forceinline__ float sob_w(int dd) { return dd == 0 ? 2.0f : 1.0f; }
 // for finite v of moderate size v * coef is exact and acc + v * coef rounds
 // exactly like fma(v, coef, acc); zero taps leave acc unchanged (acc starts at
 // +0 and never becomes -0).  Both paths give the same bits.
+template <bool LITERAL>
+__device__ __forceinline__ void sobel_taps(const float *tile, int lx, int ly, int lz, float &gx, float &gy, float &gz)
+{
+    float ax = 0.0f, ay = 0.0f, az = 0.0f;
+#pragma unroll
+    for (int dz = -1; dz <= 1; dz++)
+#pragma unroll
+        for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+            for (int dx = -1; dx <= 1; dx++) {
+                const float v = tile[(lx + 1 + dx) + (ly + 1 + dy) * kSX + (lz + 1 + dz) * kSX * kSY];
+                const float cx = sob_w(dx) * sob_w(dy) * (float)dz;
+                const float cy = (float)dx * sob_w(dy) * sob_w(dz);
+                const float cz = sob_w(dx) * (float)dy * sob_w(dz);
+                if (LITERAL) {
+                    ax = ax + v * cx;
+                    ay = ay + v * cy;
+                    az = az + v * cz;
+                } else {
+                    if (dz != 0) ax = __fmaf_rn(v, cx, ax);
+                    if (dx != 0) ay = __fmaf_rn(v, cy, ay);
+                    if (dy != 0) az = __fmaf_rn(v, cz, az);
+                }
+            }
+    gx = ax;
+    gy = ay;
+    gz = az;
+}
+
+__device__ __noinline__ void sobel_literal(const float *tile, int lx, int ly, int lz, float &gx, float &gy, float &gz)
+{
+    sobel_taps<true>(tile, lx, ly, lz, gx, gy, gz);
+}
+
 __device__ __forceinline__ void gradient(const float *tile, int lx, int ly, int lz, int sobel, bool literal,
                                          float &gx, float &gy, float &gz)
 {
     if (sobel) {
-        float ax = 0.0f, ay = 0.0f, az = 0.0f;
-#pragma unroll
-        for (int dz = -1; dz <= 1; dz++)
-#pragma unroll
-            for (int dy = -1; dy <= 1; dy++)
-#pragma unroll
-                for (int dx = -1; dx <= 1; dx++) {
-                    const float v = tile[(lx + 1 + dx) + (ly + 1 + dy) * kSX + (lz + 1 + dz) * kSX * kSY];
-                    const float cx = sob_w(dx) * sob_w(dy) * (float)dz;
-                    const float cy = (float)dx * sob_w(dy) * sob_w(dz);
-                    const float cz = sob_w(dx) * (float)dy * sob_w(dz);
-                    if (literal) {
-                        ax = ax + v * cx;
-                        ay = ay + v * cy;
-                        az = az + v * cz;
-                    } else {
-                        if (dz != 0) ax = __fmaf_rn(v, cx, ax);
-                        if (dx != 0) ay = __fmaf_rn(v, cy, ay);
-                        if (dy != 0) az = __fmaf_rn(v, cz, az);
-                    }
-                }
-        gx = ax;
-        gy = ay;
-        gz = az;
+        if (literal) sobel_literal(tile, lx, ly, lz, gx, gy, gz);
+        else sobel_taps<false>(tile, lx, ly, lz, gx, gy, gz);
     } else {
         const int c = (lx + 1) + (ly + 1) * kSX + (lz + 1) * kSX * kSY;
         gx = (tile[c + 1] - tile[c - 1]) * 0.5f;

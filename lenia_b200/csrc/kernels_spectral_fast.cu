@@ -137,7 +137,7 @@ __device__ __forceinline__ void load_packed_rows_s(float2 *buf, const float2 *s0
 }
 
 template <int W>
-__global__ void __launch_bounds__(kFastRowThreads) k_growth_rows_s(GrowthJobs jobs, const float2 *__restrict__ tw_x,
+__global__ void __launch_bounds__(kFastRowThreads, 3) k_growth_rows_s(GrowthJobs jobs, const float2 *__restrict__ tw_x,
                                                                    const float *__restrict__ lut_rows,
                                                                    const float *__restrict__ A,
                                                                    float *__restrict__ Hout, float *__restrict__ Uout,

@@ -242,11 +242,12 @@ __global__ void __launch_bounds__(256) k_transport(StepParams p, TransportBuffer
 // the column that the source reaches.  Each destination still receives its
 // contributions in the reference's (dz, dy, dx) order, with the reference's
 // float operations, so the result is bit-identical.
-constexpr int kTX = 32, kTY = 8, kTZ = 8;
+constexpr int kTX = 32, kTY = 8, kTZ = 4;
 
-__device__ __forceinline__ float overlap(float d, float si, float clip, bool torus, int ext)
+template <bool TORUS>
+__device__ __forceinline__ float overlap(float d, float si, float clip, int ext)
 {
-    if (torus) d = torus_wrap(d, ext);
+    if (TORUS) d = torus_wrap(d, ext);
     d = fabsf(d);
     d = si - d;
     d = tmax(d, 0.0f);
@@ -269,7 +270,7 @@ __device__ __forceinline__ bool tb_source(const Dims &d, int dd, int &x, int &y,
     return true;
 }
 
-template <int DD>
+template <int DD, bool TORUS>
 __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, TransportBuffers b)
 {
     constexpr int SX = kTX + 2 * DD, SY = kTY + 2 * DD, SZ = kTZ + 2 * DD, SV = SX * SY * SZ;
@@ -284,7 +285,6 @@ __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, Tran
     const int z0 = blockIdx.y * kTZ;
     const int x = x0 + tx, y = y0 + ty;
     const float px = (float)x + 0.5f, py = (float)y + 0.5f;
-    const bool torus = p.border == kBorderTorus;
     const bool srt = p.mode_type == kModeSRT;
     const int crt = p.rt_all_channels ? C : (C < 3 ? C : 3);
     const int tid = tx + ty * kTX;
@@ -351,8 +351,8 @@ __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, Tran
 #pragma unroll
                     for (int ox = -DD; ox <= DD; ox++) {
                         const int e = (tx + DD + ox) + (ty + DD + oy) * SX + lz * SX * SY;
-                        const float mx = overlap(px - tmx[e], p.si, p.clip, torus, d.W);
-                        const float my = overlap(py - tmy[e], p.si, p.clip, torus, d.H);
+                        const float mx = overlap<TORUS>(px - tmx[e], p.si, p.clip, d.W);
+                        const float my = overlap<TORUS>(py - tmy[e], p.si, p.clip, d.H);
                         const float am = tar[e] * mx;
                         const float amy = am * my;
                         const float smz = tmz[e];
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, Tran
                             const int j = lz - DD - oz;  // destination whose offset to this source is oz
                             if (j < 0 || j >= kTZ) continue;
                             const float pz = (float)(z0 + j) + 0.5f;
-                            const float mz = overlap(pz - smz, p.si, p.clip, torus, d.D);
+                            const float mz = overlap<TORUS>(pz - smz, p.si, p.clip, d.D);
                             float w = amy * mz;
                             w = w * p.sn;
                             acc[j] = acc[j] + w;
@@ -397,22 +397,17 @@ cudaError_t launch_transport(const StepParams &p, const TransportBuffers &b, cud
     if ((p.mode_type == kModeRT || p.mode_type == kModeSRT) && p.dd >= 1 && p.dd <= 2) {
         const int tiles_x = (p.d.W + kTX - 1) / kTX, tiles_y = (p.d.H + kTY - 1) / kTY;
         dim3 grid(tiles_x * tiles_y, (p.d.D + kTZ - 1) / kTZ), block(kTX, kTY);
-        if (p.dd == 1) {
-            constexpr int SV = (kTX + 2) * (kTY + 2) * (kTZ + 2);
-            const size_t smem = 2 * 4 * SV * sizeof(float);
-            cudaError_t e = cudaFuncSetAttribute(k_transport_tiled<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
+        const bool torus = p.border == kBorderTorus;
+        auto go = [&](auto kern, int dd) -> cudaError_t {
+            const int sv = (kTX + 2 * dd) * (kTY + 2 * dd) * (kTZ + 2 * dd);
+            const size_t smem = 2 * 4 * (size_t)sv * sizeof(float);
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
-            k_transport_tiled<1><<<grid, block, smem, st>>>(p, b);
-        } else {
-            constexpr int SV = (kTX + 4) * (kTY + 4) * (kTZ + 4);
-            const size_t smem = 2 * 4 * SV * sizeof(float);
-            cudaError_t e = cudaFuncSetAttribute(k_transport_tiled<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
-            if (e != cudaSuccess) return e;
-            k_transport_tiled<2><<<grid, block, smem, st>>>(p, b);
-        }
-        return cudaGetLastError();
+            kern<<<grid, block, smem, st>>>(p, b);
+            return cudaGetLastError();
+        };
+        if (p.dd == 1) return torus ? go(k_transport_tiled<1, true>, 1) : go(k_transport_tiled<1, false>, 1);
+        return torus ? go(k_transport_tiled<2, true>, 2) : go(k_transport_tiled<2, false>, 2);
     }
     k_transport<<<(unsigned)((p.d.N + 255) / 256), 256, 0, st>>>(p, b);
     return cudaGetLastError();
