@@ -12,14 +12,23 @@ namespace lenia {
 
 namespace {
 
+#ifndef LENIA_PLANE_THREADS
+#define LENIA_PLANE_THREADS 1024
+#endif
+#ifndef LENIA_GROWTH_THREADS
+#define LENIA_GROWTH_THREADS 256
+#endif
+#ifndef LENIA_GROWTH_ROWS
+#define LENIA_GROWTH_ROWS 16
+#endif
 constexpr int kFastRowThreads = 256;
-constexpr int kFastPlaneThreads = 512;
+constexpr int kFastPlaneThreads = LENIA_PLANE_THREADS;    // block of the plane transform
+constexpr int kGrowthThreads = LENIA_GROWTH_THREADS;      // block of the growth pass
 
-// Rows per tile of the growth pass: at most 8 (the accumulators live in
-// registers, so smaller tiles keep more blocks resident).
+// Rows per tile of the growth pass.
 constexpr int growth_tile_for(int n)
 {
-    for (int t = 8; t > 1; t--)
+    for (int t = LENIA_GROWTH_ROWS; t > 1; t--)
         if (n % t == 0) return t;
     return 1;
 }
@@ -28,7 +37,8 @@ template <int W, bool GROWTH = false>
 struct RowShape {
     static constexpr int TY = GROWTH ? growth_tile_for(W) : row_tile_for(W);
     static constexpr int T = TY * W;                       // cells of a tile
-    static constexpr int NCELL = (T + kFastRowThreads - 1) / kFastRowThreads;  // cells per thread
+    static constexpr int THREADS = GROWTH ? kGrowthThreads : kFastRowThreads;
+    static constexpr int NCELL = (T + THREADS - 1) / THREADS;  // cells per thread
     using PM = PadMat<W>;
 };
 
@@ -137,7 +147,7 @@ __device__ __forceinline__ void load_packed_rows_s(float2 *buf, const float2 *s0
 }
 
 template <int W>
-__global__ void __launch_bounds__(kFastRowThreads, 3) k_growth_rows_s(GrowthJobs jobs, const float2 *__restrict__ tw_x,
+__global__ void __launch_bounds__(kGrowthThreads) k_growth_rows_s(GrowthJobs jobs, const float2 *__restrict__ tw_x,
                                                                    const float *__restrict__ lut_rows,
                                                                    const float *__restrict__ A,
                                                                    float *__restrict__ Hout, float *__restrict__ Uout,
@@ -156,8 +166,8 @@ __global__ void __launch_bounds__(kFastRowThreads, 3) k_growth_rows_s(GrowthJobs
     const int y0 = (blockIdx.x % (H / TY)) * TY;
     const long long base = ((long long)z * H + y0) * W;
     const float nf = (float)N;
-    for (int i = threadIdx.x; i < W; i += kFastRowThreads) tw[i] = tw_x[i];
-    for (int i = threadIdx.x; i < 256 * K; i += kFastRowThreads) lut[i] = lut_rows[i];
+    for (int i = threadIdx.x; i < W; i += kGrowthThreads) tw[i] = tw_x[i];
+    for (int i = threadIdx.x; i < 256 * K; i += kGrowthThreads) lut[i] = lut_rows[i];
 
     // The packed row spectrum of a kernel pair: element e of the tile is
     // (ty = e % TY, kx = e / TY); its half-spectrum values are prefetched into
@@ -168,8 +178,8 @@ __global__ void __launch_bounds__(kFastRowThreads, 3) k_growth_rows_s(GrowthJobs
         const float2 *s1 = k0 + 1 < K ? jobs.spec[k0 + 1] : nullptr;
 #pragma unroll
         for (int i = 0; i < NCELL; i++) {
-            const int e = threadIdx.x + i * kFastRowThreads;
-            if (T % kFastRowThreads != 0 && e >= T) continue;
+            const int e = threadIdx.x + i * kGrowthThreads;
+            if (T % kGrowthThreads != 0 && e >= T) continue;
             const int ty = e % TY, kx = e / TY;
             const int m = kx < KX ? kx : W - kx;
             const long long o = ((long long)m * D + z) * H + y0 + ty;
@@ -178,22 +188,25 @@ __global__ void __launch_bounds__(kFastRowThreads, 3) k_growth_rows_s(GrowthJobs
         }
     };
 
-    float hacc[NCELL][kMaxChannels], uacc[NCELL][kMaxChannels];
+    // H accumulates in registers, U_SUM in shared memory (channel-major)
+    float *uacc = lut + 256 * K;
+    for (int i = threadIdx.x; i < C * T; i += kGrowthThreads) uacc[i] = 0.0f;
+    float hacc[NCELL][kMaxChannels];
 #pragma unroll
     for (int i = 0; i < NCELL; i++)
 #pragma unroll
-        for (int c = 0; c < kMaxChannels; c++) {
-            hacc[i][c] = 0.0f;
-            uacc[i][c] = 0.0f;
-        }
+        for (int c = 0; c < kMaxChannels; c++) hacc[i][c] = 0.0f;
     int bad = 0;
+    // u = re / N; for N a power of two the quotient is exactly re * (1/N)
+    constexpr bool kPow2 = (N & (N - 1)) == 0;
+    constexpr float kInvN = 1.0f / (float)N;
     if (K > 0) prefetch(0);
     for (int k0 = 0; k0 < K; k0 += 2) {
         const int k1 = k0 + 1 < K ? k0 + 1 : -1;
 #pragma unroll
         for (int i = 0; i < NCELL; i++) {
-            const int e = threadIdx.x + i * kFastRowThreads;
-            if (T % kFastRowThreads != 0 && e >= T) continue;
+            const int e = threadIdx.x + i * kGrowthThreads;
+            if (T % kGrowthThreads != 0 && e >= T) continue;
             const int ty = e % TY, kx = e / TY;
             const float2 a = pa[i], b = pb[i];
             float2 r;
@@ -203,51 +216,58 @@ __global__ void __launch_bounds__(kFastRowThreads, 3) k_growth_rows_s(GrowthJobs
         }
         __syncthreads();
         if (k0 + 2 < K) prefetch(k0 + 2);
-        static_fft<W, TY, false, W, kFastRowThreads>(buf, tw, +1);
+        static_fft<W, TY, false, W, kGrowthThreads>(buf, tw, +1);
 #pragma unroll
-        for (int i = 0; i < NCELL; i++) {
-            const int e = threadIdx.x + i * kFastRowThreads;
-            if (T % kFastRowThreads != 0 && e >= T) continue;
-            const float2 zz = buf[S::PM::at(e / W, e % W)];
+        for (int q = 0; q < 2; q++) {
+            const int k = q == 0 ? k0 : k1;
+            if (k < 0) continue;
+            const int c1 = jobs.c1[k];
+            const float h = jobs.h[k];
+            const int asym = jobs.asymptotic[c1];
+            float u[NCELL], g[NCELL];
 #pragma unroll
-            for (int q = 0; q < 2; q++) {
-                const int k = q == 0 ? k0 : k1;
-                if (k < 0) continue;
-                const float u = (q == 0 ? zz.x : zz.y) / nf;
-                const int c1 = jobs.c1[k];
-                const float h = jobs.h[k];
-                const int ui = (int)(u * 255);
+            for (int i = 0; i < NCELL; i++) {
+                const int e = threadIdx.x + i * kGrowthThreads;
+                u[i] = 0.0f;
+                g[i] = 0.0f;
+                if (T % kGrowthThreads != 0 && e >= T) continue;
+                const float2 zz = buf[S::PM::at(e / W, e % W)];
+                const float re = q == 0 ? zz.x : zz.y;
+                u[i] = kPow2 ? re * kInvN : re / nf;
+                const int ui = (int)(u[i] * 255);
                 float l;
                 if (ui >= 0 && ui < 256) l = lut[k * 256 + ui];
                 else {
-                    if (!(u == u)) bad = 1;
+                    if (!(u[i] == u[i])) bad = 1;
                     l = lut_flat_dev((long long)jobs.lut_base[k] + ui);
                 }
-#pragma unroll
-                for (int c = 0; c < kMaxChannels; c++) {
-                    if (c == c1) {
-                        uacc[i][c] = uacc[i][c] + u;
-                        const float g =
-                            jobs.asymptotic[c] ? (l - __ldg(A + (long long)c * N + base + e)) * h : l * h;
-                        hacc[i][c] = hacc[i][c] + g;
-                    }
-                }
-                if (Udbg) Udbg[(long long)k * N + base + e] = u;
+                g[i] = asym ? (l - __ldg(A + (long long)c1 * N + base + e)) * h : l * h;
+                uacc[c1 * T + e] = uacc[c1 * T + e] + u[i];
+                if (Udbg) Udbg[(long long)k * N + base + e] = u[i];
+            }
+            // uniform branch on the destination channel keeps hacc in registers
+            switch (c1) {
+#define LENIA_ACC(cc)                                                              \
+    case cc:                                                                       \
+        _Pragma("unroll") for (int i = 0; i < NCELL; i++) hacc[i][cc] = hacc[i][cc] + g[i]; \
+        break;
+                LENIA_ACC(0) LENIA_ACC(1) LENIA_ACC(2) LENIA_ACC(3)
+#undef LENIA_ACC
             }
         }
         __syncthreads();
     }
 #pragma unroll
     for (int i = 0; i < NCELL; i++) {
-        const int e = threadIdx.x + i * kFastRowThreads;
-        if (T % kFastRowThreads != 0 && e >= T) continue;
+        const int e = threadIdx.x + i * kGrowthThreads;
+        if (T % kGrowthThreads != 0 && e >= T) continue;
 #pragma unroll
         for (int c = 0; c < kMaxChannels; c++) {
             if (c >= C) continue;
             const long long o = (long long)c * N + base + e;
             const float hv = hacc[i][c];
             Hout[o] = hv;
-            Uout[o] = uacc[i][c];
+            Uout[o] = uacc[c * T + e];
             if (jobs.growth_rt) BACK[o] = early_growth(__ldg(A + o), hv, jobs.timestep, jobs.soft_clip[c]);
         }
     }
@@ -313,10 +333,11 @@ cudaError_t growth_rows_w(const float2 *tw, const GrowthJobs &jobs, const float 
                           float *U, float *BACK, float *Udbg, int *err, cudaStream_t st)
 {
     using S = RowShape<W, true>;
-    const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2) + (size_t)256 * jobs.K * sizeof(float);
+    const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2) + (size_t)256 * jobs.K * sizeof(float) +
+                        (size_t)jobs.C * S::T * sizeof(float);
     cudaError_t e = smem_attr((const void *)k_growth_rows_s<W>, smem);
     if (e != cudaSuccess) return e;
-    k_growth_rows_s<W><<<W * (W / S::TY), kFastRowThreads, smem, st>>>(jobs, tw, lut, A, H, U, BACK, Udbg, err);
+    k_growth_rows_s<W><<<W * (W / S::TY), kGrowthThreads, smem, st>>>(jobs, tw, lut, A, H, U, BACK, Udbg, err);
     return cudaGetLastError();
 }
 
