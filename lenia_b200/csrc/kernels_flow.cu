@@ -53,7 +53,7 @@ __device__ __forceinline__ void issue_tile(float *tile, const float *f, const Di
         const int lx = e % kSX, ly = (e / kSX) % kSY, lz = e / (kSX * kSY);
         int x = x0 + lx - 1, y = y0 + ly - 1, z = z0 + lz - 1;
         const bool ok = gb_source(d, border, x, y, z);
-        const float *src = ok ? f + x + (long long)y * d.W + (long long)z * d.W * d.H : f;
+        const float *src = ok ? f + x + y * d.W + z * d.W * d.H : f;
         cp_async_f32(tile + e, src, ok);
     }
     cp_async_commit();
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kFX *kFY) k_flow(StepParams p, FlowBuffers b)
     __shared__ float tiles[2][kSX * kSY * kSZ];
     const Dims &d = p.d;
     const int C = p.C;
-    const long long N = d.N;
+    const int N = d.N;
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int tiles_x = (d.W + kFX - 1) / kFX;
     const int x0 = (blockIdx.x % tiles_x) * kFX;
@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(kFX *kFY) k_flow(StepParams p, FlowBuffers b)
     issue_tile(tiles[0], b.SUM, d, x0, y0, z0, p.sobel_border);
     for (int f = 0; f <= C; f++) {
         float *tile = tiles[f & 1];
-        if (f < C) issue_tile(tiles[(f + 1) & 1], b.H + (long long)f * N, d, x0, y0, z0, p.sobel_border);
+        if (f < C) issue_tile(tiles[(f + 1) & 1], b.H + f * N, d, x0, y0, z0, p.sobel_border);
         // per-cell inputs of this channel, loaded while the tile lands
         float v3[3][kFZ], gal[kFZ];
         unsigned gvalid = 0;  // bit lz: the alpha source of cell lz was written
@@ -157,16 +157,17 @@ __global__ void __launch_bounds__(kFX *kFY) k_flow(StepParams p, FlowBuffers b)
             for (int lz = 0; lz < kFZ; lz++) {
                 const int z = z0 + lz;
                 if (z >= d.D) continue;
-                const long long i = x + (long long)y * d.W + (long long)z * d.W * d.H;
-                const long long ci = (long long)c * N + i;
+                const int i = x + y * d.W + z * d.W * d.H;
+                const int ci = c * N + i;
 #pragma unroll
-                for (int q = 0; q < 3; q++) v3[q][lz] = b.V[(long long)q * C * N + ci];
+                for (int q = 0; q < 3; q++) v3[q][lz] = b.V[q * C * N + ci];
                 // alpha source: PREALPHA as compute_f reads it (flat c*N + i),
                 // written by sobel_convolve_h from channel f / P, cell f % P (Q20)
-                long long src_c = c, src_i = i;
+                int src_c = c, src_i = i;
                 bool valid = true;
                 if (!p.alpha_index_fix) {
-                    src_c = ci / d.P;
+                    // ci < 4 N < 4 P, so the block index is 0..3
+                    src_c = (ci >= d.P) + (ci >= 2 * d.P) + (ci >= 3 * d.P);
                     src_i = ci - src_c * d.P;
                     valid = src_c < C && src_i < N;
                 }
@@ -186,7 +187,7 @@ __global__ void __launch_bounds__(kFX *kFY) k_flow(StepParams p, FlowBuffers b)
                 for (int lz = 0; lz < kFZ; lz++) {
                     const int z = z0 + lz;
                     if (z >= d.D) continue;
-                    const long long i = x + (long long)y * d.W + (long long)z * d.W * d.H;
+                    const int i = x + y * d.W + z * d.W * d.H;
                     b.NA[i] = na[lz][0];
                     b.NA[N + i] = na[lz][1];
                     b.NA[2 * N + i] = na[lz][2];
@@ -197,8 +198,8 @@ __global__ void __launch_bounds__(kFX *kFY) k_flow(StepParams p, FlowBuffers b)
             for (int lz = 0; lz < kFZ; lz++) {
                 const int z = z0 + lz;
                 if (z >= d.D) continue;
-                const long long i = x + (long long)y * d.W + (long long)z * d.W * d.H;
-                const long long ci = (long long)c * N + i;
+                const int i = x + y * d.W + z * d.W * d.H;
+                const int ci = c * N + i;
                 float nu[3];
                 gradient(tile, tx, ty, lz, sobel, literal, nu[0], nu[1], nu[2]);
                 float alpha;
@@ -215,15 +216,15 @@ __global__ void __launch_bounds__(kFX *kFY) k_flow(StepParams p, FlowBuffers b)
                 if (b.PREALPHA) b.PREALPHA[ci] = alpha;
                 if (b.NU) {
                     b.NU[ci] = nu[0];
-                    b.NU[(long long)C * N + ci] = nu[1];
+                    b.NU[C * N + ci] = nu[1];
                     b.NU[2LL * C * N + ci] = nu[2];
                 }
                 if (b.ALPHA) {
                     // ALPHA = |GRID - GA| with GA read at c*P + i (Q20)
                     // (GA blocks past the last channel are never written: 0)
                     const float g = __ldg(b.A + ci);
-                    const long long fi = p.alpha_index_fix ? ci : (long long)c * d.P + i;
-                    const float ga = fi < (long long)C * N ? __ldg(b.GA + fi) : 0.0f;
+                    const int fi = p.alpha_index_fix ? ci : c * d.P + i;
+                    const float ga = fi < C * N ? __ldg(b.GA + fi) : 0.0f;
                     b.ALPHA[ci] = fabsf(g - ga);
                 }
                 const float a1 = 1.0f - alpha;
@@ -232,7 +233,7 @@ __global__ void __launch_bounds__(kFX *kFY) k_flow(StepParams p, FlowBuffers b)
                 for (int q = 0; q < 3; q++) f3[q] = nu[q] * a1 - na[lz][q] * alpha;
                 if (b.F) {
 #pragma unroll
-                    for (int q = 0; q < 3; q++) b.F[(long long)q * C * N + ci] = f3[q];
+                    for (int q = 0; q < 3; q++) b.F[q * C * N + ci] = f3[q];
                 }
                 float vv[3] = {v3[0][lz], v3[1][lz], v3[2][lz]};
                 const float pos[3] = {(float)x + 0.5f, (float)y + 0.5f, (float)z + 0.5f};
@@ -250,14 +251,14 @@ __global__ void __launch_bounds__(kFX *kFY) k_flow(StepParams p, FlowBuffers b)
                         m = smax(m, p.sigma);
                         m = smin(m, q == 1 ? p.ghs : p.gws);
                     }
-                    b.MU[(long long)q * C * N + ci] = m;
+                    b.MU[q * C * N + ci] = m;
                 }
                 if (!p.mu_vel) {
 #pragma unroll
                     for (int q = 0; q < 3; q++) vv[q] = (vv[q] + f3[q]) * p.v_damp;
                 }
 #pragma unroll
-                for (int q = 0; q < 3; q++) b.V[(long long)q * C * N + ci] = vv[q];
+                for (int q = 0; q < 3; q++) b.V[q * C * N + ci] = vv[q];
             }
         }
         __syncthreads();

@@ -244,11 +244,15 @@ __global__ void __launch_bounds__(256) k_transport(StepParams p, TransportBuffer
 // float operations, so the result is bit-identical.
 constexpr int kTX = 32, kTY = 8, kTZ = 4;
 
-template <bool TORUS>
+// min(max(si - |d|, 0), clip).  With clip == 1 the clamp is a saturating
+// add: identical for every input (NaN and negative values give +0 either
+// way, and a -0 factor cannot change the accumulated sum).
+template <bool TORUS, bool CLIP1>
 __device__ __forceinline__ float overlap(float d, float si, float clip, int ext)
 {
     if (TORUS) d = torus_wrap(d, ext);
     d = fabsf(d);
+    if (CLIP1) return __saturatef(si - d);
     d = si - d;
     d = tmax(d, 0.0f);
     d = tmin(d, clip);
@@ -270,7 +274,7 @@ __device__ __forceinline__ bool tb_source(const Dims &d, int dd, int &x, int &y,
     return true;
 }
 
-template <int DD, bool TORUS>
+template <int DD, bool TORUS, bool CLIP1>
 __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, TransportBuffers b)
 {
     constexpr int SX = kTX + 2 * DD, SY = kTY + 2 * DD, SZ = kTZ + 2 * DD, SV = SX * SY * SZ;
@@ -300,7 +304,7 @@ __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, Tran
             const int lx = e % SX, ly = (e / SX) % SY, lz = e / (SX * SY);
             int gx = x0 + lx - DD, gy = y0 + ly - DD, gz = z0 + lz - DD;
             const bool ok = tb_source(d, p.dd, gx, gy, gz);
-            const long long o = ok ? gx + (long long)gy * d.W + (long long)gz * d.W * d.H : 0;
+            const int o = ok ? gx + gy * d.W + gz * d.W * d.H : 0;
             cp_async_f32(buf + e, mux + o, ok);
             cp_async_f32(buf + SV + e, muy + o, ok);
             cp_async_f32(buf + 2 * SV + e, muz + o, ok);
@@ -351,8 +355,8 @@ __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, Tran
 #pragma unroll
                     for (int ox = -DD; ox <= DD; ox++) {
                         const int e = (tx + DD + ox) + (ty + DD + oy) * SX + lz * SX * SY;
-                        const float mx = overlap<TORUS>(px - tmx[e], p.si, p.clip, d.W);
-                        const float my = overlap<TORUS>(py - tmy[e], p.si, p.clip, d.H);
+                        const float mx = overlap<TORUS, CLIP1>(px - tmx[e], p.si, p.clip, d.W);
+                        const float my = overlap<TORUS, CLIP1>(py - tmy[e], p.si, p.clip, d.H);
                         const float am = tar[e] * mx;
                         const float amy = am * my;
                         const float smz = tmz[e];
@@ -361,7 +365,7 @@ __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, Tran
                             const int j = lz - DD - oz;  // destination whose offset to this source is oz
                             if (j < 0 || j >= kTZ) continue;
                             const float pz = (float)(z0 + j) + 0.5f;
-                            const float mz = overlap<TORUS>(pz - smz, p.si, p.clip, d.D);
+                            const float mz = overlap<TORUS, CLIP1>(pz - smz, p.si, p.clip, d.D);
                             float w = amy * mz;
                             w = w * p.sn;
                             acc[j] = acc[j] + w;
@@ -406,8 +410,13 @@ cudaError_t launch_transport(const StepParams &p, const TransportBuffers &b, cud
             kern<<<grid, block, smem, st>>>(p, b);
             return cudaGetLastError();
         };
-        if (p.dd == 1) return torus ? go(k_transport_tiled<1, true>, 1) : go(k_transport_tiled<1, false>, 1);
-        return torus ? go(k_transport_tiled<2, true>, 2) : go(k_transport_tiled<2, false>, 2);
+        const bool c1 = p.clip == 1.0f;
+        if (p.dd == 1) {
+            if (c1) return torus ? go(k_transport_tiled<1, true, true>, 1) : go(k_transport_tiled<1, false, true>, 1);
+            return torus ? go(k_transport_tiled<1, true, false>, 1) : go(k_transport_tiled<1, false, false>, 1);
+        }
+        if (c1) return torus ? go(k_transport_tiled<2, true, true>, 2) : go(k_transport_tiled<2, false, true>, 2);
+        return torus ? go(k_transport_tiled<2, true, false>, 2) : go(k_transport_tiled<2, false, false>, 2);
     }
     k_transport<<<(unsigned)((p.d.N + 255) / 256), 256, 0, st>>>(p, b);
     return cudaGetLastError();
