@@ -7,6 +7,7 @@
 #include "lenia_internal.h"
 #include "lfft_static.cuh"
 #include "growth_common.cuh"
+#include "async_copy.cuh"
 
 namespace lenia {
 
@@ -274,6 +275,153 @@ __global__ void __launch_bounds__(kGrowthThreads) k_growth_rows_s(GrowthJobs job
     if (bad && err_flag) atomicOr(err_flag, 1);
 }
 
+// Growth pass with warp-level transforms.  A block owns 8 warps x 2 rows of
+// one z slice.  For each kernel pair the block stages the pair's half-spectrum
+// rows with cp.async (double buffered, one block barrier per pair); each warp
+// then builds its two packed rows, transforms them with warp-scope barriers
+// only, and accumulates the growth of its 2 x W cells.  Arithmetic and order
+// are those of k_growth_rows_s.
+constexpr int kGwWarps = 8, kGwRows = 2, kGwRowsBlock = kGwWarps * kGwRows;
+
+template <int W>
+struct GrowthWarpShape {
+    static constexpr int KX = W / 2 + 1;
+    static constexpr int STAGE = 2 * KX * kGwRowsBlock;          // float2 per staged pair
+    static constexpr int CELLS = kGwRows * W / 32;                // cells per lane
+    using PM = PadMat<W>;
+    static constexpr int ZW = PM::RP * kGwRows;                   // float2 per warp row buffer
+    static size_t smem(int K, int C)
+    {
+        return (size_t)(W + 2 * STAGE + kGwWarps * ZW) * sizeof(float2) + (size_t)256 * K * sizeof(float) +
+               (size_t)kGwWarps * C * kGwRows * W * sizeof(float);
+    }
+};
+
+template <int W>
+__global__ void __launch_bounds__(kGwWarps * 32) k_growth_warp(GrowthJobs jobs, const float2 *__restrict__ tw_x,
+                                                               const float *__restrict__ lut_rows,
+                                                               const float *__restrict__ A, float *__restrict__ Hout,
+                                                               float *__restrict__ Uout, float *__restrict__ BACK,
+                                                               float *__restrict__ Udbg, int *err_flag)
+{
+    using S = GrowthWarpShape<W>;
+    constexpr int H = W, D = W, KX = S::KX, CELLS = S::CELLS, RB = kGwRowsBlock;
+    constexpr int T = kGwRows * W;  // cells of a warp
+    constexpr long long N = (long long)W * W * W;
+    extern __shared__ float2 smem[];
+    float2 *tw = smem;
+    float2 *stage = tw + W;                          // [2][kernel 0/1][KX][RB]
+    float2 *zrows = stage + 2 * S::STAGE;            // [warp][PadMat rows]
+    float *lut = reinterpret_cast<float *>(zrows + kGwWarps * S::ZW);
+    float *uall = lut + 256 * jobs.K;                // [warp][C][T]
+    const int C = jobs.C, K = jobs.K;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int z = blockIdx.x / (H / RB);
+    const int y0 = (blockIdx.x % (H / RB)) * RB;
+    const int yw = warp * kGwRows;                   // first row of this warp within the block
+    const long long base = ((long long)z * H + y0 + yw) * W;
+    float2 *zb = zrows + warp * S::ZW;
+    float *uacc = uall + warp * C * T;
+    for (int i = threadIdx.x; i < W; i += kGwWarps * 32) tw[i] = tw_x[i];
+    for (int i = threadIdx.x; i < 256 * K; i += kGwWarps * 32) lut[i] = lut_rows[i];
+    for (int i = lane; i < C * T; i += 32) uacc[i] = 0.0f;
+
+    auto issue = [&](int k0, int buf) {
+        float2 *dst = stage + buf * S::STAGE;
+        for (int e = threadIdx.x; e < S::STAGE; e += kGwWarps * 32) {
+            const int q = e / (KX * RB), rem = e % (KX * RB);
+            const int kx = rem / RB, ty = rem % RB;
+            const int k = k0 + q;
+            const bool ok = k < K;
+            const float2 *src = ok ? jobs.spec[k] + ((long long)kx * D + z) * H + y0 + ty : jobs.spec[k0];
+            cp_async_f64(dst + e, src, ok);
+        }
+        cp_async_commit();
+    };
+
+    float hacc[CELLS][kMaxChannels];
+#pragma unroll
+    for (int i = 0; i < CELLS; i++)
+#pragma unroll
+        for (int c = 0; c < kMaxChannels; c++) hacc[i][c] = 0.0f;
+    int bad = 0;
+    constexpr bool kPow2 = (N & (N - 1)) == 0;
+    constexpr float kInvN = 1.0f / (float)N;
+    const float nf = (float)N;
+    if (K > 0) issue(0, 0);
+    for (int k0 = 0, it = 0; k0 < K; k0 += 2, it++) {
+        const int k1 = k0 + 1 < K ? k0 + 1 : -1;
+        cp_async_wait<0>();
+        __syncthreads();  // staged pair visible; every warp is done with the other buffer
+        if (k0 + 2 < K) issue(k0 + 2, (it + 1) & 1);
+        const float2 *st = stage + (it & 1) * S::STAGE;
+        // packed rows of this warp: element (r, kx), kx over the full length
+#pragma unroll
+        for (int i = 0; i < CELLS; i++) {
+            const int e = lane + 32 * i;
+            const int r = e % kGwRows, kx = e / kGwRows;
+            const int m = kx < KX ? kx : W - kx;
+            const float2 a = st[m * RB + yw + r];
+            const float2 b = st[KX * RB + m * RB + yw + r];
+            float2 v;
+            if (kx < KX) v = make_float2(a.x - b.y, a.y + b.x);
+            else v = make_float2(a.x + b.y, b.x - a.y);
+            zb[S::PM::at(r, kx)] = v;
+        }
+        __syncwarp();
+        warp_fft_rows<W, kGwRows, W>(zb, tw, +1);
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int k = q == 0 ? k0 : k1;
+            if (k < 0) continue;
+            const int c1 = jobs.c1[k];
+            const float h = jobs.h[k];
+            const int asym = jobs.asymptotic[c1];
+            float g[CELLS];
+#pragma unroll
+            for (int i = 0; i < CELLS; i++) {
+                const int e = lane + 32 * i;
+                const float2 zz = zb[S::PM::at(e / W, e % W)];
+                const float re = q == 0 ? zz.x : zz.y;
+                const float u = kPow2 ? re * kInvN : re / nf;
+                const int ui = (int)(u * 255);
+                float l;
+                if (ui >= 0 && ui < 256) l = lut[k * 256 + ui];
+                else {
+                    if (!(u == u)) bad = 1;
+                    l = lut_flat_dev((long long)jobs.lut_base[k] + ui);
+                }
+                g[i] = asym ? (l - __ldg(A + (long long)c1 * N + base + e)) * h : l * h;
+                uacc[c1 * T + e] = uacc[c1 * T + e] + u;
+                if (Udbg) Udbg[(long long)k * N + base + e] = u;
+            }
+            switch (c1) {
+#define LENIA_ACC(cc)                                                                       \
+    case cc:                                                                                \
+        _Pragma("unroll") for (int i = 0; i < CELLS; i++) hacc[i][cc] = hacc[i][cc] + g[i]; \
+        break;
+                LENIA_ACC(0) LENIA_ACC(1) LENIA_ACC(2) LENIA_ACC(3)
+#undef LENIA_ACC
+            }
+        }
+        __syncwarp();
+    }
+#pragma unroll
+    for (int i = 0; i < CELLS; i++) {
+        const int e = lane + 32 * i;
+#pragma unroll
+        for (int c = 0; c < kMaxChannels; c++) {
+            if (c >= C) continue;
+            const long long o = (long long)c * N + base + e;
+            const float hv = hacc[i][c];
+            Hout[o] = hv;
+            Uout[o] = uacc[c * T + e];
+            if (jobs.growth_rt) BACK[o] = early_growth(__ldg(A + o), hv, jobs.timestep, jobs.soft_clip[c]);
+        }
+    }
+    if (bad && err_flag) atomicOr(err_flag, 1);
+}
+
 template <int W>
 __global__ void __launch_bounds__(kFastRowThreads) k_blur_rows_s(BlurJobs jobs, const float2 *__restrict__ tw_x)
 {
@@ -332,13 +480,23 @@ template <int W>
 cudaError_t growth_rows_w(const float2 *tw, const GrowthJobs &jobs, const float *lut, const float *A, float *H,
                           float *U, float *BACK, float *Udbg, int *err, cudaStream_t st)
 {
-    using S = RowShape<W, true>;
-    const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2) + (size_t)256 * jobs.K * sizeof(float) +
-                        (size_t)jobs.C * S::T * sizeof(float);
-    cudaError_t e = smem_attr((const void *)k_growth_rows_s<W>, smem);
-    if (e != cudaSuccess) return e;
-    k_growth_rows_s<W><<<W * (W / S::TY), kGrowthThreads, smem, st>>>(jobs, tw, lut, A, H, U, BACK, Udbg, err);
-    return cudaGetLastError();
+    if constexpr (W % kGwRowsBlock == 0 && (kGwRows * W) % 32 == 0) {
+        using G = GrowthWarpShape<W>;
+        const size_t smem = G::smem(jobs.K, jobs.C);
+        cudaError_t e = smem_attr((const void *)k_growth_warp<W>, smem);
+        if (e != cudaSuccess) return e;
+        k_growth_warp<W><<<W * (W / kGwRowsBlock), kGwWarps * 32, smem, st>>>(jobs, tw, lut, A, H, U, BACK, Udbg,
+                                                                              err);
+        return cudaGetLastError();
+    } else {
+        using S = RowShape<W, true>;
+        const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2) + (size_t)256 * jobs.K * sizeof(float) +
+                            (size_t)jobs.C * S::T * sizeof(float);
+        cudaError_t e = smem_attr((const void *)k_growth_rows_s<W>, smem);
+        if (e != cudaSuccess) return e;
+        k_growth_rows_s<W><<<W * (W / S::TY), kGrowthThreads, smem, st>>>(jobs, tw, lut, A, H, U, BACK, Udbg, err);
+        return cudaGetLastError();
+    }
 }
 
 template <int W>

@@ -54,9 +54,10 @@ struct PadMat {
 
 // One Stockham stage.  COLS = false: NLINES rows of length N along the
 // matrix columns (contiguous); COLS = true: NLINES matrix columns of length N
-// along the rows.
-template <int N, int S, int NLINES, bool COLS, int NC, int THREADS>
-__device__ __forceinline__ void static_stage(float2 *buf, const float2 *tw, int sign)
+// along the rows.  THREADS threads with indices `tid` take part; WARP selects
+// a warp-scope barrier (the lines belong to one warp) instead of the block's.
+template <int N, int S, int NLINES, bool COLS, int NC, int THREADS, bool WARP>
+__device__ __forceinline__ void static_stage(float2 *buf, const float2 *tw, int sign, int tid)
 {
     constexpr int R = plan_radix(N, S);
     constexpr int NS = plan_ns(N, S);
@@ -68,7 +69,7 @@ __device__ __forceinline__ void static_stage(float2 *buf, const float2 *tw, int 
     float2 v[NB][R];
 #pragma unroll
     for (int i = 0; i < NB; i++) {
-        const int b = threadIdx.x + i * THREADS;
+        const int b = tid + i * THREADS;
         if (TOTAL % THREADS == 0 || b < TOTAL) {
             int l, j;
             if (COLS) { l = b % NLINES; j = b / NLINES; }
@@ -77,10 +78,11 @@ __device__ __forceinline__ void static_stage(float2 *buf, const float2 *tw, int 
             for (int r = 0; r < R; r++) v[i][r] = COLS ? buf[PM::at(j + r * M, l)] : buf[PM::at(l, j + r * M)];
         }
     }
-    __syncthreads();
+    if (WARP) __syncwarp();
+    else __syncthreads();
 #pragma unroll
     for (int i = 0; i < NB; i++) {
-        const int b = threadIdx.x + i * THREADS;
+        const int b = tid + i * THREADS;
         if (TOTAL % THREADS == 0 || b < TOTAL) {
             int l, j;
             if (COLS) { l = b % NLINES; j = b / NLINES; }
@@ -99,24 +101,33 @@ __device__ __forceinline__ void static_stage(float2 *buf, const float2 *tw, int 
             }
         }
     }
-    __syncthreads();
+    if (WARP) __syncwarp();
+    else __syncthreads();
 }
 
-template <int N, int S, int NLINES, bool COLS, int NC, int THREADS>
-__device__ __forceinline__ void static_stages(float2 *buf, const float2 *tw, int sign)
+template <int N, int S, int NLINES, bool COLS, int NC, int THREADS, bool WARP>
+__device__ __forceinline__ void static_stages(float2 *buf, const float2 *tw, int sign, int tid)
 {
     if constexpr (S < plan_count(N)) {
-        static_stage<N, S, NLINES, COLS, NC, THREADS>(buf, tw, sign);
-        static_stages<N, S + 1, NLINES, COLS, NC, THREADS>(buf, tw, sign);
+        static_stage<N, S, NLINES, COLS, NC, THREADS, WARP>(buf, tw, sign, tid);
+        static_stages<N, S + 1, NLINES, COLS, NC, THREADS, WARP>(buf, tw, sign, tid);
     }
 }
 
-// Whole transform of NLINES lines held in a PadMat<NC>.
+// Whole transform of NLINES lines held in a PadMat<NC>, by the whole block.
 template <int N, int NLINES, bool COLS, int NC, int THREADS>
 __device__ __forceinline__ void static_fft(float2 *buf, const float2 *tw, int sign)
 {
     static_assert(plan_count(N) > 0, "unsupported transform length");
-    static_stages<N, 0, NLINES, COLS, NC, THREADS>(buf, tw, sign);
+    static_stages<N, 0, NLINES, COLS, NC, THREADS, false>(buf, tw, sign, threadIdx.x);
+}
+
+// Whole transform of NLINES rows owned by one warp (lane = threadIdx.x & 31).
+template <int N, int NLINES, int NC>
+__device__ __forceinline__ void warp_fft_rows(float2 *buf, const float2 *tw, int sign)
+{
+    static_assert(plan_count(N) > 0, "unsupported transform length");
+    static_stages<N, 0, NLINES, false, NC, 32, true>(buf, tw, sign, threadIdx.x & 31);
 }
 
 // Largest divisor of n not above 16: rows per tile of the row kernels.
