@@ -286,7 +286,8 @@ constexpr int kGwWarps = 8, kGwRows = 2, kGwRowsBlock = kGwWarps * kGwRows;
 template <int W>
 struct GrowthWarpShape {
     static constexpr int KX = W / 2 + 1;
-    static constexpr int STAGE = 2 * KX * kGwRowsBlock;          // float2 per staged pair
+    static constexpr int SP = kGwRowsBlock + 2;                   // staged row pitch (bank-conflict free)
+    static constexpr int STAGE = 2 * KX * SP;                     // float2 per staged pair
     static constexpr int CELLS = kGwRows * W / 32;                // cells per lane
     using PM = PadMat<W>;
     static constexpr int ZW = PM::RP * kGwRows;                   // float2 per warp row buffer
@@ -328,13 +329,13 @@ __global__ void __launch_bounds__(kGwWarps * 32) k_growth_warp(GrowthJobs jobs, 
 
     auto issue = [&](int k0, int buf) {
         float2 *dst = stage + buf * S::STAGE;
-        for (int e = threadIdx.x; e < S::STAGE; e += kGwWarps * 32) {
+        for (int e = threadIdx.x; e < 2 * KX * RB; e += kGwWarps * 32) {
             const int q = e / (KX * RB), rem = e % (KX * RB);
             const int kx = rem / RB, ty = rem % RB;
             const int k = k0 + q;
             const bool ok = k < K;
             const float2 *src = ok ? jobs.spec[k] + ((long long)kx * D + z) * H + y0 + ty : jobs.spec[k0];
-            cp_async_f64(dst + e, src, ok);
+            cp_async_f64(dst + (q * KX + kx) * S::SP + ty, src, ok);
         }
         cp_async_commit();
     };
@@ -361,8 +362,8 @@ __global__ void __launch_bounds__(kGwWarps * 32) k_growth_warp(GrowthJobs jobs, 
             const int e = lane + 32 * i;
             const int r = e % kGwRows, kx = e / kGwRows;
             const int m = kx < KX ? kx : W - kx;
-            const float2 a = st[m * RB + yw + r];
-            const float2 b = st[KX * RB + m * RB + yw + r];
+            const float2 a = st[m * S::SP + yw + r];
+            const float2 b = st[(KX + m) * S::SP + yw + r];
             float2 v;
             if (kx < KX) v = make_float2(a.x - b.y, a.y + b.x);
             else v = make_float2(a.x + b.y, b.x - a.y);
@@ -480,7 +481,11 @@ template <int W>
 cudaError_t growth_rows_w(const float2 *tw, const GrowthJobs &jobs, const float *lut, const float *A, float *H,
                           float *U, float *BACK, float *Udbg, int *err, cudaStream_t st)
 {
+#ifndef LENIA_GROWTH_BLOCK
     if constexpr (W % kGwRowsBlock == 0 && (kGwRows * W) % 32 == 0) {
+#else
+    if constexpr (false) {
+#endif
         using G = GrowthWarpShape<W>;
         const size_t smem = G::smem(jobs.K, jobs.C);
         cudaError_t e = smem_attr((const void *)k_growth_warp<W>, smem);
