@@ -187,6 +187,18 @@ int lenia_profile_read(lenia_world *w, double *ms, long long *launches, int n);
 /* Name of kernel id `kid` of lenia_profile_read (NULL past the last). */
 const char *lenia_kernel_name(int kid);
 
+/* No counterpart in the reference.  u_out = Re(IFFT(FFT(field) * K^))/N for
+ * one field and one kernel, computed exactly as a world's growth stage computes
+ * u for that kernel, for callers that cannot allocate device memory: every
+ * intermediate buffer lives in one fixed __device__ array (about 3.4 MB per
+ * GPU, held until exit), so this call allocates nothing.  field and u_out are
+ * device pointers of width*height*width floats; grids up to 64^3 are accepted
+ * (larger ones return LENIA_ERR_INVALID_ARG).  Calls share that array, so
+ * calls that overlap on the GPU race; the first call on a device looks up the
+ * array's address (cudaGetSymbolAddress) with that device current. */
+lenia_status lenia_convolve_noalloc(int width, int height, const float *field, const LeniaKernelParams *kernel,
+                                    float *u_out, void *stream);
+
 /* Number of kernel launches the last lenia_step issued per step. */
 int lenia_launches_per_step(const lenia_world *w);
 /* Human-readable description of the last failure on w (never NULL). */

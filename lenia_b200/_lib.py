@@ -117,6 +117,8 @@ def load() -> ctypes.CDLL:
         "lenia_profile_read": ([P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
                                 ctypes.c_int], ctypes.c_int),
         "lenia_kernel_name": ([ctypes.c_int], ctypes.c_char_p),
+        "lenia_convolve_noalloc": ([ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(LeniaKernelParams),
+                                    ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
         "lenia_last_error": ([P], ctypes.c_char_p),
         "lenia_version": ([], ctypes.c_char_p),
     }
