@@ -56,6 +56,17 @@ class LeniaKernelParams(ctypes.Structure):
     ]
 
 
+class LeniaMeshDesc(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_int), ("height", ctypes.c_int), ("channels", ctypes.c_int),
+        ("iso_value", ctypes.c_float), ("cell_size", ctypes.c_float), ("x_offset", ctypes.c_float),
+        ("slabs", ctypes.c_int), ("share_channels", ctypes.c_int),
+    ]
+
+
+MESH_ARRAY = {"positions": 0, "normals": 1, "vertex_channel": 2, "indices": 3, "face_normals": 4, "cases": 5}
+
+
 def to_c_desc(desc: WorldDesc) -> LeniaWorldDesc:
     d = desc.as_dict()
     c = LeniaWorldDesc()
@@ -119,6 +130,15 @@ def load() -> ctypes.CDLL:
         "lenia_kernel_name": ([ctypes.c_int], ctypes.c_char_p),
         "lenia_convolve_noalloc": ([ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(LeniaKernelParams),
                                     ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+        "lenia_mesher_create": ([ctypes.POINTER(LeniaMeshDesc), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+        "lenia_mesher_destroy": ([P], ctypes.c_int),
+        "lenia_mesher_run": ([P, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
+                              ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+        "lenia_mesher_get": ([P, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int], ctypes.c_int),
+        "lenia_mesh_world": ([P, ctypes.c_int, P, ctypes.POINTER(ctypes.c_longlong),
+                              ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+        "lenia_mc_triangle_table": ([ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+        "lenia_mesher_last_error": ([P], ctypes.c_char_p),
         "lenia_last_error": ([P], ctypes.c_char_p),
         "lenia_version": ([], ctypes.c_char_p),
     }

@@ -1,0 +1,849 @@
+// Marching cubes: generate_mesh_v1 (mesh.cpp:34-431) with the buffer reset
+// and concatenation around it (render.cpp:153-212), as five launches.
+//
+// The reference creates vertices in a fixed order: slab (mesh thread), then
+// channel, then cube (x fastest), then triangle slot; an edge's vertex is
+// created by the first triangle slot that names the edge (its vertex map,
+// V1_EDGES, is keyed by edge origin and axis, per slab), and every triangle
+// that names the edge adds its face normal to it.  On the GPU:
+//
+//   mc_count    per cube and channel: case index, triangle count, and how many
+//               vertices the cube creates; per chunk of kMcThreads cubes the
+//               two sums;
+//   mc_scan     exclusive scan of the chunk sums (one block): each cube's first
+//               triangle and first created vertex;
+//   mc_emit     per cube: face normals of its triangles; position, channel and
+//               source edge of the vertices it creates;
+//   mc_index    per cube: the vertex of every triangle slot;
+//   mc_normals  per vertex: the face normals of the triangles that name its
+//               edge, summed in creation order.
+//
+// No atomics and no edge-keyed map: the cube that creates an edge's vertex is
+// the edge's first neighbouring cube in scan order within the slab (every
+// neighbour of an intersected edge has triangles on it), in the first channel
+// where the edge is intersected when channels share vertices.  Each cube
+// therefore knows which vertices it creates, and the creator of any edge, and
+// the rank of the vertex among the creator's, follow from the stored case
+// indices.  Every value is computed with the reference's operations in its
+// order, so the result is bit-identical to a sequential run.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+
+#include "lenia_internal.h"
+
+namespace {
+
+constexpr int kMcThreads = 256;          // threads per block = cubes per chunk
+constexpr int kMcWarps = kMcThreads / 32;
+constexpr int kMcMaxDim = 512;
+
+// ---- cube geometry (corner order of mesh.cpp:19-32) ----------------------
+// corner i: x = bit i of 0x66, y = i >= 4, z = bit i of 0xCC
+__host__ __device__ constexpr int mc_cx(int i) { return (0x66 >> i) & 1; }
+__host__ __device__ constexpr int mc_cy(int i) { return (i >> 2) & 1; }
+__host__ __device__ constexpr int mc_cz(int i) { return (0xCC >> i) & 1; }
+__host__ __device__ constexpr int mc_coord(int i, int d) { return d == 0 ? mc_cx(i) : d == 1 ? mc_cy(i) : mc_cz(i); }
+// edge e joins corners p and q: e < 4: e, e+1 mod 4; e < 8: e, 4 + (e-3) mod 4;
+// else e-8, e-4.  Its vertex is interpolated from the lower-numbered corner.
+__host__ __device__ constexpr int mc_p(int e) { return e < 8 ? e : e - 8; }
+__host__ __device__ constexpr int mc_q(int e) { return e < 4 ? ((e + 1) & 3) : e < 8 ? 4 + ((e - 3) & 3) : e - 4; }
+__host__ __device__ constexpr int mc_a(int e) { return mc_p(e) < mc_q(e) ? mc_p(e) : mc_q(e); }
+__host__ __device__ constexpr int mc_b(int e) { return mc_p(e) < mc_q(e) ? mc_q(e) : mc_p(e); }
+__host__ __device__ constexpr int mc_axis(int e)
+{
+    return mc_cx(mc_a(e)) != mc_cx(mc_b(e)) ? 0 : mc_cy(mc_a(e)) != mc_cy(mc_b(e)) ? 1 : 2;
+}
+// origin of edge e relative to its cube, coordinate d
+__host__ __device__ constexpr int mc_off(int e, int d)
+{
+    return mc_coord(mc_a(e), d) < mc_coord(mc_b(e), d) ? mc_coord(mc_a(e), d) : mc_coord(mc_b(e), d);
+}
+// The four cubes around a grid edge of axis `ax`, in scan order (z, then y,
+// then x ascending): the cube that has the edge as its local edge e sits at
+// the edge origin minus mc_off(e), so the order is descending (oz, oy, ox).
+__host__ __device__ constexpr int mc_axis_edge(int ax, int j)
+{
+    for (int e = 0; e < 12; e++) {
+        if (mc_axis(e) != ax) continue;
+        const int key = mc_off(e, 2) * 4 + mc_off(e, 1) * 2 + mc_off(e, 0);
+        int rank = 0;
+        for (int f = 0; f < 12; f++)
+            if (mc_axis(f) == ax && mc_off(f, 2) * 4 + mc_off(f, 1) * 2 + mc_off(f, 0) > key) rank++;
+        if (rank == j) return e;
+    }
+    return -1;
+}
+
+// Edge descriptor: a | b << 3 | axis << 6 | ox << 8 | oy << 9 | oz << 10.
+__host__ __device__ constexpr unsigned mc_edge_desc(int e)
+{
+    return (unsigned)(mc_a(e) | mc_b(e) << 3 | mc_axis(e) << 6 | mc_off(e, 0) << 8 | mc_off(e, 1) << 9 |
+                      mc_off(e, 2) << 10);
+}
+
+__device__ __forceinline__ unsigned active_edges(int cs)
+{
+    unsigned m = 0;
+#pragma unroll
+    for (int e = 0; e < 12; e++) m |= (unsigned)(((cs >> mc_a(e)) ^ (cs >> mc_b(e))) & 1) << e;
+    return m;
+}
+
+// Tables shared by the kernels (copied to shared memory per block).
+struct McTables {
+    // per case: edge of slot k in bits 4k..4k+3 (k < 15), triangle count in bits 60..63
+    unsigned long long tri[256];
+    // per boundary class (see boundary_class): the edges whose vertex this cube creates
+    unsigned short owned[64];
+    unsigned edge[12];              // mc_edge_desc
+    unsigned char axis_edges[12];   // mc_axis_edge(ax, j) at 4 * ax + j
+};
+
+struct McGeom {
+    int W, H, D, C;
+    int slabs, nblk;  // z slabs; chunks per slab (of the largest slab)
+    long long N;
+    int share;
+    float iso, cell, xoff;
+};
+
+__device__ __forceinline__ int slot_edge(unsigned long long t, int k) { return (int)((t >> (4 * k)) & 15); }
+__device__ __forceinline__ int tri_count(unsigned long long t) { return (int)(t >> 60); }
+
+__device__ __forceinline__ void slab_range(const McGeom &g, int s, int &z0, int &z1)
+{
+    z0 = (g.D / g.slabs) * s;
+    z1 = s == g.slabs - 1 ? g.D : z0 + g.D / g.slabs;
+}
+
+// Which of the six slab boundaries cube (x, y, z) touches; the edges a cube
+// creates depend only on this.
+__device__ __forceinline__ int boundary_class(const McGeom &g, int x, int y, int z, int z0, int z1)
+{
+    return (x == 0) | (x == g.W - 1) << 1 | (y == 0) << 2 | (y == g.H - 1) << 3 | (z == z0) << 4 |
+           (z == z1 - 1) << 5;
+}
+
+// Corner values of cube (gx, gy, gz) of one channel.  Corners on the +1 faces
+// read the periodic copy; corners on two or three +1 faces (halo edges and
+// corners) read 0.
+__device__ __forceinline__ void load_corners(const float *f, const McGeom &g, int gx, int gy, int gz, float *v)
+{
+    const int W = g.W, WH = g.W * g.H;
+    if (gx + 1 < g.W && gy + 1 < g.H && gz + 1 < g.D) {
+        const float *p = f + gx + gy * W + (long long)gz * WH;
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[i] = __ldg(p + mc_cx(i) + mc_cy(i) * W + (long long)mc_cz(i) * WH);
+        return;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        int x = gx + mc_cx(i), y = gy + mc_cy(i), z = gz + mc_cz(i);
+        const int out = (x >= g.W) + (y >= g.H) + (z >= g.D);
+        if (x >= g.W) x -= g.W;
+        if (y >= g.H) y -= g.H;
+        if (z >= g.D) z -= g.D;
+        v[i] = out > 1 ? 0.0f : __ldg(f + x + y * W + (long long)z * WH);
+    }
+}
+
+__device__ __forceinline__ float sel8(const float *v, int i)
+{
+    const float a = (i & 1) ? v[1] : v[0], b = (i & 1) ? v[3] : v[2];
+    const float c = (i & 1) ? v[5] : v[4], d = (i & 1) ? v[7] : v[6];
+    const float ab = (i & 2) ? b : a, cd = (i & 2) ? d : c;
+    return (i & 4) ? cd : ab;
+}
+
+// Vertex on edge e of cube (gx, gy, gz): Pa + (Pb - Pa) * ((iso - va) / (vb - va))
+// with P = (g + delta) * cell (mesh.cpp:86-196), then x + x_offset.
+__device__ __forceinline__ float3 edge_vertex(const McGeom &g, unsigned ed, const float *v, int gx, int gy, int gz)
+{
+    const int a = ed & 7, b = (ed >> 3) & 7;
+    const float va = sel8(v, a), vb = sel8(v, b);
+    const float T = (g.iso - va) / (vb - va);
+    const float ax = ((float)gx + (float)mc_cx(a)) * g.cell, bx = ((float)gx + (float)mc_cx(b)) * g.cell;
+    const float ay = ((float)gy + (float)mc_cy(a)) * g.cell, by = ((float)gy + (float)mc_cy(b)) * g.cell;
+    const float az = ((float)gz + (float)mc_cz(a)) * g.cell, bz = ((float)gz + (float)mc_cz(b)) * g.cell;
+    float3 r;
+    r.x = ax + (bx - ax) * T;
+    r.y = ay + (by - ay) * T;
+    r.z = az + (bz - az) * T;
+    if (g.xoff != 0.0f) r.x = r.x + g.xoff;
+    return r;
+}
+
+__device__ __forceinline__ void load_tables(const McTables *src, McTables &dst)
+{
+    const unsigned *s = (const unsigned *)src;
+    unsigned *d = (unsigned *)&dst;
+    for (int i = threadIdx.x; i < (int)(sizeof(McTables) / 4); i += blockDim.x) d[i] = s[i];
+    __syncthreads();
+}
+
+// Exclusive scan over the block of packed counts (triangles in the low 16
+// bits, created vertices in the high 16); *total receives the block sum.
+__device__ __forceinline__ unsigned block_scan(unsigned v, unsigned *s_warp, unsigned *total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        unsigned w = lane < kMcWarps ? s_warp[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < kMcWarps; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < kMcWarps) s_warp[lane] = w;
+    }
+    __syncthreads();
+    const unsigned base = wid > 0 ? s_warp[wid - 1] : 0u;
+    *total = s_warp[kMcWarps - 1];
+    __syncthreads();
+    return base + x - v;
+}
+
+// Cube of chunk `chunk`, thread threadIdx.x: slab s, chunk b in the slab.
+struct CubeRef {
+    int s, b, z0, z1, gx, gy, gz;
+    long long p;
+    bool valid;
+};
+
+__device__ __forceinline__ CubeRef cube_of(const McGeom &g, int chunk)
+{
+    CubeRef r;
+    r.s = chunk / g.nblk;
+    r.b = chunk - r.s * g.nblk;
+    slab_range(g, r.s, r.z0, r.z1);
+    const long long WH = (long long)g.W * g.H;
+    const long long i = (long long)r.b * kMcThreads + threadIdx.x;
+    r.valid = i < WH * (r.z1 - r.z0);
+    r.p = r.z0 * WH + (r.valid ? i : 0);
+    r.gz = (int)(r.p / WH);
+    const int rem = (int)(r.p - r.gz * WH);
+    r.gy = rem / g.W;
+    r.gx = rem - r.gy * g.W;
+    return r;
+}
+
+__global__ void __launch_bounds__(kMcThreads) k_mc_count(const float *__restrict__ field, McGeom g,
+                                                        const McTables *__restrict__ tab,
+                                                        unsigned char *__restrict__ cases,
+                                                        long long *__restrict__ blk_tri,
+                                                        long long *__restrict__ blk_vert)
+{
+    __shared__ McTables s_tab;
+    __shared__ unsigned s_warp[kMcWarps];
+    load_tables(tab, s_tab);
+    const int nchunks = g.slabs * g.nblk;
+    for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+        const CubeRef q = cube_of(g, chunk);
+        const unsigned owned = q.valid ? s_tab.owned[boundary_class(g, q.gx, q.gy, q.gz, q.z0, q.z1)] : 0u;
+        unsigned prev = 0;
+        for (int c = 0; c < g.C; c++) {
+            int cs = 0;
+            if (q.valid) {
+                float v[8];
+                load_corners(field + c * g.N, g, q.gx, q.gy, q.gz, v);
+#pragma unroll
+                for (int i = 0; i < 8; i++) cs |= (v[i] > g.iso) << i;
+                cases[c * g.N + q.p] = (unsigned char)cs;
+            }
+            const unsigned act = active_edges(cs);
+            const unsigned nt = tri_count(s_tab.tri[cs]);
+            const unsigned nn = __popc(owned & act & ~prev);
+            if (g.share) prev |= act;
+            unsigned total;
+            block_scan(nt | nn << 16, s_warp, &total);
+            if (threadIdx.x == 0) {
+                const long long o = ((long long)q.s * g.C + c) * g.nblk + q.b;
+                blk_tri[o] = total & 0xffff;
+                blk_vert[o] = total >> 16;
+            }
+        }
+    }
+}
+
+// Exclusive scan of the chunk sums in place (one block of 1024 threads);
+// totals[0..1] = triangles, vertices.
+__global__ void __launch_bounds__(1024) k_mc_scan(long long *tri, long long *vert, long long M, long long *totals)
+{
+    __shared__ long long s_a[1024], s_b[1024];
+    const int t = threadIdx.x;
+    const long long per = (M + 1023) / 1024;
+    const long long beg = t * per, end = beg + per < M ? beg + per : M;
+    long long st = 0, sv = 0;
+    for (long long i = beg; i < end; i++) {
+        st += tri[i];
+        sv += vert[i];
+    }
+    s_a[t] = st;
+    s_b[t] = sv;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        const long long a = t >= o ? s_a[t - o] : 0, b = t >= o ? s_b[t - o] : 0;
+        __syncthreads();
+        s_a[t] += a;
+        s_b[t] += b;
+        __syncthreads();
+    }
+    long long ba = s_a[t] - st, bb = s_b[t] - sv;
+    for (long long i = beg; i < end; i++) {
+        const long long x = tri[i], y = vert[i];
+        tri[i] = ba;
+        vert[i] = bb;
+        ba += x;
+        bb += y;
+    }
+    if (t == 1023) {
+        totals[0] = s_a[t];
+        totals[1] = s_b[t];
+    }
+}
+
+__global__ void __launch_bounds__(kMcThreads) k_mc_emit(const float *__restrict__ field, McGeom g,
+                                                       const McTables *__restrict__ tab,
+                                                       const unsigned char *__restrict__ cases,
+                                                       const long long *__restrict__ blk_tri,
+                                                       const long long *__restrict__ blk_vert,
+                                                       int *__restrict__ tri_base, int *__restrict__ vert_base,
+                                                       float *__restrict__ fn, float *__restrict__ pos,
+                                                       int *__restrict__ vch, unsigned long long *__restrict__ vsrc)
+{
+    __shared__ McTables s_tab;
+    __shared__ unsigned s_warp[kMcWarps];
+    load_tables(tab, s_tab);
+    const int nchunks = g.slabs * g.nblk;
+    for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+        const CubeRef q = cube_of(g, chunk);
+        const unsigned owned = q.valid ? s_tab.owned[boundary_class(g, q.gx, q.gy, q.gz, q.z0, q.z1)] : 0u;
+        unsigned prev = 0;
+        for (int c = 0; c < g.C; c++) {
+            const int cs = q.valid ? cases[c * g.N + q.p] : 0;
+            const unsigned act = active_edges(cs);
+            const unsigned long long tl = s_tab.tri[cs];
+            const int nt = tri_count(tl);
+            const unsigned newm = owned & act & ~prev;
+            if (g.share) prev |= act;
+            unsigned total;
+            const unsigned pre = block_scan((unsigned)nt | (unsigned)__popc(newm) << 16, s_warp, &total);
+            if (nt == 0) continue;
+            const long long o = ((long long)q.s * g.C + c) * g.nblk + q.b;
+            const long long tb = blk_tri[o] + (pre & 0xffff);
+            const long long vb = blk_vert[o] + (pre >> 16);
+            tri_base[c * g.N + q.p] = (int)tb;
+            if (newm) vert_base[c * g.N + q.p] = (int)vb;
+            float v[8];
+            load_corners(field + c * g.N, g, q.gx, q.gy, q.gz, v);
+            for (int t = 0; t < nt; t++) {
+                const float3 A = edge_vertex(g, s_tab.edge[slot_edge(tl, 3 * t)], v, q.gx, q.gy, q.gz);
+                const float3 B = edge_vertex(g, s_tab.edge[slot_edge(tl, 3 * t + 1)], v, q.gx, q.gy, q.gz);
+                const float3 C = edge_vertex(g, s_tab.edge[slot_edge(tl, 3 * t + 2)], v, q.gx, q.gy, q.gz);
+                const float ux = B.x - A.x, uy = B.y - A.y, uz = B.z - A.z;
+                const float wx = C.x - A.x, wy = C.y - A.y, wz = C.z - A.z;
+                float *f = fn + 3 * (tb + t);
+                f[0] = uy * wz - uz * wy;
+                f[1] = uz * wx - ux * wz;
+                f[2] = ux * wy - uy * wx;
+            }
+            if (newm) {
+                unsigned seen = 0;
+                long long r = vb;
+                for (int k = 0; k < 3 * nt; k++) {
+                    const int e = slot_edge(tl, k);
+                    if ((seen >> e) & 1) continue;
+                    seen |= 1u << e;
+                    if (!((newm >> e) & 1)) continue;
+                    const float3 P = edge_vertex(g, s_tab.edge[e], v, q.gx, q.gy, q.gz);
+                    pos[3 * r] = P.x;
+                    pos[3 * r + 1] = P.y;
+                    pos[3 * r + 2] = P.z;
+                    vch[r] = c;
+                    vsrc[r] = (unsigned long long)(c * g.N + q.p) << 4 | (unsigned)e;
+                    r++;
+                }
+            }
+        }
+    }
+}
+
+// Creator of the vertex on local edge e of cube (gx, gy, gz): the first cube
+// around the edge in scan order inside the slab.  Returns the creator's
+// linear index and its local edge.
+__device__ __forceinline__ long long edge_creator(const McGeom &g, const McTables &t, int e, int gx, int gy, int gz,
+                                                  int z0, int z1, int *e_out)
+{
+    const unsigned ed = t.edge[e];
+    const int ax = (ed >> 6) & 3;
+    const int Gx = gx + ((ed >> 8) & 1), Gy = gy + ((ed >> 9) & 1), Gz = gz + ((ed >> 10) & 1);
+    for (int j = 0; j < 4; j++) {
+        const int e2 = t.axis_edges[4 * ax + j];
+        const unsigned d2 = t.edge[e2];
+        const int x = Gx - (int)((d2 >> 8) & 1), y = Gy - (int)((d2 >> 9) & 1), z = Gz - (int)((d2 >> 10) & 1);
+        if (x >= 0 && x < g.W && y >= 0 && y < g.H && z >= z0 && z < z1) {
+            *e_out = e2;
+            return x + (long long)y * g.W + (long long)z * g.W * g.H;
+        }
+    }
+    *e_out = e;  // unreachable: the cube itself is always a candidate
+    return gx + (long long)gy * g.W + (long long)gz * g.W * g.H;
+}
+
+__global__ void __launch_bounds__(kMcThreads) k_mc_index(McGeom g, const McTables *__restrict__ tab,
+                                                        const unsigned char *__restrict__ cases,
+                                                        const int *__restrict__ tri_base,
+                                                        const int *__restrict__ vert_base,
+                                                        unsigned *__restrict__ idx)
+{
+    __shared__ McTables s_tab;
+    load_tables(tab, s_tab);
+    const int nchunks = g.slabs * g.nblk;
+    const long long WH = (long long)g.W * g.H;
+    for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+        const CubeRef q = cube_of(g, chunk);
+        if (!q.valid) continue;
+        for (int c = 0; c < g.C; c++) {
+            const int cs = cases[c * g.N + q.p];
+            const unsigned long long tl = s_tab.tri[cs];
+            const int nt = tri_count(tl);
+            if (nt == 0) continue;
+            const long long tb = tri_base[c * g.N + q.p];
+            for (int k = 0; k < 3 * nt; k++) {
+                const int e = slot_edge(tl, k);
+                // channel that created the vertex
+                int c0 = c;
+                if (g.share)
+                    for (int c2 = 0; c2 < c; c2++)
+                        if ((active_edges(cases[c2 * g.N + q.p]) >> e) & 1) {
+                            c0 = c2;
+                            break;
+                        }
+                int eo;
+                const long long op = edge_creator(g, s_tab, e, q.gx, q.gy, q.gz, q.z0, q.z1, &eo);
+                const int oz = (int)(op / WH), rem = (int)(op - oz * WH);
+                const int oy = rem / g.W, ox = rem - oy * g.W;
+                const int ocs = cases[c0 * g.N + op];
+                unsigned oprev = 0;
+                if (g.share)
+                    for (int c2 = 0; c2 < c0; c2++) oprev |= active_edges(cases[c2 * g.N + op]);
+                const unsigned onew =
+                    s_tab.owned[boundary_class(g, ox, oy, oz, q.z0, q.z1)] & active_edges(ocs) & ~oprev;
+                // rank of eo among the creator's new vertices, in first-slot order
+                const unsigned long long otl = s_tab.tri[ocs];
+                unsigned seen = 0;
+                int r = 0;
+                for (int k2 = 0; k2 < 3 * tri_count(otl); k2++) {
+                    const int e2 = slot_edge(otl, k2);
+                    if ((seen >> e2) & 1) continue;
+                    seen |= 1u << e2;
+                    if (e2 == eo) break;
+                    r += (onew >> e2) & 1;
+                }
+                idx[3 * tb + k] = (unsigned)(vert_base[c0 * g.N + op] + r);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kMcThreads) k_mc_normals(McGeom g, const McTables *__restrict__ tab,
+                                                          const unsigned char *__restrict__ cases,
+                                                          const int *__restrict__ tri_base,
+                                                          const unsigned long long *__restrict__ vsrc,
+                                                          const float *__restrict__ fn, float *__restrict__ nrm,
+                                                          long long nv)
+{
+    __shared__ McTables s_tab;
+    load_tables(tab, s_tab);
+    const long long WH = (long long)g.W * g.H;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nv;
+         v += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long src = vsrc[v];
+        const int e0 = (int)(src & 15);
+        const long long cp = (long long)(src >> 4);
+        const int c0 = (int)(cp / g.N);
+        const long long p0 = cp - c0 * g.N;
+        const int gz = (int)(p0 / WH), rem = (int)(p0 - gz * WH);
+        const int gy = rem / g.W, gx = rem - gy * g.W;
+        int s = gz / (g.D / g.slabs);
+        if (s > g.slabs - 1) s = g.slabs - 1;
+        int z0, z1;
+        slab_range(g, s, z0, z1);
+        const unsigned ed = s_tab.edge[e0];
+        const int ax = (ed >> 6) & 3;
+        const int Gx = gx + ((ed >> 8) & 1), Gy = gy + ((ed >> 9) & 1), Gz = gz + ((ed >> 10) & 1);
+        float nx = 0.0f, ny = 0.0f, nz = 0.0f;
+        const int c_end = g.share ? g.C : c0 + 1;
+        for (int c = c0; c < c_end; c++) {
+            if (c > c0 && !((active_edges(cases[c * g.N + p0]) >> e0) & 1)) continue;
+            for (int j = 0; j < 4; j++) {
+                const int e2 = s_tab.axis_edges[4 * ax + j];
+                const unsigned d2 = s_tab.edge[e2];
+                const int x = Gx - (int)((d2 >> 8) & 1), y = Gy - (int)((d2 >> 9) & 1),
+                          z = Gz - (int)((d2 >> 10) & 1);
+                if (x < 0 || x >= g.W || y < 0 || y >= g.H || z < z0 || z >= z1) continue;
+                const long long qp = x + (long long)y * g.W + (long long)z * WH;
+                const unsigned long long tl = s_tab.tri[cases[c * g.N + qp]];
+                const int nt = tri_count(tl);
+                const long long tb = tri_base[c * g.N + qp];
+                for (int t = 0; t < nt; t++) {
+                    if (slot_edge(tl, 3 * t) == e2 || slot_edge(tl, 3 * t + 1) == e2 ||
+                        slot_edge(tl, 3 * t + 2) == e2) {
+                        const float *f = fn + 3 * (tb + t);
+                        nx += f[0];
+                        ny += f[1];
+                        nz += f[2];
+                    }
+                }
+            }
+        }
+        nrm[3 * v] = nx;
+        nrm[3 * v + 1] = ny;
+        nrm[3 * v + 2] = nz;
+    }
+}
+
+// ---- host: the triangle table --------------------------------------------
+//
+// Polygons of a case: on each cube face the intersected edges pair into
+// segments (two intersected edges: one segment; four: the face is ambiguous
+// and each of its two inside corners, value > iso, is cut off by the segment
+// between its two edges); the segments link into closed loops, each walked
+// from its lowest edge towards the lower of that edge's two neighbours and
+// cut into a fan of triangles from its first edge.  This resolves every
+// ambiguous face the same way the reference's table does (same triangle
+// count in all 256 cases).
+int case_triangles(int cs, int *tri)
+{
+    int nb[12][2], deg[12] = {0};
+    for (int ax = 0; ax < 3; ax++)
+        for (int side = 0; side <= 1; side++) {
+            int act[4], na = 0;
+            for (int e = 0; e < 12; e++) {
+                const int a = mc_a(e), b = mc_b(e);
+                if (mc_coord(a, ax) == side && mc_coord(b, ax) == side && (((cs >> a) ^ (cs >> b)) & 1))
+                    act[na++] = e;
+            }
+            int seg[2][2], ns = 0;
+            if (na == 2) {
+                seg[0][0] = act[0];
+                seg[0][1] = act[1];
+                ns = 1;
+            } else if (na == 4) {
+                for (int k = 0; k < 8; k++) {
+                    if (mc_coord(k, ax) != side || !((cs >> k) & 1)) continue;
+                    int m = 0;
+                    for (int i = 0; i < 4; i++)
+                        if (mc_a(act[i]) == k || mc_b(act[i]) == k) seg[ns][m++] = act[i];
+                    ns++;
+                }
+            }
+            for (int i = 0; i < ns; i++) {
+                const int a = seg[i][0], b = seg[i][1];
+                nb[a][deg[a]++] = b;
+                nb[b][deg[b]++] = a;
+            }
+        }
+    bool visited[12] = {false};
+    int nt = 0;
+    for (int s = 0; s < 12; s++) {
+        if (deg[s] == 0 || visited[s]) continue;
+        int loop[12], n = 0, prev = -1, cur = s;
+        for (;;) {
+            loop[n++] = cur;
+            visited[cur] = true;
+            const int nx = prev < 0 ? (nb[cur][0] < nb[cur][1] ? nb[cur][0] : nb[cur][1])
+                                    : (nb[cur][0] == prev ? nb[cur][1] : nb[cur][0]);
+            if (nx == s) break;
+            prev = cur;
+            cur = nx;
+        }
+        for (int i = 1; i + 1 < n; i++) {
+            tri[3 * nt] = loop[0];
+            tri[3 * nt + 1] = loop[i];
+            tri[3 * nt + 2] = loop[i + 1];
+            nt++;
+        }
+    }
+    return nt;
+}
+
+// The edges a cube creates, per boundary class: those whose first
+// neighbouring cube in scan order (inside the slab) is this cube.
+unsigned short owned_edges(int cls)
+{
+    const bool lo[3] = {(cls & 1) != 0, (cls & 4) != 0, (cls & 16) != 0};
+    const bool hi[3] = {(cls & 2) != 0, (cls & 8) != 0, (cls & 32) != 0};
+    unsigned short m = 0;
+    for (int e = 0; e < 12; e++) {
+        const int ax = mc_axis(e);
+        for (int j = 0; j < 4; j++) {
+            const int e2 = mc_axis_edge(ax, j);
+            bool ok = true;
+            for (int d = 0; d < 3; d++) {
+                const int delta = mc_off(e, d) - mc_off(e2, d);  // neighbour = this cube + delta
+                if ((delta < 0 && lo[d]) || (delta > 0 && hi[d])) ok = false;
+            }
+            if (ok) {
+                if (e2 == e) m |= (unsigned short)(1u << e);
+                break;
+            }
+        }
+    }
+    return m;
+}
+
+void build_tables(McTables *t)
+{
+    memset(t, 0, sizeof(*t));
+    for (int cs = 0; cs < 256; cs++) {
+        int tri[15];
+        const int n = case_triangles(cs, tri);
+        unsigned long long w = (unsigned long long)n << 60;
+        for (int k = 0; k < 3 * n; k++) w |= (unsigned long long)tri[k] << (4 * k);
+        t->tri[cs] = w;
+    }
+    for (int cls = 0; cls < 64; cls++) t->owned[cls] = owned_edges(cls);
+    for (int e = 0; e < 12; e++) t->edge[e] = mc_edge_desc(e);
+    for (int ax = 0; ax < 3; ax++)
+        for (int j = 0; j < 4; j++) t->axis_edges[4 * ax + j] = (unsigned char)mc_axis_edge(ax, j);
+}
+
+}  // namespace
+
+struct lenia_mesher {
+    LeniaMeshDesc desc;
+    McGeom g;
+    int device = 0;
+    int grid = 0;
+    std::string err;
+    McTables *tab = nullptr;
+    unsigned char *cases = nullptr;
+    int *tri_base = nullptr, *vert_base = nullptr;
+    long long *blk_tri = nullptr, *blk_vert = nullptr, *totals = nullptr, *h_totals = nullptr;
+    float *fn = nullptr, *pos = nullptr, *nrm = nullptr;
+    int *vch = nullptr;
+    unsigned long long *vsrc = nullptr;
+    unsigned *idx = nullptr;
+    long long cap_t = 0, cap_v = 0, n_t = 0, n_v = 0;
+    bool have_mesh = false;
+    cudaStream_t stream = nullptr;
+};
+
+namespace {
+
+lenia_status mfail(lenia_mesher *m, lenia_status s, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (m) m->err = buf;
+    return s;
+}
+
+lenia_status mcuda(lenia_mesher *m, cudaError_t e, const char *where)
+{
+    return mfail(m, e == cudaErrorMemoryAllocation ? LENIA_ERR_OOM : LENIA_ERR_CUDA, "%s: %s", where,
+                 cudaGetErrorString(e));
+}
+
+template <typename T>
+void dfree(T *&p)
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+void free_outputs(lenia_mesher *m)
+{
+    dfree(m->fn);
+    dfree(m->idx);
+    dfree(m->pos);
+    dfree(m->nrm);
+    dfree(m->vch);
+    dfree(m->vsrc);
+    m->cap_t = m->cap_v = 0;
+}
+
+}  // namespace
+
+namespace lenia {
+long long mesher_field_floats(const lenia_mesher *m) { return m ? (long long)m->g.C * m->g.N : 0; }
+cudaStream_t mesher_stream(const lenia_mesher *m) { return m ? m->stream : nullptr; }
+}  // namespace lenia
+
+extern "C" {
+
+int lenia_mc_triangle_table(int *table)
+{
+    if (!table) return -1;
+    for (int cs = 0; cs < 256; cs++) {
+        int tri[15];
+        const int n = case_triangles(cs, tri);
+        for (int k = 0; k < 16; k++) table[cs * 16 + k] = k < 3 * n ? tri[k] : -1;
+    }
+    return 0;
+}
+
+lenia_status lenia_mesher_create(const LeniaMeshDesc *desc, lenia_mesher **out)
+{
+    if (!desc || !out) return LENIA_ERR_INVALID_ARG;
+    *out = nullptr;
+    const LeniaMeshDesc &d = *desc;
+    if (d.width < 2 || d.width > kMcMaxDim || d.height < 2 || d.height > kMcMaxDim || d.channels < 1 ||
+        d.channels > LENIA_MAX_CHANNELS || d.slabs < 1 || d.slabs > d.width || !(d.cell_size > 0.0f))
+        return LENIA_ERR_INVALID_ARG;
+    int dev = 0, nsm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return LENIA_ERR_NO_DEVICE;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return LENIA_ERR_NO_DEVICE;
+    lenia_mesher *m = new lenia_mesher();
+    m->desc = d;
+    m->device = dev;
+    McGeom &g = m->g;
+    g.W = d.width;
+    g.H = d.height;
+    g.D = d.width;
+    g.C = d.channels;
+    g.N = (long long)g.W * g.H * g.D;
+    g.slabs = d.slabs;
+    const long long largest = (long long)g.W * g.H * (g.D - (g.D / g.slabs) * (g.slabs - 1));
+    g.nblk = (int)((largest + kMcThreads - 1) / kMcThreads);
+    g.share = d.share_channels != 0;
+    g.iso = d.iso_value;
+    g.cell = d.cell_size;
+    g.xoff = d.x_offset;
+    const long long nchunks = (long long)g.slabs * g.nblk;
+    m->grid = (int)(nchunks < 8LL * nsm ? nchunks : 8LL * nsm);
+    const long long M = nchunks * g.C;
+    McTables host;
+    build_tables(&host);
+    cudaError_t e = cudaSuccess;
+    auto alloc = [&](auto *&p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc((void **)&p, bytes);
+    };
+    alloc(m->tab, sizeof(McTables));
+    alloc(m->cases, (size_t)g.C * g.N);
+    alloc(m->tri_base, sizeof(int) * (size_t)g.C * g.N);
+    alloc(m->vert_base, sizeof(int) * (size_t)g.C * g.N);
+    alloc(m->blk_tri, sizeof(long long) * (size_t)M);
+    alloc(m->blk_vert, sizeof(long long) * (size_t)M);
+    alloc(m->totals, 2 * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&m->h_totals, 2 * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMemcpy(m->tab, &host, sizeof(McTables), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        lenia_mesher_destroy(m);
+        return e == cudaErrorMemoryAllocation ? LENIA_ERR_OOM : LENIA_ERR_CUDA;
+    }
+    *out = m;
+    return LENIA_OK;
+}
+
+lenia_status lenia_mesher_destroy(lenia_mesher *m)
+{
+    if (!m) return LENIA_ERR_INVALID_ARG;
+    // cudaFree waits for the device; the last run's stream may be gone already
+    free_outputs(m);
+    dfree(m->tab);
+    dfree(m->cases);
+    dfree(m->tri_base);
+    dfree(m->vert_base);
+    dfree(m->blk_tri);
+    dfree(m->blk_vert);
+    dfree(m->totals);
+    if (m->h_totals) cudaFreeHost(m->h_totals);
+    delete m;
+    return LENIA_OK;
+}
+
+lenia_status lenia_mesher_run(lenia_mesher *m, const float *field, void *stream, long long *n_vertices,
+                              long long *n_triangles)
+{
+    if (!m || !field) return LENIA_ERR_INVALID_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    m->stream = st;
+    m->have_mesh = false;
+    const McGeom &g = m->g;
+    const long long M = (long long)g.slabs * g.nblk * g.C;
+    k_mc_count<<<m->grid, kMcThreads, 0, st>>>(field, g, m->tab, m->cases, m->blk_tri, m->blk_vert);
+    k_mc_scan<<<1, 1024, 0, st>>>(m->blk_tri, m->blk_vert, M, m->totals);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m->h_totals, m->totals, 2 * sizeof(long long), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return mcuda(m, e, "mesher count");
+    const long long nt = m->h_totals[0], nv = m->h_totals[1];
+    if (3 * nt > 0xffffffffLL || nv > 0x7fffffffLL)
+        return mfail(m, LENIA_ERR_UNSUPPORTED, "mesh of %lld triangles exceeds 32-bit indices", nt);
+    if (nt > m->cap_t || nv > m->cap_v) {
+        const long long ct = nt > m->cap_t ? nt + nt / 4 + 1024 : m->cap_t;
+        const long long cv = nv > m->cap_v ? nv + nv / 4 + 1024 : m->cap_v;
+        free_outputs(m);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&m->fn, sizeof(float) * 3 * ct);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&m->idx, sizeof(unsigned) * 3 * ct);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&m->pos, sizeof(float) * 3 * cv);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&m->nrm, sizeof(float) * 3 * cv);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&m->vch, sizeof(int) * cv);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&m->vsrc, sizeof(unsigned long long) * cv);
+        if (e != cudaSuccess) {
+            free_outputs(m);
+            return mcuda(m, e, "mesher buffers");
+        }
+        m->cap_t = ct;
+        m->cap_v = cv;
+    }
+    if (nt > 0) {
+        k_mc_emit<<<m->grid, kMcThreads, 0, st>>>(field, g, m->tab, m->cases, m->blk_tri, m->blk_vert, m->tri_base,
+                                                  m->vert_base, m->fn, m->pos, m->vch, m->vsrc);
+        k_mc_index<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vert_base, m->idx);
+        const long long nb = (nv + kMcThreads - 1) / kMcThreads;
+        const int gn = (int)(nb < 64LL * m->grid ? (nb > 0 ? nb : 1) : 64LL * m->grid);
+        k_mc_normals<<<gn, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vsrc, m->fn, m->nrm, nv);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return mcuda(m, e, "mesher emit");
+    }
+    m->n_t = nt;
+    m->n_v = nv;
+    m->have_mesh = true;
+    if (n_vertices) *n_vertices = nv;
+    if (n_triangles) *n_triangles = nt;
+    return LENIA_OK;
+}
+
+lenia_status lenia_mesher_get(lenia_mesher *m, int which, void *dst, size_t count, int on_device)
+{
+    if (!m || !dst) return LENIA_ERR_INVALID_ARG;
+    if (!m->have_mesh) return mfail(m, LENIA_ERR_INVALID_ARG, "no mesh: run the mesher first");
+    const void *src = nullptr;
+    size_t n = 0, elem = 4;
+    switch (which) {
+    case LENIA_MESH_POSITIONS: src = m->pos; n = 3 * (size_t)m->n_v; break;
+    case LENIA_MESH_NORMALS: src = m->nrm; n = 3 * (size_t)m->n_v; break;
+    case LENIA_MESH_VERTEX_CHANNEL: src = m->vch; n = (size_t)m->n_v; break;
+    case LENIA_MESH_INDICES: src = m->idx; n = 3 * (size_t)m->n_t; break;
+    case LENIA_MESH_FACE_NORMALS: src = m->fn; n = 3 * (size_t)m->n_t; break;
+    case LENIA_MESH_CASES: src = m->cases; n = (size_t)m->g.C * m->g.N; elem = 1; break;
+    default: return mfail(m, LENIA_ERR_INVALID_ARG, "unknown mesh array %d", which);
+    }
+    if (count != n) return mfail(m, LENIA_ERR_INVALID_ARG, "mesh array %d holds %zu elements, got %zu", which, n, count);
+    if (n == 0) return LENIA_OK;
+    cudaError_t e = cudaMemcpyAsync(dst, src, n * elem, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                    m->stream);
+    if (e == cudaSuccess && !on_device) e = cudaStreamSynchronize(m->stream);
+    if (e != cudaSuccess) return mcuda(m, e, "mesher get");
+    return LENIA_OK;
+}
+
+const char *lenia_mesher_last_error(const lenia_mesher *m) { return m ? m->err.c_str() : "null mesher"; }
+
+}  // extern "C"

@@ -929,6 +929,23 @@ int lenia_profile_read(lenia_world *w, double *ms, long long *launches, int n)
     return KID_MAX;
 }
 
+lenia_status lenia_mesh_world(lenia_world *w, int field, lenia_mesher *m, long long *n_vertices,
+                              long long *n_triangles)
+{
+    if (!w || !m) return LENIA_ERR_INVALID_ARG;
+    if (field != LENIA_FIELD_A && field != LENIA_FIELD_RBB && field != LENIA_FIELD_H_RB &&
+        field != LENIA_FIELD_U_SUM_RB && field != LENIA_FIELD_H && field != LENIA_FIELD_U_SUM)
+        return fail(w, LENIA_ERR_INVALID_ARG, "field %d cannot be meshed", field);
+    size_t n = 0;
+    const float *p = field_ptr(w, field, &n);
+    if (!p) return fail(w, LENIA_ERR_INVALID_ARG, "field %d is not available (enable snapshots?)", field);
+    if ((long long)n != mesher_field_floats(m))
+        return fail(w, LENIA_ERR_INVALID_ARG, "mesher shape does not match the world (%zu floats)", n);
+    const lenia_status s = lenia_mesher_run(m, p, w->stream, n_vertices, n_triangles);
+    if (s != LENIA_OK) return fail(w, s, "mesh: %s", lenia_mesher_last_error(m));
+    return LENIA_OK;
+}
+
 const char *lenia_kernel_name(int kid) { return kid >= 0 && kid < KID_MAX ? kKernelNames[kid] : nullptr; }
 
 int lenia_launches_per_step(const lenia_world *w) { return w ? w->launches : 0; }

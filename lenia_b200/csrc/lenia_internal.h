@@ -143,4 +143,7 @@ cudaError_t launch_blur_rows_fast(const Dims &d, const float2 *tw_x_inv, const B
 // Host FFT plans and twiddle tables (lenia_api.cu).
 int fft_factor(int n, int *radix);
 
+// Marching-cubes mesher (kernels_mesh.cu): floats of the field it meshes.
+long long mesher_field_floats(const lenia_mesher *m);
+
 }  // namespace lenia

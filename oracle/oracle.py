@@ -314,3 +314,91 @@ class RestateOracle(_Base):
     @classmethod
     def bell_lut(cls, m, s, u):
         return cls.lib().ora_bell_lut(m, s, u)
+
+
+class Mesh:
+    """A marching-cubes mesh as flat arrays: positions and normals (V x 3
+    float32), vertex channel (V int32, None from the reference build), indices
+    (3T uint32) and the case index of every cube (C x N uint8, or None)."""
+
+    def __init__(self, positions, normals, indices, vertex_channel=None, cases=None):
+        self.positions = positions
+        self.normals = normals
+        self.indices = indices
+        self.vertex_channel = vertex_channel
+        self.cases = cases
+
+    @property
+    def n_vertices(self):
+        return self.positions.shape[0]
+
+    @property
+    def n_triangles(self):
+        return self.indices.size // 3
+
+
+def mc_table(kind: str = "own") -> np.ndarray:
+    """256 x 16 triangle table (edge indices, -1 terminated).  "own" is the
+    restatement's table built from geometry (oracle/restate/mc_tables.c)."""
+    assert kind == "own"
+    lib = RestateOracle.lib()
+    t = np.zeros(256 * 16, dtype=np.int32)
+    lib.mc_own_table(t.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    return t.reshape(256, 16)
+
+
+def mesh_restated(field: np.ndarray, W: int, H: int, C: int, iso: float, cell: float = 3.5,
+                  x_offset: float = 0.0, table: np.ndarray | None = None, slabs: int = 1,
+                  share_channels: bool = False) -> Mesh:
+    """Marching cubes of the C-channel field (channel-major, x fastest) by the
+    restatement of generate_mesh_v1 (ora_mesh in oracle/restate/mc_tables.c)."""
+    lib = RestateOracle.lib()
+    f = np.ascontiguousarray(field, dtype=np.float32).ravel()
+    N = W * H * W
+    assert f.size >= C * N
+    tab = None
+    if table is not None:
+        tab = np.ascontiguousarray(table, dtype=np.int32).ravel()
+        assert tab.size == 256 * 16
+    cases = np.zeros(C * N, dtype=np.uint8)
+    cap_v = cap_i = 1024
+    while True:
+        pos = np.zeros(3 * cap_v, dtype=np.float32)
+        nrm = np.zeros(3 * cap_v, dtype=np.float32)
+        vch = np.zeros(cap_v, dtype=np.int32)
+        idx = np.zeros(cap_i, dtype=np.uint32)
+        fn = np.zeros(cap_i, dtype=np.float32)
+        nv, ni = ctypes.c_long(0), ctypes.c_long(0)
+        rc = lib.ora_mesh(_fp(f), ctypes.c_int(W), ctypes.c_int(H), ctypes.c_int(C), ctypes.c_float(iso),
+                          ctypes.c_float(cell), ctypes.c_float(x_offset),
+                          None if tab is None else tab.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                          ctypes.c_int(slabs), ctypes.c_int(1 if share_channels else 0),
+                          cases.ctypes.data_as(ctypes.c_void_p), _fp(pos), _fp(nrm),
+                          vch.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(cap_v),
+                          idx.ctypes.data_as(ctypes.c_void_p), _fp(fn), ctypes.c_long(cap_i),
+                          ctypes.byref(nv), ctypes.byref(ni))
+        if rc == 0:
+            break
+        cap_v, cap_i = max(nv.value, 1), max(ni.value, 1)
+    m = Mesh(pos[:3 * nv.value].reshape(-1, 3), nrm[:3 * nv.value].reshape(-1, 3), idx[:ni.value],
+             vch[:nv.value], cases.reshape(C, N))
+    m.face_normals = fn[:ni.value].reshape(-1, 3)
+    return m
+
+
+def mesh_reference(ref: "RefOracle") -> Mesh:
+    """The reference's own generate_mesh_v1 on its RBB snapshot (run the TMB
+    event first), both mesh threads concatenated, without stitching."""
+    lib = ref.lib()
+    cap_v = cap_i = 1024
+    while True:
+        pos = np.zeros(3 * cap_v, dtype=np.float32)
+        nrm = np.zeros(3 * cap_v, dtype=np.float32)
+        idx = np.zeros(cap_i, dtype=np.uint32)
+        nv, ni = ctypes.c_long(0), ctypes.c_long(0)
+        rc = lib.ref_mesh_v1(_fp(pos), _fp(nrm), ctypes.c_long(cap_v), idx.ctypes.data_as(ctypes.c_void_p),
+                             ctypes.c_long(cap_i), ctypes.byref(nv), ctypes.byref(ni))
+        if rc == 0:
+            break
+        cap_v, cap_i = max(nv.value, 1), max(ni.value, 1)
+    return Mesh(pos[:3 * nv.value].reshape(-1, 3), nrm[:3 * nv.value].reshape(-1, 3), idx[:ni.value])

@@ -479,4 +479,63 @@ void ref_get_spectrum(int c, float *out_complex)
     memcpy(out_complex, T[c], sizeof(fftwf_complex) * GRID_SIZE);
 }
 
+/* One mesh of the NORMAL view: the buffer reset of reset_mesh_generation
+ * (render.cpp:182-200), generate_mesh_v1 (mesh.cpp:34-431) for every mesh
+ * thread on RBB (filled by ORA_EV_TMB), and the concatenation of
+ * render.cpp:161-179 (thread order; indices offset by the vertices before
+ * them).  stitch_borders (main.cpp:101-163) is not run.  Writes positions and
+ * normals (3 floats per vertex) and indices; returns 0, or -1 when the output
+ * capacity is too small. */
+int ref_mesh_v1(float *pos, float *nrm, long max_v, unsigned *idx, long max_i, long *n_v, long *n_i)
+{
+    static Vertex *vbuf[MESH_THREADS];
+    static DWORD *ibuf[MESH_THREADS];
+    const long cap = 15L * GRID_WIDTH * GRID_HEIGHT * GRID_WIDTH * MAX_CHANNELS;
+    cur_buf = 0;
+    memset(V1_EDGES, -1, sizeof(V1_EDGES));
+    for (int t = 0; t < MESH_THREADS; t++) {
+        if (!vbuf[t]) {
+            vbuf[t] = (Vertex *)malloc(sizeof(Vertex) * cap);
+            ibuf[t] = (DWORD *)malloc(sizeof(DWORD) * cap);
+            if (!vbuf[t] || !ibuf[t]) return -1;
+        }
+        TD *td = &mesh_td[t];
+        td->id = t;
+        td->v = vbuf[t];
+        td->ib = ibuf[t];
+        td->vidx[cur_buf] = 0;
+        td->iidx[cur_buf] = 0;
+        td->lower_stitches = 0;
+        td->upper_stitches = 0;
+        memset(td->lower_border, -1, sizeof(td->lower_border));
+        memset(td->upper_border, -1, sizeof(td->upper_border));
+        memset(td->lower_indices, 0, sizeof(td->lower_indices));
+        memset(td->upper_indices, 0, sizeof(td->upper_indices));
+        generate_mesh_v1(td);
+    }
+    long nv = 0, ni = 0;
+    for (int t = 0; t < MESH_THREADS; t++) {
+        const TD *td = &mesh_td[t];
+        for (int i = 0; i < td->iidx[cur_buf]; i++) {
+            if (ni < max_i) idx[ni] = (unsigned)(td->ib[i] + nv);
+            ni++;
+        }
+        for (int i = 0; i < td->vidx[cur_buf]; i++) {
+            if (nv < max_v) {
+                const Vertex &v = td->v[i];
+                pos[3 * nv] = v._x;
+                pos[3 * nv + 1] = v._y;
+                pos[3 * nv + 2] = v._z;
+                nrm[3 * nv] = v._nx;
+                nrm[3 * nv + 1] = v._ny;
+                nrm[3 * nv + 2] = v._nz;
+            }
+            nv++;
+        }
+    }
+    *n_v = nv;
+    *n_i = ni;
+    return (nv > max_v || ni > max_i) ? -1 : 0;
+}
+
 }  /* extern "C" */

@@ -1,3 +1,22 @@
+/* Oracle test infrastructure: marching-cubes tables and restatement
+ * (mc_tables.c). */
 #ifndef LENIA_ORACLE_MC_TABLES_H
 #define LENIA_ORACLE_MC_TABLES_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+void mc_edge_corners(int e, int *a, int *b);
+int mc_edge_mask(int c);
+int mc_triangles(int c, int *tri);
+int mc_triangle_count(int c);
+void mc_own_table(int *table);
+int ora_mesh(const float *field, int W, int H, int C, float iso, float cell, float x_offset, const int *table,
+             int slabs, int share, unsigned char *cases, float *pos, float *nrm, int *vch, long max_v,
+             unsigned *idx, float *fnrm, long max_i, long *n_v, long *n_i);
+
+#ifdef __cplusplus
+}
+#endif
 #endif
