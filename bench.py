@@ -158,6 +158,31 @@ def kernel_bytes(wl) -> dict:
     }
 
 
+def step_bytes_per_cell(wl) -> int:
+    """Algorithmic HBM bytes per cell of one whole step: every field crosses
+    HBM once per producer-consumer edge (forward spectra C*8P with P = 2 passes
+    above 36 cells per side, inverse spectra K*(14 + 8(P-1)), stencil C*48 + 4,
+    reintegration C*20 + 4)."""
+    d = wl.desc
+    C, K = d.channels, len(wl.kernels)
+    P = 1 if max(d.width, d.height) <= 36 else 2
+    return C * 8 * P + K * (14 + 8 * (P - 1)) + C * 48 + 4 + C * 20 + 4
+
+
+def ncu_traffic(kernel: str):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
+    a kernel from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    try:
+        for line in open(path):
+            parts = line.split()
+            if len(parts) >= 2 and not line.startswith("#") and parts[0] == kernel:
+                return float(parts[1])
+    except OSError:
+        pass
+    return None
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -307,6 +332,28 @@ def run_ours(args):
     e2e = {"value": n * N * C * e2e_steps / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": h2d}
 
+    # marching cubes of the final grid, every channel at the reference's iso
+    # value, two slabs with a shared vertex map as the reference meshes; each
+    # mesh includes the one host synchronisation that sizes its output
+    from lenia_b200.mesh import Mesher
+    A_dev = torch.empty(C * N, dtype=torch.float32, device="cuda")
+    w.get("A", out=A_dev)
+    mesher = Mesher(wl.desc.width, wl.desc.height, C, iso_value=wl.desc.iso_value, slabs=2, share_channels=True)
+    for _ in range(3):
+        mesher.run(A_dev, stream.cuda_stream)
+    mesh_runs = 10
+    barrier()
+    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0.record(stream)
+    for _ in range(mesh_runs):
+        mesher.run(A_dev, stream.cuda_stream)
+    m1.record(stream)
+    barrier()
+    mesh_ms = m0.elapsed_time(m1) / mesh_runs
+    mesh = {"ms_per_mesh": mesh_ms, "cubes_per_s": C * N / (mesh_ms / 1000.0),
+            "vertices": mesher.n_vertices, "triangles": mesher.n_triangles, "gpu_launches_per_mesh": 5}
+    mesher.close()
+
     line = None
     if rank == 0:
         line = {
@@ -318,9 +365,15 @@ def run_ours(args):
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "roofline": {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": ncu_traffic(top_name),
                          "algorithmic_bytes_per_launch": kb.get(top_name)},
+            "step_roofline": {"bytes_per_cell": step_bytes_per_cell(wl),
+                              "achieved": step_bytes_per_cell(wl) * N * args.steps / (ms / 1000.0) / 1e9,
+                              "peak": peak, "unit": "GB/s",
+                              "frac": step_bytes_per_cell(wl) * N * args.steps / (ms / 1000.0) / 1e9 / peak},
             "kernels": kernels_table,
+            "mesh": mesh,
         }
         if n == 1 and not args.no_cpu_baseline:
             rate, dt = cpu_port_rate(wl, 2, 1)
