@@ -340,13 +340,13 @@ def run_ours(args):
     w.get("A", out=A_dev)
     mesher = Mesher(wl.desc.width, wl.desc.height, C, iso_value=wl.desc.iso_value, slabs=2, share_channels=True)
     for _ in range(3):
-        mesher.run(A_dev, stream.cuda_stream)
+        mesher.run(A_dev, stream=stream.cuda_stream)
     mesh_runs = 10
     barrier()
     m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     m0.record(stream)
     for _ in range(mesh_runs):
-        mesher.run(A_dev, stream.cuda_stream)
+        mesher.run(A_dev, stream=stream.cuda_stream)
     m1.record(stream)
     barrier()
     mesh_ms = m0.elapsed_time(m1) / mesh_runs

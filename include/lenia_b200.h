@@ -201,66 +201,79 @@ lenia_status lenia_convolve_noalloc(int width, int height, const float *field, c
 
 /* ---- Marching cubes --------------------------------------------------
  *
- * Replaces generate_mesh_v1 (mesh.cpp:34-431) with the buffer reset and
- * concatenation around it (render.cpp:153-212): an iso-surface of every
- * channel of a field, one vertex per intersected grid edge, face normals
- * summed into the vertices, and a triangle index buffer.  The reference's
- * D3D vertex buffers (position, normal, colour) become flat arrays; the
- * colour becomes the vertex's channel.  Cube (gx, gy, gz), gx, gy, gz in
- * [0, width), reads its corners at +1 from the field's periodic copy on the
+ * Replaces generate_mesh_v1/v2/v3 (mesh.cpp:34-431, 434-1109, 1115-2037)
+ * with the buffer reset and concatenation around them (render.cpp:153-212):
+ * an iso-surface of every channel of one to three fields meshed together, one
+ * vertex per intersected grid edge and field, face normals summed into the
+ * vertices, and a triangle index buffer.  The reference's D3D vertex buffers
+ * (position, normal, colour) become flat arrays; the colour becomes the
+ * vertex's channel.  Cube (gx, gy, gz), gx, gy, gz in [0, width), reads its
+ * corners at +1 from the periodic copy of the field's halo source on the
  * +x/+y/+z faces and 0 on the halo edges (transpose_mesh_borders,
  * transposition.cpp:881-995).
  *
  * The triangle table is this library's own (the reference's is third-party
  * data): built from geometry, it has the same triangle count as the
  * reference's for every one of the 256 cases (lenia_mc_triangle_table). */
+
+/* The reference's views (render.cpp:625-636): NORMAL meshes RBB (v1); U adds
+ * U_SUM_RB shifted along x (v2); H adds U_SUM_RB along x and H_RB along z (v3). */
+enum { LENIA_VIEW_NORMAL = 0, LENIA_VIEW_U = 1, LENIA_VIEW_H = 2 };
+
 typedef struct LeniaMeshDesc {
-    int width;          /* grid width (= depth) */
+    int width;            /* grid width (= depth) */
     int height;
-    int channels;       /* meshed channels 0 .. channels-1 of the field */
-    float iso_value;    /* ISO_VALUE (render.h:61): a corner is inside when value > iso_value */
-    float cell_size;    /* CELL_SIZE (render.h:26), 3.5 */
-    float x_offset;     /* added to x after interpolation when nonzero (the second mesh of the U/H views,
-                           mesh.cpp:434-1109, uses width * cell_size) */
-    int slabs;          /* z ranges meshed with separate vertex maps, as the MESH_THREADS (render.h:15)
-                           mesh threads split z (mesh.cpp:42-43): 2 reproduces the reference, 1 gives one
-                           mesh without seam duplicates */
-    int share_channels; /* 1: one vertex map for all channels, as V1_EDGES is cleared only per mesh
-                           (render.cpp:182), so a channel reuses the vertex an earlier channel put on the
-                           same edge; 0: a vertex map per channel */
+    int channels;         /* meshed channels 0 .. channels-1 of every field */
+    int fields;           /* 1..3 fields meshed together; per cube their triangles follow in field order */
+    float iso_value;      /* ISO_VALUE (render.h:61): a corner is inside when value > iso_value */
+    float cell_size;      /* CELL_SIZE (render.h:26), 3.5 */
+    float offset[3][3];   /* per field, added to x, y, z after interpolation where nonzero */
+    int slabs;            /* z ranges meshed with separate vertex maps, as the MESH_THREADS (render.h:15)
+                             mesh threads split z (mesh.cpp:42-43): 2 reproduces the reference, 1 gives one
+                             mesh without seam duplicates */
+    int share_channels;   /* 1: one vertex map per field for all channels, as V1_EDGES is cleared only per
+                             mesh (render.cpp:182), so a channel reuses the vertex an earlier channel put on
+                             the same edge; 0: a vertex map per field and channel */
 } LeniaMeshDesc;
 
 /* Arrays of the last mesh (lenia_mesher_get).  Vertices are numbered in the
  * order the reference creates them: by slab, then channel, then cube
- * (x fastest), then triangle slot. */
+ * (x fastest), then field, then triangle slot. */
 typedef enum LeniaMeshArray {
     LENIA_MESH_POSITIONS = 0,      /* float, 3 per vertex */
     LENIA_MESH_NORMALS = 1,        /* float, 3 per vertex: unnormalised sums of face normals (B-A)x(C-A) */
-    LENIA_MESH_VERTEX_CHANNEL = 2, /* int32, 1 per vertex: the channel whose triangle created it */
+    LENIA_MESH_VERTEX_CHANNEL = 2, /* int32, 1 per vertex: channel + channels * field of the creating triangle */
     LENIA_MESH_INDICES = 3,        /* uint32, 3 per triangle */
     LENIA_MESH_FACE_NORMALS = 4,   /* float, 3 per triangle */
-    LENIA_MESH_CASES = 5           /* uint8, channels * width * height * width: case index per cube */
+    LENIA_MESH_CASES = 5           /* uint8, fields * channels * width * height * width: case index per cube */
 } LeniaMeshArray;
 
 typedef struct lenia_mesher lenia_mesher;
 
+/* Fills a description for one of the reference's views (two slabs, channels
+ * sharing vertex maps, CELL_SIZE 3.5, offsets width * 3.5). */
+lenia_status lenia_mesh_desc_for_view(int view, int width, int height, int channels, float iso_value,
+                                      LeniaMeshDesc *out);
 /* Creates a mesher on the current CUDA device for fields of desc's shape
- * (width/height in [2, 1024], channels 1..4, slabs 1..width). */
+ * (width/height in [2, 512], channels 1..4, fields 1..3, slabs 1..width). */
 lenia_status lenia_mesher_create(const LeniaMeshDesc *desc, lenia_mesher **out);
 lenia_status lenia_mesher_destroy(lenia_mesher *m);
-/* Meshes `field` (device memory, channels * width * height * width floats,
- * channel-major, x fastest) on `stream` (a cudaStream_t; NULL = default).
- * Synchronises once, to size the output, and returns the counts; the arrays
- * are then ready on `stream`.  Output buffers grow as needed. */
-lenia_status lenia_mesher_run(lenia_mesher *m, const float *field, void *stream, long long *n_vertices,
-                              long long *n_triangles);
+/* Meshes desc.fields fields (device pointers, each channels * width * height *
+ * width floats, channel-major, x fastest) on `stream` (a cudaStream_t; NULL =
+ * default).  halos: per field the array whose periodic copy the +1 faces
+ * hold (NULL, or a NULL entry: the field itself).  Synchronises once, to size
+ * the output, and returns the counts; the arrays are then ready on `stream`.
+ * Output buffers grow as needed. */
+lenia_status lenia_mesher_run(lenia_mesher *m, const float *const *fields, const float *const *halos, void *stream,
+                              long long *n_vertices, long long *n_triangles);
 /* Copies one LeniaMeshArray of the last mesh, on the stream of the last run
  * (which must still exist); `count` is in elements and must equal the array's
  * size.  on_device: dst is device memory. */
 lenia_status lenia_mesher_get(lenia_mesher *m, int which, void *dst, size_t count, int on_device);
-/* lenia_mesher_run on a field of a world (A, RBB, H_RB, U_SUM_RB, H, U_SUM:
- * the NORMAL/U/H views read RBB, U_SUM_RB, H_RB), on the world's stream. */
-lenia_status lenia_mesh_world(lenia_world *w, int field, lenia_mesher *m, long long *n_vertices,
+/* lenia_mesher_run on a world's snapshots for a view (snapshots on; a mesher
+ * of view + 1 fields): RBB, U_SUM_RB, H_RB, whose +1 faces copy RBB, U_SUM
+ * and H, on the world's stream. */
+lenia_status lenia_mesh_world(lenia_world *w, int view, lenia_mesher *m, long long *n_vertices,
                               long long *n_triangles);
 /* Writes the triangle table (256 cases x 16 edge indices, -1 after the last
  * triangle; edges numbered as EDGE_TO_VERTICES, marching_cubes.h:17-22) and

@@ -59,11 +59,12 @@ class LeniaKernelParams(ctypes.Structure):
 class LeniaMeshDesc(ctypes.Structure):
     _fields_ = [
         ("width", ctypes.c_int), ("height", ctypes.c_int), ("channels", ctypes.c_int),
-        ("iso_value", ctypes.c_float), ("cell_size", ctypes.c_float), ("x_offset", ctypes.c_float),
-        ("slabs", ctypes.c_int), ("share_channels", ctypes.c_int),
+        ("fields", ctypes.c_int), ("iso_value", ctypes.c_float), ("cell_size", ctypes.c_float),
+        ("offset", (ctypes.c_float * 3) * 3), ("slabs", ctypes.c_int), ("share_channels", ctypes.c_int),
     ]
 
 
+VIEW = {"NORMAL": 0, "U": 1, "H": 2}
 MESH_ARRAY = {"positions": 0, "normals": 1, "vertex_channel": 2, "indices": 3, "face_normals": 4, "cases": 5}
 
 
@@ -132,8 +133,10 @@ def load() -> ctypes.CDLL:
                                     ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
         "lenia_mesher_create": ([ctypes.POINTER(LeniaMeshDesc), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
         "lenia_mesher_destroy": ([P], ctypes.c_int),
-        "lenia_mesher_run": ([P, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
-                              ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+        "lenia_mesher_run": ([P, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p,
+                              ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+        "lenia_mesh_desc_for_view": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                      ctypes.POINTER(LeniaMeshDesc)], ctypes.c_int),
         "lenia_mesher_get": ([P, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int], ctypes.c_int),
         "lenia_mesh_world": ([P, ctypes.c_int, P, ctypes.POINTER(ctypes.c_longlong),
                               ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),

@@ -1,11 +1,14 @@
-// Marching cubes: generate_mesh_v1 (mesh.cpp:34-431) with the buffer reset
-// and concatenation around it (render.cpp:153-212), as five launches.
+// Marching cubes: generate_mesh_v1/v2/v3 (mesh.cpp:34-431, 434-1109,
+// 1115-2037) with the buffer reset and concatenation around them
+// (render.cpp:153-212), as five launches.
 //
 // The reference creates vertices in a fixed order: slab (mesh thread), then
-// channel, then cube (x fastest), then triangle slot; an edge's vertex is
-// created by the first triangle slot that names the edge (its vertex map,
-// V1_EDGES, is keyed by edge origin and axis, per slab), and every triangle
-// that names the edge adds its face normal to it.  On the GPU:
+// channel, then cube (x fastest), then field (v1 meshes RBB; v2 adds U_SUM_RB,
+// v3 adds H_RB, each with its own vertex map), then triangle slot; an edge's
+// vertex is created by the first triangle slot that names the edge (a vertex
+// map, V1_EDGES/V2_EDGES/V3_EDGES, is keyed by edge origin and axis, per
+// slab), and every triangle that names the edge adds its face normal to it.
+// On the GPU:
 //
 //   mc_count    per cube and channel: case index, triangle count, and how many
 //               vertices the cube creates; per chunk of kMcThreads cubes the
@@ -102,13 +105,22 @@ struct McTables {
     unsigned char axis_edges[12];   // mc_axis_edge(ax, j) at 4 * ax + j
 };
 
+constexpr int kMcMaxFields = 3;
+
 struct McGeom {
-    int W, H, D, C;
+    int W, H, D, C, F;
     int slabs, nblk;  // z slabs; chunks per slab (of the largest slab)
     long long N;
     int share;
-    float iso, cell, xoff;
+    float iso, cell;
+    float off[kMcMaxFields][3];
+    const float *fld[kMcMaxFields];   // interiors
+    const float *halo[kMcMaxFields];  // arrays the +1 faces copy
 };
+
+// Offset of (field f, channel c) in the per-cube arrays (cases, tri_base,
+// vert_base): fields outermost.
+__device__ __forceinline__ long long fc_off(const McGeom &g, int f, int c) { return (long long)(f * g.C + c) * g.N; }
 
 __device__ __forceinline__ int slot_edge(unsigned long long t, int k) { return (int)((t >> (4 * k)) & 15); }
 __device__ __forceinline__ int tri_count(unsigned long long t) { return (int)(t >> 60); }
@@ -127,10 +139,13 @@ __device__ __forceinline__ int boundary_class(const McGeom &g, int x, int y, int
            (z == z1 - 1) << 5;
 }
 
-// Corner values of cube (gx, gy, gz) of one channel.  Corners on the +1 faces
-// read the periodic copy; corners on two or three +1 faces (halo edges and
-// corners) read 0.
-__device__ __forceinline__ void load_corners(const float *f, const McGeom &g, int gx, int gy, int gz, float *v)
+// Corner values of cube (gx, gy, gz) of one channel.  Corners on one +1 face
+// read the periodic copy of `halo` (transpose_mesh_borders copies GRID into
+// RBB's faces, but H and U_SUM of the current step into those of H_RB and
+// U_SUM_RB, transposition.cpp:881-995); corners on two or three +1 faces
+// (halo edges and corners) read 0.
+__device__ __forceinline__ void load_corners(const float *f, const float *halo, const McGeom &g, int gx, int gy,
+                                             int gz, float *v)
 {
     const int W = g.W, WH = g.W * g.H;
     if (gx + 1 < g.W && gy + 1 < g.H && gz + 1 < g.D) {
@@ -146,7 +161,7 @@ __device__ __forceinline__ void load_corners(const float *f, const McGeom &g, in
         if (x >= g.W) x -= g.W;
         if (y >= g.H) y -= g.H;
         if (z >= g.D) z -= g.D;
-        v[i] = out > 1 ? 0.0f : __ldg(f + x + y * W + (long long)z * WH);
+        v[i] = out > 1 ? 0.0f : __ldg((out ? halo : f) + x + y * W + (long long)z * WH);
     }
 }
 
@@ -159,8 +174,11 @@ __device__ __forceinline__ float sel8(const float *v, int i)
 }
 
 // Vertex on edge e of cube (gx, gy, gz): Pa + (Pb - Pa) * ((iso - va) / (vb - va))
-// with P = (g + delta) * cell (mesh.cpp:86-196), then x + x_offset.
-__device__ __forceinline__ float3 edge_vertex(const McGeom &g, unsigned ed, const float *v, int gx, int gy, int gz)
+// with P = (g + delta) * cell (mesh.cpp:86-196), then + the field's offset on
+// each axis where it is nonzero (mesh.cpp:434-1109 shifts U_SUM_RB's mesh
+// along x, mesh.cpp:1375-1397 H_RB's along z).
+__device__ __forceinline__ float3 edge_vertex(const McGeom &g, int f, unsigned ed, const float *v, int gx, int gy,
+                                              int gz)
 {
     const int a = ed & 7, b = (ed >> 3) & 7;
     const float va = sel8(v, a), vb = sel8(v, b);
@@ -172,7 +190,9 @@ __device__ __forceinline__ float3 edge_vertex(const McGeom &g, unsigned ed, cons
     r.x = ax + (bx - ax) * T;
     r.y = ay + (by - ay) * T;
     r.z = az + (bz - az) * T;
-    if (g.xoff != 0.0f) r.x = r.x + g.xoff;
+    if (g.off[f][0] != 0.0f) r.x = r.x + g.off[f][0];
+    if (g.off[f][1] != 0.0f) r.y = r.y + g.off[f][1];
+    if (g.off[f][2] != 0.0f) r.z = r.z + g.off[f][2];
     return r;
 }
 
@@ -237,8 +257,7 @@ __device__ __forceinline__ CubeRef cube_of(const McGeom &g, int chunk)
     return r;
 }
 
-__global__ void __launch_bounds__(kMcThreads) k_mc_count(const float *__restrict__ field, McGeom g,
-                                                        const McTables *__restrict__ tab,
+__global__ void __launch_bounds__(kMcThreads) k_mc_count(McGeom g, const McTables *__restrict__ tab,
                                                         unsigned char *__restrict__ cases,
                                                         long long *__restrict__ blk_tri,
                                                         long long *__restrict__ blk_vert)
@@ -250,20 +269,25 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_count(const float *__restrict
     for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const CubeRef q = cube_of(g, chunk);
         const unsigned owned = q.valid ? s_tab.owned[boundary_class(g, q.gx, q.gy, q.gz, q.z0, q.z1)] : 0u;
-        unsigned prev = 0;
+        unsigned prev[kMcMaxFields] = {0u, 0u, 0u};
         for (int c = 0; c < g.C; c++) {
-            int cs = 0;
-            if (q.valid) {
-                float v[8];
-                load_corners(field + c * g.N, g, q.gx, q.gy, q.gz, v);
+            unsigned nt = 0, nn = 0;
 #pragma unroll
-                for (int i = 0; i < 8; i++) cs |= (v[i] > g.iso) << i;
-                cases[c * g.N + q.p] = (unsigned char)cs;
+            for (int f = 0; f < kMcMaxFields; f++) {
+                if (f >= g.F) break;
+                int cs = 0;
+                if (q.valid) {
+                    float v[8];
+                    load_corners(g.fld[f] + c * g.N, g.halo[f] + c * g.N, g, q.gx, q.gy, q.gz, v);
+#pragma unroll
+                    for (int i = 0; i < 8; i++) cs |= (v[i] > g.iso) << i;
+                    cases[fc_off(g, f, c) + q.p] = (unsigned char)cs;
+                }
+                const unsigned act = active_edges(cs);
+                nt += tri_count(s_tab.tri[cs]);
+                nn += __popc(owned & act & ~prev[f]);
+                if (g.share) prev[f] |= act;
             }
-            const unsigned act = active_edges(cs);
-            const unsigned nt = tri_count(s_tab.tri[cs]);
-            const unsigned nn = __popc(owned & act & ~prev);
-            if (g.share) prev |= act;
             unsigned total;
             block_scan(nt | nn << 16, s_warp, &total);
             if (threadIdx.x == 0) {
@@ -312,8 +336,7 @@ __global__ void __launch_bounds__(1024) k_mc_scan(long long *tri, long long *ver
     }
 }
 
-__global__ void __launch_bounds__(kMcThreads) k_mc_emit(const float *__restrict__ field, McGeom g,
-                                                       const McTables *__restrict__ tab,
+__global__ void __launch_bounds__(kMcThreads) k_mc_emit(McGeom g, const McTables *__restrict__ tab,
                                                        const unsigned char *__restrict__ cases,
                                                        const long long *__restrict__ blk_tri,
                                                        const long long *__restrict__ blk_vert,
@@ -328,51 +351,65 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_emit(const float *__restrict_
     for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const CubeRef q = cube_of(g, chunk);
         const unsigned owned = q.valid ? s_tab.owned[boundary_class(g, q.gx, q.gy, q.gz, q.z0, q.z1)] : 0u;
-        unsigned prev = 0;
+        unsigned prev[kMcMaxFields] = {0u, 0u, 0u};
         for (int c = 0; c < g.C; c++) {
-            const int cs = q.valid ? cases[c * g.N + q.p] : 0;
-            const unsigned act = active_edges(cs);
-            const unsigned long long tl = s_tab.tri[cs];
-            const int nt = tri_count(tl);
-            const unsigned newm = owned & act & ~prev;
-            if (g.share) prev |= act;
+            int cs[kMcMaxFields] = {0, 0, 0};
+            unsigned newm[kMcMaxFields] = {0u, 0u, 0u};
+            unsigned nt = 0, nn = 0;
+#pragma unroll
+            for (int f = 0; f < kMcMaxFields; f++) {
+                if (f >= g.F) break;
+                cs[f] = q.valid ? cases[fc_off(g, f, c) + q.p] : 0;
+                const unsigned act = active_edges(cs[f]);
+                newm[f] = owned & act & ~prev[f];
+                if (g.share) prev[f] |= act;
+                nt += tri_count(s_tab.tri[cs[f]]);
+                nn += __popc(newm[f]);
+            }
             unsigned total;
-            const unsigned pre = block_scan((unsigned)nt | (unsigned)__popc(newm) << 16, s_warp, &total);
+            const unsigned pre = block_scan(nt | nn << 16, s_warp, &total);
             if (nt == 0) continue;
             const long long o = ((long long)q.s * g.C + c) * g.nblk + q.b;
-            const long long tb = blk_tri[o] + (pre & 0xffff);
-            const long long vb = blk_vert[o] + (pre >> 16);
-            tri_base[c * g.N + q.p] = (int)tb;
-            if (newm) vert_base[c * g.N + q.p] = (int)vb;
-            float v[8];
-            load_corners(field + c * g.N, g, q.gx, q.gy, q.gz, v);
-            for (int t = 0; t < nt; t++) {
-                const float3 A = edge_vertex(g, s_tab.edge[slot_edge(tl, 3 * t)], v, q.gx, q.gy, q.gz);
-                const float3 B = edge_vertex(g, s_tab.edge[slot_edge(tl, 3 * t + 1)], v, q.gx, q.gy, q.gz);
-                const float3 C = edge_vertex(g, s_tab.edge[slot_edge(tl, 3 * t + 2)], v, q.gx, q.gy, q.gz);
-                const float ux = B.x - A.x, uy = B.y - A.y, uz = B.z - A.z;
-                const float wx = C.x - A.x, wy = C.y - A.y, wz = C.z - A.z;
-                float *f = fn + 3 * (tb + t);
-                f[0] = uy * wz - uz * wy;
-                f[1] = uz * wx - ux * wz;
-                f[2] = ux * wy - uy * wx;
-            }
-            if (newm) {
-                unsigned seen = 0;
-                long long r = vb;
-                for (int k = 0; k < 3 * nt; k++) {
-                    const int e = slot_edge(tl, k);
-                    if ((seen >> e) & 1) continue;
-                    seen |= 1u << e;
-                    if (!((newm >> e) & 1)) continue;
-                    const float3 P = edge_vertex(g, s_tab.edge[e], v, q.gx, q.gy, q.gz);
-                    pos[3 * r] = P.x;
-                    pos[3 * r + 1] = P.y;
-                    pos[3 * r + 2] = P.z;
-                    vch[r] = c;
-                    vsrc[r] = (unsigned long long)(c * g.N + q.p) << 4 | (unsigned)e;
-                    r++;
+            long long tb = blk_tri[o] + (pre & 0xffff);
+            long long vb = blk_vert[o] + (pre >> 16);
+#pragma unroll
+            for (int f = 0; f < kMcMaxFields; f++) {
+                if (f >= g.F) break;
+                const unsigned long long tl = s_tab.tri[cs[f]];
+                const int ntf = tri_count(tl);
+                if (ntf == 0) continue;
+                tri_base[fc_off(g, f, c) + q.p] = (int)tb;
+                if (newm[f]) vert_base[fc_off(g, f, c) + q.p] = (int)vb;
+                float v[8];
+                load_corners(g.fld[f] + c * g.N, g.halo[f] + c * g.N, g, q.gx, q.gy, q.gz, v);
+                for (int t = 0; t < ntf; t++) {
+                    const float3 A = edge_vertex(g, f, s_tab.edge[slot_edge(tl, 3 * t)], v, q.gx, q.gy, q.gz);
+                    const float3 B = edge_vertex(g, f, s_tab.edge[slot_edge(tl, 3 * t + 1)], v, q.gx, q.gy, q.gz);
+                    const float3 C = edge_vertex(g, f, s_tab.edge[slot_edge(tl, 3 * t + 2)], v, q.gx, q.gy, q.gz);
+                    const float ux = B.x - A.x, uy = B.y - A.y, uz = B.z - A.z;
+                    const float wx = C.x - A.x, wy = C.y - A.y, wz = C.z - A.z;
+                    float *fo = fn + 3 * (tb + t);
+                    fo[0] = uy * wz - uz * wy;
+                    fo[1] = uz * wx - ux * wz;
+                    fo[2] = ux * wy - uy * wx;
                 }
+                if (newm[f]) {
+                    unsigned seen = 0;
+                    for (int k = 0; k < 3 * ntf; k++) {
+                        const int e = slot_edge(tl, k);
+                        if ((seen >> e) & 1) continue;
+                        seen |= 1u << e;
+                        if (!((newm[f] >> e) & 1)) continue;
+                        const float3 P = edge_vertex(g, f, s_tab.edge[e], v, q.gx, q.gy, q.gz);
+                        pos[3 * vb] = P.x;
+                        pos[3 * vb + 1] = P.y;
+                        pos[3 * vb + 2] = P.z;
+                        vch[vb] = c + g.C * f;
+                        vsrc[vb] = (unsigned long long)(fc_off(g, f, c) + q.p) << 4 | (unsigned)e;
+                        vb++;
+                    }
+                }
+                tb += ntf;
             }
         }
     }
@@ -414,43 +451,45 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_index(McGeom g, const McTable
         const CubeRef q = cube_of(g, chunk);
         if (!q.valid) continue;
         for (int c = 0; c < g.C; c++) {
-            const int cs = cases[c * g.N + q.p];
-            const unsigned long long tl = s_tab.tri[cs];
-            const int nt = tri_count(tl);
-            if (nt == 0) continue;
-            const long long tb = tri_base[c * g.N + q.p];
-            for (int k = 0; k < 3 * nt; k++) {
-                const int e = slot_edge(tl, k);
-                // channel that created the vertex
-                int c0 = c;
-                if (g.share)
-                    for (int c2 = 0; c2 < c; c2++)
-                        if ((active_edges(cases[c2 * g.N + q.p]) >> e) & 1) {
-                            c0 = c2;
-                            break;
-                        }
-                int eo;
-                const long long op = edge_creator(g, s_tab, e, q.gx, q.gy, q.gz, q.z0, q.z1, &eo);
-                const int oz = (int)(op / WH), rem = (int)(op - oz * WH);
-                const int oy = rem / g.W, ox = rem - oy * g.W;
-                const int ocs = cases[c0 * g.N + op];
-                unsigned oprev = 0;
-                if (g.share)
-                    for (int c2 = 0; c2 < c0; c2++) oprev |= active_edges(cases[c2 * g.N + op]);
-                const unsigned onew =
-                    s_tab.owned[boundary_class(g, ox, oy, oz, q.z0, q.z1)] & active_edges(ocs) & ~oprev;
-                // rank of eo among the creator's new vertices, in first-slot order
-                const unsigned long long otl = s_tab.tri[ocs];
-                unsigned seen = 0;
-                int r = 0;
-                for (int k2 = 0; k2 < 3 * tri_count(otl); k2++) {
-                    const int e2 = slot_edge(otl, k2);
-                    if ((seen >> e2) & 1) continue;
-                    seen |= 1u << e2;
-                    if (e2 == eo) break;
-                    r += (onew >> e2) & 1;
+            for (int f = 0; f < g.F; f++) {
+                const int cs = cases[fc_off(g, f, c) + q.p];
+                const unsigned long long tl = s_tab.tri[cs];
+                const int nt = tri_count(tl);
+                if (nt == 0) continue;
+                const long long tb = tri_base[fc_off(g, f, c) + q.p];
+                for (int k = 0; k < 3 * nt; k++) {
+                    const int e = slot_edge(tl, k);
+                    // channel that created the vertex
+                    int c0 = c;
+                    if (g.share)
+                        for (int c2 = 0; c2 < c; c2++)
+                            if ((active_edges(cases[fc_off(g, f, c2) + q.p]) >> e) & 1) {
+                                c0 = c2;
+                                break;
+                            }
+                    int eo;
+                    const long long op = edge_creator(g, s_tab, e, q.gx, q.gy, q.gz, q.z0, q.z1, &eo);
+                    const int oz = (int)(op / WH), rem = (int)(op - oz * WH);
+                    const int oy = rem / g.W, ox = rem - oy * g.W;
+                    const int ocs = cases[fc_off(g, f, c0) + op];
+                    unsigned oprev = 0;
+                    if (g.share)
+                        for (int c2 = 0; c2 < c0; c2++) oprev |= active_edges(cases[fc_off(g, f, c2) + op]);
+                    const unsigned onew =
+                        s_tab.owned[boundary_class(g, ox, oy, oz, q.z0, q.z1)] & active_edges(ocs) & ~oprev;
+                    // rank of eo among the creator's new vertices, in first-slot order
+                    const unsigned long long otl = s_tab.tri[ocs];
+                    unsigned seen = 0;
+                    int r = 0;
+                    for (int k2 = 0; k2 < 3 * tri_count(otl); k2++) {
+                        const int e2 = slot_edge(otl, k2);
+                        if ((seen >> e2) & 1) continue;
+                        seen |= 1u << e2;
+                        if (e2 == eo) break;
+                        r += (onew >> e2) & 1;
+                    }
+                    idx[3 * tb + k] = (unsigned)(vert_base[fc_off(g, f, c0) + op] + r);
                 }
-                idx[3 * tb + k] = (unsigned)(vert_base[c0 * g.N + op] + r);
             }
         }
     }
@@ -471,8 +510,9 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_normals(McGeom g, const McTab
         const unsigned long long src = vsrc[v];
         const int e0 = (int)(src & 15);
         const long long cp = (long long)(src >> 4);
-        const int c0 = (int)(cp / g.N);
-        const long long p0 = cp - c0 * g.N;
+        const int fc0 = (int)(cp / g.N);
+        const int f = fc0 / g.C, c0 = fc0 - f * g.C;
+        const long long p0 = cp - fc0 * g.N;
         const int gz = (int)(p0 / WH), rem = (int)(p0 - gz * WH);
         const int gy = rem / g.W, gx = rem - gy * g.W;
         int s = gz / (g.D / g.slabs);
@@ -485,7 +525,7 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_normals(McGeom g, const McTab
         float nx = 0.0f, ny = 0.0f, nz = 0.0f;
         const int c_end = g.share ? g.C : c0 + 1;
         for (int c = c0; c < c_end; c++) {
-            if (c > c0 && !((active_edges(cases[c * g.N + p0]) >> e0) & 1)) continue;
+            if (c > c0 && !((active_edges(cases[fc_off(g, f, c) + p0]) >> e0) & 1)) continue;
             for (int j = 0; j < 4; j++) {
                 const int e2 = s_tab.axis_edges[4 * ax + j];
                 const unsigned d2 = s_tab.edge[e2];
@@ -493,9 +533,9 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_normals(McGeom g, const McTab
                           z = Gz - (int)((d2 >> 10) & 1);
                 if (x < 0 || x >= g.W || y < 0 || y >= g.H || z < z0 || z >= z1) continue;
                 const long long qp = x + (long long)y * g.W + (long long)z * WH;
-                const unsigned long long tl = s_tab.tri[cases[c * g.N + qp]];
+                const unsigned long long tl = s_tab.tri[cases[fc_off(g, f, c) + qp]];
                 const int nt = tri_count(tl);
-                const long long tb = tri_base[c * g.N + qp];
+                const long long tb = tri_base[fc_off(g, f, c) + qp];
                 for (int t = 0; t < nt; t++) {
                     if (slot_edge(tl, 3 * t) == e2 || slot_edge(tl, 3 * t + 1) == e2 ||
                         slot_edge(tl, 3 * t + 2) == e2) {
@@ -681,7 +721,7 @@ void free_outputs(lenia_mesher *m)
 
 namespace lenia {
 long long mesher_field_floats(const lenia_mesher *m) { return m ? (long long)m->g.C * m->g.N : 0; }
-cudaStream_t mesher_stream(const lenia_mesher *m) { return m ? m->stream : nullptr; }
+int mesher_fields(const lenia_mesher *m) { return m ? m->g.F : 0; }
 }  // namespace lenia
 
 extern "C" {
@@ -697,13 +737,34 @@ int lenia_mc_triangle_table(int *table)
     return 0;
 }
 
+lenia_status lenia_mesh_desc_for_view(int view, int width, int height, int channels, float iso_value,
+                                      LeniaMeshDesc *out)
+{
+    if (!out || view < LENIA_VIEW_NORMAL || view > LENIA_VIEW_H) return LENIA_ERR_INVALID_ARG;
+    memset(out, 0, sizeof(*out));
+    out->width = width;
+    out->height = height;
+    out->channels = channels;
+    out->fields = view + 1;
+    out->iso_value = iso_value;
+    out->cell_size = 3.5f;  // CELL_SIZE, render.h:26
+    // GRID_WIDTH * CELL_SIZE, the shift of the second and third meshes
+    const float shift = (float)width * 3.5f;
+    if (view >= LENIA_VIEW_U) out->offset[1][0] = shift;
+    if (view == LENIA_VIEW_H) out->offset[2][2] = shift;
+    out->slabs = 2;          // MESH_THREADS, render.h:15
+    out->share_channels = 1;
+    return LENIA_OK;
+}
+
 lenia_status lenia_mesher_create(const LeniaMeshDesc *desc, lenia_mesher **out)
 {
     if (!desc || !out) return LENIA_ERR_INVALID_ARG;
     *out = nullptr;
     const LeniaMeshDesc &d = *desc;
     if (d.width < 2 || d.width > kMcMaxDim || d.height < 2 || d.height > kMcMaxDim || d.channels < 1 ||
-        d.channels > LENIA_MAX_CHANNELS || d.slabs < 1 || d.slabs > d.width || !(d.cell_size > 0.0f))
+        d.channels > LENIA_MAX_CHANNELS || d.fields < 1 || d.fields > kMcMaxFields || d.slabs < 1 ||
+        d.slabs > d.width || !(d.cell_size > 0.0f))
         return LENIA_ERR_INVALID_ARG;
     int dev = 0, nsm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return LENIA_ERR_NO_DEVICE;
@@ -716,6 +777,7 @@ lenia_status lenia_mesher_create(const LeniaMeshDesc *desc, lenia_mesher **out)
     g.H = d.height;
     g.D = d.width;
     g.C = d.channels;
+    g.F = d.fields;
     g.N = (long long)g.W * g.H * g.D;
     g.slabs = d.slabs;
     const long long largest = (long long)g.W * g.H * (g.D - (g.D / g.slabs) * (g.slabs - 1));
@@ -723,7 +785,8 @@ lenia_status lenia_mesher_create(const LeniaMeshDesc *desc, lenia_mesher **out)
     g.share = d.share_channels != 0;
     g.iso = d.iso_value;
     g.cell = d.cell_size;
-    g.xoff = d.x_offset;
+    for (int f = 0; f < kMcMaxFields; f++)
+        for (int a = 0; a < 3; a++) g.off[f][a] = f < g.F ? d.offset[f][a] : 0.0f;
     const long long nchunks = (long long)g.slabs * g.nblk;
     m->grid = (int)(nchunks < 8LL * nsm ? nchunks : 8LL * nsm);
     const long long M = nchunks * g.C;
@@ -734,9 +797,10 @@ lenia_status lenia_mesher_create(const LeniaMeshDesc *desc, lenia_mesher **out)
         if (e == cudaSuccess) e = cudaMalloc((void **)&p, bytes);
     };
     alloc(m->tab, sizeof(McTables));
-    alloc(m->cases, (size_t)g.C * g.N);
-    alloc(m->tri_base, sizeof(int) * (size_t)g.C * g.N);
-    alloc(m->vert_base, sizeof(int) * (size_t)g.C * g.N);
+    const size_t cubes = (size_t)g.F * g.C * g.N;
+    alloc(m->cases, cubes);
+    alloc(m->tri_base, sizeof(int) * cubes);
+    alloc(m->vert_base, sizeof(int) * cubes);
     alloc(m->blk_tri, sizeof(long long) * (size_t)M);
     alloc(m->blk_vert, sizeof(long long) * (size_t)M);
     alloc(m->totals, 2 * sizeof(long long));
@@ -767,16 +831,21 @@ lenia_status lenia_mesher_destroy(lenia_mesher *m)
     return LENIA_OK;
 }
 
-lenia_status lenia_mesher_run(lenia_mesher *m, const float *field, void *stream, long long *n_vertices,
-                              long long *n_triangles)
+lenia_status lenia_mesher_run(lenia_mesher *m, const float *const *fields, const float *const *halos, void *stream,
+                              long long *n_vertices, long long *n_triangles)
 {
-    if (!m || !field) return LENIA_ERR_INVALID_ARG;
+    if (!m || !fields) return LENIA_ERR_INVALID_ARG;
+    McGeom &g = m->g;
+    for (int f = 0; f < kMcMaxFields; f++) {
+        if (f < g.F && !fields[f]) return mfail(m, LENIA_ERR_INVALID_ARG, "field %d is NULL", f);
+        g.fld[f] = f < g.F ? fields[f] : nullptr;
+        g.halo[f] = f < g.F ? (halos && halos[f] ? halos[f] : fields[f]) : nullptr;
+    }
     cudaStream_t st = (cudaStream_t)stream;
     m->stream = st;
     m->have_mesh = false;
-    const McGeom &g = m->g;
     const long long M = (long long)g.slabs * g.nblk * g.C;
-    k_mc_count<<<m->grid, kMcThreads, 0, st>>>(field, g, m->tab, m->cases, m->blk_tri, m->blk_vert);
+    k_mc_count<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk_tri, m->blk_vert);
     k_mc_scan<<<1, 1024, 0, st>>>(m->blk_tri, m->blk_vert, M, m->totals);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(m->h_totals, m->totals, 2 * sizeof(long long), cudaMemcpyDeviceToHost, st);
@@ -803,7 +872,7 @@ lenia_status lenia_mesher_run(lenia_mesher *m, const float *field, void *stream,
         m->cap_v = cv;
     }
     if (nt > 0) {
-        k_mc_emit<<<m->grid, kMcThreads, 0, st>>>(field, g, m->tab, m->cases, m->blk_tri, m->blk_vert, m->tri_base,
+        k_mc_emit<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk_tri, m->blk_vert, m->tri_base,
                                                   m->vert_base, m->fn, m->pos, m->vch, m->vsrc);
         k_mc_index<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vert_base, m->idx);
         const long long nb = (nv + kMcThreads - 1) / kMcThreads;
@@ -832,7 +901,7 @@ lenia_status lenia_mesher_get(lenia_mesher *m, int which, void *dst, size_t coun
     case LENIA_MESH_VERTEX_CHANNEL: src = m->vch; n = (size_t)m->n_v; break;
     case LENIA_MESH_INDICES: src = m->idx; n = 3 * (size_t)m->n_t; break;
     case LENIA_MESH_FACE_NORMALS: src = m->fn; n = 3 * (size_t)m->n_t; break;
-    case LENIA_MESH_CASES: src = m->cases; n = (size_t)m->g.C * m->g.N; elem = 1; break;
+    case LENIA_MESH_CASES: src = m->cases; n = (size_t)m->g.F * m->g.C * m->g.N; elem = 1; break;
     default: return mfail(m, LENIA_ERR_INVALID_ARG, "unknown mesh array %d", which);
     }
     if (count != n) return mfail(m, LENIA_ERR_INVALID_ARG, "mesh array %d holds %zu elements, got %zu", which, n, count);

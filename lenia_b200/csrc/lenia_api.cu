@@ -929,19 +929,22 @@ int lenia_profile_read(lenia_world *w, double *ms, long long *launches, int n)
     return KID_MAX;
 }
 
-lenia_status lenia_mesh_world(lenia_world *w, int field, lenia_mesher *m, long long *n_vertices,
+lenia_status lenia_mesh_world(lenia_world *w, int view, lenia_mesher *m, long long *n_vertices,
                               long long *n_triangles)
 {
     if (!w || !m) return LENIA_ERR_INVALID_ARG;
-    if (field != LENIA_FIELD_A && field != LENIA_FIELD_RBB && field != LENIA_FIELD_H_RB &&
-        field != LENIA_FIELD_U_SUM_RB && field != LENIA_FIELD_H && field != LENIA_FIELD_U_SUM)
-        return fail(w, LENIA_ERR_INVALID_ARG, "field %d cannot be meshed", field);
-    size_t n = 0;
-    const float *p = field_ptr(w, field, &n);
-    if (!p) return fail(w, LENIA_ERR_INVALID_ARG, "field %d is not available (enable snapshots?)", field);
-    if ((long long)n != mesher_field_floats(m))
-        return fail(w, LENIA_ERR_INVALID_ARG, "mesher shape does not match the world (%zu floats)", n);
-    const lenia_status s = lenia_mesher_run(m, p, w->stream, n_vertices, n_triangles);
+    if (view < LENIA_VIEW_NORMAL || view > LENIA_VIEW_H)
+        return fail(w, LENIA_ERR_INVALID_ARG, "unknown view %d", view);
+    if (!w->snapshots || !w->RBB) return fail(w, LENIA_ERR_INVALID_ARG, "meshing reads the snapshots: enable them");
+    if (mesher_fields(m) != view + 1)
+        return fail(w, LENIA_ERR_INVALID_ARG, "view %d meshes %d fields, the mesher %d", view, view + 1,
+                    mesher_fields(m));
+    if (mesher_field_floats(m) != (long long)w->C * w->d.N)
+        return fail(w, LENIA_ERR_INVALID_ARG, "mesher shape does not match the world");
+    // the snapshots, and the arrays their +1 faces copy (transposition.cpp:881-995)
+    const float *fields[3] = {w->RBB, w->U_SUM_RB, w->H_RB};
+    const float *halos[3] = {w->RBB, w->U_SUM, w->H};
+    const lenia_status s = lenia_mesher_run(m, fields, halos, w->stream, n_vertices, n_triangles);
     if (s != LENIA_OK) return fail(w, s, "mesh: %s", lenia_mesher_last_error(m));
     return LENIA_OK;
 }

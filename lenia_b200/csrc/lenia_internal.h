@@ -143,7 +143,9 @@ cudaError_t launch_blur_rows_fast(const Dims &d, const float2 *tw_x_inv, const B
 // Host FFT plans and twiddle tables (lenia_api.cu).
 int fft_factor(int n, int *radix);
 
-// Marching-cubes mesher (kernels_mesh.cu): floats of the field it meshes.
+// Marching-cubes mesher (kernels_mesh.cu): floats of each field it meshes,
+// and the number of fields.
 long long mesher_field_floats(const lenia_mesher *m);
+int mesher_fields(const lenia_mesher *m);
 
 }  // namespace lenia

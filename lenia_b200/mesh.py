@@ -1,9 +1,10 @@
-"""Marching cubes over the C ABI: the reference's generate_mesh_v1
-(mesh.cpp:34-431) with its buffer reset and concatenation
-(render.cpp:153-212), headless.
+"""Marching cubes over the C ABI: the reference's generate_mesh_v1/v2/v3
+(mesh.cpp) with its buffer reset and concatenation (render.cpp:153-212),
+headless.
 
-`Mesher` meshes every channel of a field (a World's field, or a CUDA tensor
-of channels x depth x height x width floats) and returns flat arrays:
+`Mesher` meshes every channel of one to three fields (a World's snapshots,
+or CUDA tensors of channels x depth x height x width floats) and returns flat
+arrays:
 positions and normals (V x 3), the creating channel of each vertex, triangle
 indices (T x 3), face normals (T x 3) and, on request, the case index of every
 cube.  `write_ply` / `write_obj` dump a mesh to a file.
@@ -26,10 +27,10 @@ MESH_THREADS = 2    # render.h:15
 class MeshArrays:
     positions: np.ndarray       # (V, 3) float32
     normals: np.ndarray         # (V, 3) float32, unnormalised
-    vertex_channel: np.ndarray  # (V,) int32
+    vertex_channel: np.ndarray  # (V,) int32: channel + channels * field
     indices: np.ndarray         # (T, 3) uint32
     face_normals: np.ndarray    # (T, 3) float32
-    cases: Optional[np.ndarray] = None  # (C, N) uint8
+    cases: Optional[np.ndarray] = None  # (F, C, N) uint8
 
     @property
     def n_vertices(self) -> int:
@@ -52,17 +53,41 @@ def triangle_table() -> np.ndarray:
 class Mesher:
     """Iso-surface extraction for fields of one shape.
 
-    slabs=2, share_channels=True reproduce the reference's two mesh threads
-    and its vertex map shared by all channels; slabs=1, share_channels=False
-    give one mesh per channel without seam duplicates."""
+    fields > 1 meshes several fields together (the reference's U and H
+    views), each with its own vertex map and its own offset (one (x, y, z)
+    per field).  slabs=2, share_channels=True reproduce the reference's two
+    mesh threads and its vertex maps shared by all channels; slabs=1,
+    share_channels=False give one mesh per channel without seam duplicates."""
 
     def __init__(self, width: int, height: int, channels: int, iso_value: float = 0.5,
-                 cell_size: float = CELL_SIZE, x_offset: float = 0.0, slabs: int = MESH_THREADS,
+                 cell_size: float = CELL_SIZE, fields: int = 1, offsets=None, slabs: int = MESH_THREADS,
                  share_channels: bool = True):
+        d = _lib.LeniaMeshDesc()
+        d.width, d.height, d.channels, d.fields = width, height, channels, fields
+        d.iso_value, d.cell_size = float(iso_value), float(cell_size)
+        if offsets is not None:
+            for f, o in enumerate(offsets):
+                for a in range(3):
+                    d.offset[f][a] = float(o[a])
+        d.slabs, d.share_channels = int(slabs), 1 if share_channels else 0
+        self._init(d)
+
+    @classmethod
+    def for_view(cls, view: str, width: int, height: int, channels: int, iso_value: float = 0.5) -> "Mesher":
+        """A mesher set up as the reference meshes view NORMAL, U or H."""
+        lib = _lib.load()
+        d = _lib.LeniaMeshDesc()
+        st = lib.lenia_mesh_desc_for_view(_lib.VIEW[view], width, height, channels, float(iso_value),
+                                          ctypes.byref(d))
+        if st != _lib.LENIA_OK:
+            raise _lib.LeniaError(st, "lenia_mesh_desc_for_view failed")
+        m = cls.__new__(cls)
+        m._init(d)
+        return m
+
+    def _init(self, d):
         self._lib = _lib.load()
-        self.width, self.height, self.channels = width, height, channels
-        d = _lib.LeniaMeshDesc(width, height, channels, float(iso_value), float(cell_size), float(x_offset),
-                               int(slabs), 1 if share_channels else 0)
+        self.width, self.height, self.channels, self.fields = d.width, d.height, d.channels, d.fields
         self._d = d
         h = ctypes.c_void_p()
         st = self._lib.lenia_mesher_create(ctypes.byref(d), ctypes.byref(h))
@@ -88,27 +113,46 @@ class Mesher:
         if st != _lib.LENIA_OK:
             raise _lib.LeniaError(st, self._lib.lenia_mesher_last_error(self._h).decode())
 
-    def run(self, field, stream: int = 0) -> tuple[int, int]:
-        """Meshes a CUDA tensor (channels x depth x height x width float32) on
-        `stream` (a cudaStream_t as int; 0 = default).  Returns (V, T)."""
-        if not (hasattr(field, "is_cuda") and field.is_cuda):
-            raise TypeError("Mesher.run takes a CUDA tensor; use run_world for a World's field")
-        t = field.contiguous()
-        if t.numel() != self.channels * self.width * self.height * self.width:
-            raise ValueError("field shape does not match the mesher")
+    def run(self, fields, halos=None, stream: int = 0) -> tuple[int, int]:
+        """Meshes CUDA tensors (one per field, channels x depth x height x
+        width float32; a single tensor for one field) on `stream` (a
+        cudaStream_t as int; 0 = default).  halos: per field the tensor whose
+        periodic copy the +1 faces hold (None: the field).  Returns (V, T)."""
+        if not isinstance(fields, (list, tuple)):
+            fields = [fields]
+        if len(fields) != self.fields:
+            raise ValueError(f"the mesher meshes {self.fields} fields")
+        n = self.channels * self.width * self.height * self.width
+        keep = []
+
+        def ptrs(ts):
+            arr = (ctypes.c_void_p * 3)()
+            for i, t in enumerate(ts):
+                if t is None:
+                    continue
+                if not (hasattr(t, "is_cuda") and t.is_cuda):
+                    raise TypeError("Mesher.run takes CUDA tensors; use run_world for a World")
+                t = t.contiguous()
+                if t.numel() != n:
+                    raise ValueError("field shape does not match the mesher")
+                keep.append(t)
+                arr[i] = t.data_ptr()
+            return arr
+
+        fp = ptrs(fields)
+        hp = ptrs(halos) if halos is not None else None
         nv, nt = ctypes.c_longlong(), ctypes.c_longlong()
-        self._check(self._lib.lenia_mesher_run(self._h, ctypes.c_void_p(t.data_ptr()), ctypes.c_void_p(stream),
-                                               ctypes.byref(nv), ctypes.byref(nt)))
+        self._check(self._lib.lenia_mesher_run(self._h, fp, hp, ctypes.c_void_p(stream), ctypes.byref(nv),
+                                               ctypes.byref(nt)))
         self._world = None
         self.n_vertices, self.n_triangles = nv.value, nt.value
         return self.n_vertices, self.n_triangles
 
-    def run_world(self, world, field: str = "RBB") -> tuple[int, int]:
-        """Meshes a field of a World on the world's stream (RBB, H_RB and
-        U_SUM_RB are the snapshots the reference's views mesh)."""
+    def run_world(self, world, view: str = "NORMAL") -> tuple[int, int]:
+        """Meshes a World's snapshots as the reference's view NORMAL (RBB), U
+        (+ U_SUM_RB) or H (+ U_SUM_RB, H_RB) on the world's stream."""
         nv, nt = ctypes.c_longlong(), ctypes.c_longlong()
-        st = self._lib.lenia_mesh_world(world.handle, _lib.FIELD[field], self._h, ctypes.byref(nv),
-                                        ctypes.byref(nt))
+        st = self._lib.lenia_mesh_world(world.handle, _lib.VIEW[view], self._h, ctypes.byref(nv), ctypes.byref(nt))
         if st != _lib.LENIA_OK:
             raise _lib.LeniaError(st, self._lib.lenia_last_error(world.handle).decode())
         self._world = world
@@ -123,7 +167,7 @@ class Mesher:
             "positions": ((nv, 3), np.float32), "normals": ((nv, 3), np.float32),
             "vertex_channel": ((nv,), np.int32), "indices": ((nt, 3), np.uint32),
             "face_normals": ((nt, 3), np.float32),
-            "cases": ((self.channels, n_cells // self.channels), np.uint8),
+            "cases": ((self.fields, self.channels, n_cells // self.channels), np.uint8),
         }[name]
         out = np.zeros(shape, dtype=dtype)
         self._check(self._lib.lenia_mesher_get(self._h, _lib.MESH_ARRAY[name], out.ctypes.data_as(ctypes.c_void_p),

@@ -347,48 +347,70 @@ def mc_table(kind: str = "own") -> np.ndarray:
     return t.reshape(256, 16)
 
 
-def mesh_restated(field: np.ndarray, W: int, H: int, C: int, iso: float, cell: float = 3.5,
-                  x_offset: float = 0.0, table: np.ndarray | None = None, slabs: int = 1,
-                  share_channels: bool = False) -> Mesh:
-    """Marching cubes of the C-channel field (channel-major, x fastest) by the
-    restatement of generate_mesh_v1 (ora_mesh in oracle/restate/mc_tables.c)."""
+def mesh_restated(fields, W: int, H: int, C: int, iso: float, cell: float = 3.5, offsets=None,
+                  table: np.ndarray | None = None, slabs: int = 1, share_channels: bool = False,
+                  halos=None, quirks: bool = False) -> Mesh:
+    """Marching cubes of one C-channel field, or of a list of fields meshed
+    together (the U/H views), by the restatement of generate_mesh_v1/v2/v3
+    (ora_mesh_fields in oracle/restate/mc_tables.c).  offsets: one (x, y, z)
+    per field added after interpolation; halos: per field the array its +1
+    faces copy (None: the field); quirks: the reference's stale normal slots
+    of fields 1 and 2 (then `unsure` flags vertices that read a slot never
+    written)."""
     lib = RestateOracle.lib()
-    f = np.ascontiguousarray(field, dtype=np.float32).ravel()
+    if isinstance(fields, np.ndarray):
+        fields = [fields]
     N = W * H * W
-    assert f.size >= C * N
+    fl = [np.ascontiguousarray(f, dtype=np.float32).ravel() for f in fields]
+    assert all(f.size >= C * N for f in fl)
+    F = len(fl)
+    FP = ctypes.POINTER(ctypes.c_float)
+    ptrs = (FP * F)(*[_fp(f) for f in fl])
+    hptrs = None
+    if halos is not None:
+        hl = [None if h is None else np.ascontiguousarray(h, dtype=np.float32).ravel() for h in halos]
+        hptrs = (FP * F)(*[_fp(h) if h is not None else FP() for h in hl])
+    off = None
+    if offsets is not None:
+        off = np.ascontiguousarray(offsets, dtype=np.float32).reshape(F, 3)
     tab = None
     if table is not None:
         tab = np.ascontiguousarray(table, dtype=np.int32).ravel()
         assert tab.size == 256 * 16
-    cases = np.zeros(C * N, dtype=np.uint8)
+    cases = np.zeros(F * C * N, dtype=np.uint8)
     cap_v = cap_i = 1024
     while True:
         pos = np.zeros(3 * cap_v, dtype=np.float32)
         nrm = np.zeros(3 * cap_v, dtype=np.float32)
         vch = np.zeros(cap_v, dtype=np.int32)
+        unsure = np.zeros(cap_v, dtype=np.uint8)
         idx = np.zeros(cap_i, dtype=np.uint32)
         fn = np.zeros(cap_i, dtype=np.float32)
         nv, ni = ctypes.c_long(0), ctypes.c_long(0)
-        rc = lib.ora_mesh(_fp(f), ctypes.c_int(W), ctypes.c_int(H), ctypes.c_int(C), ctypes.c_float(iso),
-                          ctypes.c_float(cell), ctypes.c_float(x_offset),
-                          None if tab is None else tab.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                          ctypes.c_int(slabs), ctypes.c_int(1 if share_channels else 0),
-                          cases.ctypes.data_as(ctypes.c_void_p), _fp(pos), _fp(nrm),
-                          vch.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(cap_v),
-                          idx.ctypes.data_as(ctypes.c_void_p), _fp(fn), ctypes.c_long(cap_i),
-                          ctypes.byref(nv), ctypes.byref(ni))
+        rc = lib.ora_mesh_fields(ptrs, hptrs, ctypes.c_int(F), None if off is None else _fp(off),
+                                 ctypes.c_int(W), ctypes.c_int(H), ctypes.c_int(C), ctypes.c_float(iso),
+                                 ctypes.c_float(cell),
+                                 None if tab is None else tab.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                 ctypes.c_int(slabs), ctypes.c_int(1 if share_channels else 0),
+                                 ctypes.c_int(1 if quirks else 0),
+                                 cases.ctypes.data_as(ctypes.c_void_p), _fp(pos), _fp(nrm),
+                                 vch.ctypes.data_as(ctypes.c_void_p), unsure.ctypes.data_as(ctypes.c_void_p),
+                                 ctypes.c_long(cap_v), idx.ctypes.data_as(ctypes.c_void_p), _fp(fn),
+                                 ctypes.c_long(cap_i), ctypes.byref(nv), ctypes.byref(ni))
         if rc == 0:
             break
         cap_v, cap_i = max(nv.value, 1), max(ni.value, 1)
     m = Mesh(pos[:3 * nv.value].reshape(-1, 3), nrm[:3 * nv.value].reshape(-1, 3), idx[:ni.value],
-             vch[:nv.value], cases.reshape(C, N))
+             vch[:nv.value], cases.reshape(F, C, N))
     m.face_normals = fn[:ni.value].reshape(-1, 3)
+    m.unsure = unsure[:nv.value].astype(bool)
     return m
 
 
-def mesh_reference(ref: "RefOracle") -> Mesh:
-    """The reference's own generate_mesh_v1 on its RBB snapshot (run the TMB
-    event first), both mesh threads concatenated, without stitching."""
+def mesh_reference(ref: "RefOracle", view: int = 0) -> Mesh:
+    """The reference's own generate_mesh_v1 (view 0), v2 (1) or v3 (2) on its
+    RBB / U_SUM_RB / H_RB snapshots (run a step, or the TMB event, first),
+    both mesh threads concatenated, without stitching."""
     lib = ref.lib()
     cap_v = cap_i = 1024
     while True:
@@ -396,8 +418,9 @@ def mesh_reference(ref: "RefOracle") -> Mesh:
         nrm = np.zeros(3 * cap_v, dtype=np.float32)
         idx = np.zeros(cap_i, dtype=np.uint32)
         nv, ni = ctypes.c_long(0), ctypes.c_long(0)
-        rc = lib.ref_mesh_v1(_fp(pos), _fp(nrm), ctypes.c_long(cap_v), idx.ctypes.data_as(ctypes.c_void_p),
-                             ctypes.c_long(cap_i), ctypes.byref(nv), ctypes.byref(ni))
+        rc = lib.ref_mesh(ctypes.c_int(view), _fp(pos), _fp(nrm), ctypes.c_long(cap_v),
+                          idx.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(cap_i), ctypes.byref(nv),
+                          ctypes.byref(ni))
         if rc == 0:
             break
         cap_v, cap_i = max(nv.value, 1), max(ni.value, 1)

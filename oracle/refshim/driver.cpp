@@ -479,20 +479,23 @@ void ref_get_spectrum(int c, float *out_complex)
     memcpy(out_complex, T[c], sizeof(fftwf_complex) * GRID_SIZE);
 }
 
-/* One mesh of the NORMAL view: the buffer reset of reset_mesh_generation
- * (render.cpp:182-200), generate_mesh_v1 (mesh.cpp:34-431) for every mesh
- * thread on RBB (filled by ORA_EV_TMB), and the concatenation of
- * render.cpp:161-179 (thread order; indices offset by the vertices before
- * them).  stitch_borders (main.cpp:101-163) is not run.  Writes positions and
- * normals (3 floats per vertex) and indices; returns 0, or -1 when the output
- * capacity is too small. */
-int ref_mesh_v1(float *pos, float *nrm, long max_v, unsigned *idx, long max_i, long *n_v, long *n_i)
+/* One mesh of view 0 (NORMAL), 1 (U) or 2 (H), as mesh_thread_loop picks
+ * them (render.cpp:625-636): the buffer reset of reset_mesh_generation
+ * (render.cpp:182-200), generate_mesh_v1/v2/v3 (mesh.cpp) for every mesh
+ * thread on RBB, U_SUM_RB, H_RB (filled by the step and ORA_EV_TMB), and the
+ * concatenation of render.cpp:161-179 (thread order; indices offset by the
+ * vertices before them).  stitch_borders (main.cpp:101-163) is not run.
+ * Writes positions and normals (3 floats per vertex) and indices; returns 0,
+ * or -1 when the output capacity is too small. */
+int ref_mesh(int view, float *pos, float *nrm, long max_v, unsigned *idx, long max_i, long *n_v, long *n_i)
 {
     static Vertex *vbuf[MESH_THREADS];
     static DWORD *ibuf[MESH_THREADS];
-    const long cap = 15L * GRID_WIDTH * GRID_HEIGHT * GRID_WIDTH * MAX_CHANNELS;
+    const long cap = 3 * 15L * GRID_WIDTH * GRID_HEIGHT * GRID_WIDTH * MAX_CHANNELS;
     cur_buf = 0;
     memset(V1_EDGES, -1, sizeof(V1_EDGES));
+    memset(V2_EDGES, -1, sizeof(V2_EDGES));
+    memset(V3_EDGES, -1, sizeof(V3_EDGES));
     for (int t = 0; t < MESH_THREADS; t++) {
         if (!vbuf[t]) {
             vbuf[t] = (Vertex *)malloc(sizeof(Vertex) * cap);
@@ -511,7 +514,9 @@ int ref_mesh_v1(float *pos, float *nrm, long max_v, unsigned *idx, long max_i, l
         memset(td->upper_border, -1, sizeof(td->upper_border));
         memset(td->lower_indices, 0, sizeof(td->lower_indices));
         memset(td->upper_indices, 0, sizeof(td->upper_indices));
-        generate_mesh_v1(td);
+        if (view == 1) generate_mesh_v2(td);
+        else if (view == 2) generate_mesh_v3(td);
+        else generate_mesh_v1(td);
     }
     long nv = 0, ni = 0;
     for (int t = 0; t < MESH_THREADS; t++) {

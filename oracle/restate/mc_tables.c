@@ -1,6 +1,6 @@
 /*
  * Oracle test infrastructure: marching-cubes tables derived from geometry,
- * and the marching-cubes restatement of generate_mesh_v1 (mesh.cpp:34-431).
+ * and the marching-cubes restatement of generate_mesh_v1/v2/v3 (mesh.cpp).
  *
  * The reference's tables (marching_cubes.h:61-356) are third-party data and
  * are not copied.  Here:
@@ -129,14 +129,17 @@ int mc_triangle_count(int c)
 }
 
 /* Value of channel c at cube corner (x, y, z), 0 <= x <= W, 0 <= y <= H,
- * 0 <= z <= D: the mesh snapshot RBB with its halo as transpose_mesh_borders
- * leaves it (transposition.cpp:881-995): faces hold the periodic copy, halo
- * edges and corners are never written and read 0. */
-static float mc_corner_value(const float *f, int W, int H, int c, int x, int y, int z)
+ * 0 <= z <= D, of a mesh snapshot with its halo as transpose_mesh_borders
+ * leaves it (transposition.cpp:881-995): the +1 faces hold the periodic copy
+ * of `halo` (GRID for RBB, but H for H_RB and U_SUM for U_SUM_RB, whose
+ * interiors hold the previous step); halo edges and corners are never
+ * written and read 0. */
+static float mc_corner_value(const float *f, const float *halo, int W, int H, int c, int x, int y, int z)
 {
     const int D = W;
     const int no = (x >= W) + (y >= H) + (z >= D);
     if (no > 1) return 0.0f;
+    if (no == 1) f = halo;
     if (x >= W) x -= W;
     if (y >= H) y -= H;
     if (z >= D) z -= D;
@@ -153,29 +156,49 @@ void mc_own_table(int *table)
 }
 
 /* Marching cubes with the loop order, arithmetic and vertex sharing of
- * generate_mesh_v1 (mesh.cpp:34-431):
+ * generate_mesh_v1/v2/v3 (mesh.cpp:34-431, 434-1109, 1115-2037):
+ *   - `F` fields are meshed together (v1: RBB; v2: RBB, U_SUM_RB; v3: RBB,
+ *     U_SUM_RB, H_RB), each with its own vertex map (V1_EDGES, V2_EDGES,
+ *     V3_EDGES), into one vertex and index buffer; per cube the fields'
+ *     triangles follow each other in field order;
  *   - z is split into `slabs` ranges as the mesh threads split it
- *     (mesh.cpp:42-43); each slab has its own vertex map (ETIDX's thread
+ *     (mesh.cpp:42-43); each slab has its own vertex maps (ETIDX's thread
  *     index, render.h:517) and its vertices and indices follow the previous
  *     slab's, as reset_mesh_generation concatenates them (render.cpp:161-179);
- *   - within a slab: channels, then gz, gy, gx; the vertex map is cleared per
- *     slab, and also per channel when share == 0 (the reference clears
- *     V1_EDGES only per mesh, so share == 1 reproduces it);
+ *   - within a slab: channels, then gz, gy, gx, then fields; the vertex maps
+ *     are cleared per slab, and also per channel when share == 0 (the
+ *     reference clears them only per mesh, so share == 1 reproduces it);
  *   - corner i of cube g sits at (g + delta_i) * cell and is inside when its
  *     value > iso; edge vertex Pa + (Pb - Pa) * ((iso - va) / (vb - va)),
- *     then x + x_offset when x_offset != 0 (the second mesh of the U/H views,
- *     mesh.cpp:434-1109);
+ *     then + offset[f] on each axis whose offset is nonzero (v2 and v3 shift
+ *     U_SUM_RB's mesh along x and H_RB's along z by GRID_WIDTH * CELL_SIZE);
  *   - per triangle (table order) the face normal (B-A) x (C-A); each corner
- *     looks up its edge (origin, axis) in the vertex map, creates the vertex
- *     from this cube's position if absent, adds the face normal and appends
- *     the index.
- * table: 256 x 16 edge indices, -1 terminated (NULL: mc_own_table).
- * cases (C x N, optional) receives each cube's case index; fnrm (optional,
- * 3 floats per triangle, indexed like idx) each triangle's face normal.  Returns 0, or -1
- * when max_v or max_i is too small (counts are still complete). */
-int ora_mesh(const float *field, int W, int H, int C, float iso, float cell, float x_offset, const int *table,
-             int slabs, int share, unsigned char *cases, float *pos, float *nrm, int *vch, long max_v,
-             unsigned *idx, float *fnrm, long max_i, long *n_v, long *n_i)
+ *     looks up its edge (origin, axis) in the field's vertex map, creates the
+ *     vertex from this cube's position if absent, adds the face normal and
+ *     appends the index.
+ * fields: F pointers to C-channel fields (channel-major, x fastest); halos:
+ * F pointers to the arrays the +1 halo faces copy (NULL, or a NULL entry: the
+ * field itself); offset: F x 3 floats (NULL: none); table: 256 x 16 edge
+ * indices, -1 terminated (NULL: mc_own_table).
+ *
+ * quirks != 0 reproduces how v2/v3 compute the face normals of fields 1 and
+ * 2 (mesh.cpp:741, 808, 1509-1600, 1644): the fifth triangle's normal is
+ * computed only when field 0 has five triangles (`tris1 == 5`), the SSE
+ * path writes normal slots 0-3 from whatever the triangle slots hold, and
+ * v3's scalar path for field 2 runs to field 1's triangle count.  Normal and
+ * triangle slots keep their values from cube to cube within a slab, as the
+ * reference's stack arrays do; a vertex whose normal used a slot never
+ * written in its slab (uninitialised in the reference) is flagged in
+ * `unsure`.  quirks == 0 computes every triangle's own normal.
+ *
+ * cases (F x C x N, optional) receives each cube's case index; vch
+ * (optional) each vertex's channel + C * field; fnrm (optional, 3 floats per
+ * triangle, indexed like idx) each triangle's face normal as used.  Returns
+ * 0, or -1 when max_v or max_i is too small (counts are still complete). */
+int ora_mesh_fields(const float *const *fields, const float *const *halos, int F, const float *offset, int W,
+                    int H, int C, float iso, float cell, const int *table, int slabs, int share, int quirks,
+                    unsigned char *cases, float *pos, float *nrm, int *vch, unsigned char *unsure, long max_v,
+                    unsigned *idx, float *fnrm, long max_i, long *n_v, long *n_i)
 {
     const int D = W;
     const long N = (long)W * H * D;
@@ -184,8 +207,9 @@ int ora_mesh(const float *field, int W, int H, int C, float iso, float cell, flo
         mc_own_table(own);
         table = own;
     }
+    if (F < 1 || F > 3) return -1;
     const long ne = (long)(W + 1) * (H + 1) * (D + 1);
-    int *emap = (int *)malloc(sizeof(int) * 3 * ne);
+    int *emap = (int *)malloc(sizeof(int) * 3 * ne * F);
     if (!emap) return -1;
     long nv = 0, ni = 0;
     int eax[12], eo[12][3], ea[12], eb[12];
@@ -197,73 +221,125 @@ int ora_mesh(const float *field, int W, int H, int C, float iso, float cell, flo
             if (ca != cb) eax[e] = d;
         }
     }
+    /* per field: triangle slots A, B, C and normal slots (5 x 3 floats each)
+     * and whether each slot was written in this slab */
+    float sv[3][3][5][3], sn[3][5][3];
+    int sv_ok[3][5], sn_ok[3][5];
+    memset(sv, 0, sizeof(sv));
+    memset(sn, 0, sizeof(sn));
     for (int s = 0; s < slabs; s++) {
         const int z0 = (D / slabs) * s;
         const int z1 = s == slabs - 1 ? D : z0 + D / slabs;
+        memset(sv_ok, 0, sizeof(sv_ok));
+        memset(sn_ok, 0, sizeof(sn_ok));
         for (int c = 0; c < C; c++) {
             if (c == 0 || !share)
-                for (long i = 0; i < 3 * ne; i++) emap[i] = -1;
+                for (long i = 0; i < 3 * ne * F; i++) emap[i] = -1;
             for (int gz = z0; gz < z1; gz++)
                 for (int gy = 0; gy < H; gy++)
                     for (int gx = 0; gx < W; gx++) {
-                        float val[8], px[8], py[8], pz[8];
-                        int cs = 0;
-                        for (int i = 0; i < 8; i++) {
-                            const int x = gx + kCorner[i][0], y = gy + kCorner[i][1], z = gz + kCorner[i][2];
-                            val[i] = mc_corner_value(field, W, H, c, x, y, z);
-                            px[i] = ((float)gx + (float)kCorner[i][0]) * cell;
-                            py[i] = ((float)gy + (float)kCorner[i][1]) * cell;
-                            pz[i] = ((float)gz + (float)kCorner[i][2]) * cell;
-                            if (val[i] > iso) cs |= 1 << i;
-                        }
-                        if (cases) cases[c * N + gx + (long)gy * W + (long)gz * W * H] = (unsigned char)cs;
-                        const int emask = mc_edge_mask(cs);
-                        float vx[12], vy[12], vz[12];
-                        for (int e = 0; e < 12; e++) {
-                            if (!(emask & (1 << e))) continue;
-                            const int a = ea[e], b = eb[e];
-                            const float T = (iso - val[a]) / (val[b] - val[a]);
-                            vx[e] = px[a] + (px[b] - px[a]) * T;
-                            vy[e] = py[a] + (py[b] - py[a]) * T;
-                            vz[e] = pz[a] + (pz[b] - pz[a]) * T;
-                            if (x_offset != 0.0f) vx[e] = vx[e] + x_offset;
-                        }
-                        const int *tl = table + cs * 16;
-                        for (int t = 0; t < 5 && tl[3 * t] != -1; t++) {
-                            const int e0 = tl[3 * t], e1 = tl[3 * t + 1], e2 = tl[3 * t + 2];
-                            const float ux = vx[e1] - vx[e0], uy = vy[e1] - vy[e0], uz = vz[e1] - vz[e0];
-                            const float wx = vx[e2] - vx[e0], wy = vy[e2] - vy[e0], wz = vz[e2] - vz[e0];
-                            const float nx = uy * wz - uz * wy;
-                            const float ny = uz * wx - ux * wz;
-                            const float nz = ux * wy - uy * wx;
-                            if (fnrm && ni < max_i) {
-                                fnrm[ni] = nx;
-                                fnrm[ni + 1] = ny;
-                                fnrm[ni + 2] = nz;
+                        int tris0 = 0, tris1 = 0;
+                        for (int f = 0; f < F; f++) {
+                            const float *hf = halos && halos[f] ? halos[f] : fields[f];
+                            float val[8], px[8], py[8], pz[8];
+                            int cs = 0;
+                            for (int i = 0; i < 8; i++) {
+                                const int x = gx + kCorner[i][0], y = gy + kCorner[i][1], z = gz + kCorner[i][2];
+                                val[i] = mc_corner_value(fields[f], hf, W, H, c, x, y, z);
+                                px[i] = ((float)gx + (float)kCorner[i][0]) * cell;
+                                py[i] = ((float)gy + (float)kCorner[i][1]) * cell;
+                                pz[i] = ((float)gz + (float)kCorner[i][2]) * cell;
+                                if (val[i] > iso) cs |= 1 << i;
                             }
-                            for (int k = 0; k < 3; k++) {
-                                const int e = tl[3 * t + k];
-                                const long ox = gx + eo[e][0], oy = gy + eo[e][1], oz = gz + eo[e][2];
-                                const long key = eax[e] * ne + ox + oy * (W + 1) + oz * (long)(W + 1) * (H + 1);
-                                int o = emap[key];
-                                if (o < 0) {
-                                    o = (int)nv++;
-                                    emap[key] = o;
-                                    if (o < max_v) {
-                                        pos[3 * o] = vx[e];
-                                        pos[3 * o + 1] = vy[e];
-                                        pos[3 * o + 2] = vz[e];
-                                        nrm[3 * o] = nrm[3 * o + 1] = nrm[3 * o + 2] = 0.0f;
-                                        if (vch) vch[o] = c;
+                            if (cases)
+                                cases[((long)f * C + c) * N + gx + (long)gy * W + (long)gz * W * H] = (unsigned char)cs;
+                            const int emask = mc_edge_mask(cs);
+                            const float ox = offset ? offset[3 * f] : 0.0f, oy = offset ? offset[3 * f + 1] : 0.0f,
+                                        oz = offset ? offset[3 * f + 2] : 0.0f;
+                            float vx[12], vy[12], vz[12];
+                            for (int e = 0; e < 12; e++) {
+                                if (!(emask & (1 << e))) continue;
+                                const int a = ea[e], b = eb[e];
+                                const float T = (iso - val[a]) / (val[b] - val[a]);
+                                vx[e] = px[a] + (px[b] - px[a]) * T;
+                                vy[e] = py[a] + (py[b] - py[a]) * T;
+                                vz[e] = pz[a] + (pz[b] - pz[a]) * T;
+                                if (ox != 0.0f) vx[e] = vx[e] + ox;
+                                if (oy != 0.0f) vy[e] = vy[e] + oy;
+                                if (oz != 0.0f) vz[e] = vz[e] + oz;
+                            }
+                            int *map = emap + (long)f * 3 * ne;
+                            const int *tl = table + cs * 16;
+                            int nt = 0;
+                            while (nt < 5 && tl[3 * nt] != -1) {
+                                for (int k = 0; k < 3; k++) {
+                                    const int e = tl[3 * nt + k];
+                                    sv[f][k][nt][0] = vx[e];
+                                    sv[f][k][nt][1] = vy[e];
+                                    sv[f][k][nt][2] = vz[e];
+                                }
+                                sv_ok[f][nt] = 1;
+                                nt++;
+                            }
+                            if (f == 0) tris0 = nt;
+                            if (f == 1) tris1 = nt;
+                            /* the normal slots this cube computes: [0, hi), plus slot 4 when `fifth` */
+                            int hi = nt, fifth = 0;
+                            if (quirks && f > 0) {
+                                if (nt >= 2) {
+                                    hi = 4;
+                                    fifth = tris0 == 5;
+                                } else {
+                                    hi = (F == 3 && f == 2) ? tris1 : nt;
+                                }
+                            } else if (nt == 5) {
+                                hi = 4;
+                                fifth = 1;
+                            }
+                            for (int t = 0; t < hi + fifth; t++) {
+                                const int sl = t < hi ? t : 4;
+                                const float *A = sv[f][0][sl], *B = sv[f][1][sl], *Cc = sv[f][2][sl];
+                                const float ux = B[0] - A[0], uy = B[1] - A[1], uz = B[2] - A[2];
+                                const float wx = Cc[0] - A[0], wy = Cc[1] - A[1], wz = Cc[2] - A[2];
+                                sn[f][sl][0] = uy * wz - uz * wy;
+                                sn[f][sl][1] = uz * wx - ux * wz;
+                                sn[f][sl][2] = ux * wy - uy * wx;
+                                sn_ok[f][sl] = sv_ok[f][sl];
+                            }
+                            for (int t = 0; t < nt; t++) {
+                                const float nx = sn[f][t][0], ny = sn[f][t][1], nz = sn[f][t][2];
+                                const int sure = sn_ok[f][t];
+                                if (fnrm && ni < max_i) {
+                                    fnrm[ni] = nx;
+                                    fnrm[ni + 1] = ny;
+                                    fnrm[ni + 2] = nz;
+                                }
+                                for (int k = 0; k < 3; k++) {
+                                    const int e = tl[3 * t + k];
+                                    const long ex = gx + eo[e][0], ey = gy + eo[e][1], ez = gz + eo[e][2];
+                                    const long key = eax[e] * ne + ex + ey * (W + 1) + ez * (long)(W + 1) * (H + 1);
+                                    int o = map[key];
+                                    if (o < 0) {
+                                        o = (int)nv++;
+                                        map[key] = o;
+                                        if (o < max_v) {
+                                            pos[3 * o] = vx[e];
+                                            pos[3 * o + 1] = vy[e];
+                                            pos[3 * o + 2] = vz[e];
+                                            nrm[3 * o] = nrm[3 * o + 1] = nrm[3 * o + 2] = 0.0f;
+                                            if (vch) vch[o] = c + C * f;
+                                            if (unsure) unsure[o] = 0;
+                                        }
                                     }
+                                    if (o < max_v) {
+                                        nrm[3 * o] += nx;
+                                        nrm[3 * o + 1] += ny;
+                                        nrm[3 * o + 2] += nz;
+                                        if (unsure && !sure) unsure[o] = 1;
+                                    }
+                                    if (ni < max_i) idx[ni] = (unsigned)o;
+                                    ni++;
                                 }
-                                if (o < max_v) {
-                                    nrm[3 * o] += nx;
-                                    nrm[3 * o + 1] += ny;
-                                    nrm[3 * o + 2] += nz;
-                                }
-                                if (ni < max_i) idx[ni] = (unsigned)o;
-                                ni++;
                             }
                         }
                     }

@@ -12,9 +12,10 @@ int mc_edge_mask(int c);
 int mc_triangles(int c, int *tri);
 int mc_triangle_count(int c);
 void mc_own_table(int *table);
-int ora_mesh(const float *field, int W, int H, int C, float iso, float cell, float x_offset, const int *table,
-             int slabs, int share, unsigned char *cases, float *pos, float *nrm, int *vch, long max_v,
-             unsigned *idx, float *fnrm, long max_i, long *n_v, long *n_i);
+int ora_mesh_fields(const float *const *fields, const float *const *halos, int F, const float *offset, int W,
+                    int H, int C, float iso, float cell, const int *table, int slabs, int share, int quirks,
+                    unsigned char *cases, float *pos, float *nrm, int *vch, unsigned char *unsure, long max_v,
+                    unsigned *idx, float *fnrm, long max_i, long *n_v, long *n_i);
 
 #ifdef __cplusplus
 }

@@ -126,24 +126,38 @@ def _ref_state(wl, steps):
     return ref, p
 
 
+SHIFT = np.float32(32 * 3.5)
+VIEW_OFFSETS = np.array([[0, 0, 0], [SHIFT, 0, 0], [0, 0, SHIFT]], np.float32)
+
+
 @needs_ref
-@pytest.mark.parametrize("case", [("cfg0", 1), ("cfg0", 4), ("sobel_none", 2), ("four", 2)])
-def test_restatement_reproduces_reference_mesh(case):
-    """generate_mesh_v1 of the reference build (two mesh threads, vertex map
-    shared by channels, no stitching) equals the restatement run with the
-    reference's own table: positions, normals and indices bit for bit."""
+@pytest.mark.parametrize("case", [("cfg0", 1), ("cfg0", 5), ("sobel_none", 2), ("four", 3)])
+@pytest.mark.parametrize("view", [0, 1, 2])
+def test_restatement_reproduces_reference_mesh(case, view):
+    """generate_mesh_v1/v2/v3 of the reference build (two mesh threads,
+    vertex maps shared by channels, no stitching) equal the restatement run
+    with the reference's own table, its halo sources (the +1 faces of
+    U_SUM_RB and H_RB copy U_SUM and H) and its normal-slot quirks: positions
+    and indices bit for bit, normals bit for bit except on vertices whose
+    normal read a slot the reference never wrote (uninitialised memory)."""
     name, steps = case
     wl = LC.four_channels() if name == "four" else LC.variant(name)
     ref, p = _ref_state(wl, steps)
     _, tri_table, _ = _ref_tables()
-    a = O.mesh_reference(ref)
-    b = O.mesh_restated(ref.get("RBB"), 32, 32, p["channels"], np.float32(p["iso_value"]), table=tri_table,
-                        slabs=2, share_channels=True)
+    fields = [ref.get("RBB"), ref.get("U_SUM_RB"), ref.get("H_RB")][:view + 1]
+    halos = [ref.get("A"), ref.get("U_SUM"), ref.get("H")][:view + 1]
+    a = O.mesh_reference(ref, view)
+    b = O.mesh_restated(fields, 32, 32, p["channels"], np.float32(p["iso_value"]), offsets=VIEW_OFFSETS[:view + 1],
+                        table=tri_table, slabs=2, share_channels=True, halos=halos, quirks=True)
     assert a.n_triangles > 1000
     assert a.n_vertices == b.n_vertices and a.n_triangles == b.n_triangles
     assert np.array_equal(a.indices, b.indices)
     assert np.array_equal(a.positions.view(np.uint32), b.positions.view(np.uint32))
-    assert np.array_equal(a.normals.view(np.uint32), b.normals.view(np.uint32))
+    same = (a.normals.view(np.uint32) == b.normals.view(np.uint32)).all(axis=1)
+    assert (same | b.unsure).all()
+    if view == 0:
+        assert not b.unsure.any()
+    assert b.unsure.mean() < 0.05
 
 
 @needs_ref
@@ -159,7 +173,7 @@ def test_reference_mesh_of_empty_grid_is_empty():
 
 def test_restatement_own_vs_reference_table_same_case_indices():
     """Case indices and triangle counts do not depend on the table's
-    triangulation: the restatement with either table gives the same cases."""
+    triangulation: the restatement's count equals the sum of per-case counts."""
     wl = LC.variant("cfg0")
     f = wl.A0
     m = O.mesh_restated(f, 32, 32, 3, 0.5, slabs=2, share_channels=True)
@@ -167,14 +181,35 @@ def test_restatement_own_vs_reference_table_same_case_indices():
     assert m.n_triangles == int(counts[m.cases].sum())
 
 
+def test_quirk_free_normals_are_face_normal_sums():
+    """Without the quirks every vertex normal is the sum, in creation order,
+    of the face normals of the triangles that use it."""
+    wl = LC.four_channels()
+    rng = np.random.default_rng(4)
+    fields = [wl.A0, rng.uniform(0, 1, wl.A0.shape).astype(np.float32)]
+    m = O.mesh_restated(fields, 32, 32, 4, 0.5, offsets=VIEW_OFFSETS[:2], slabs=2, share_channels=True)
+    tri = m.indices.reshape(-1, 3)
+    acc = np.zeros_like(m.normals)
+    for t in range(tri.shape[0]):
+        for v in tri[t]:
+            acc[v] = (acc[v] + m.face_normals[t]).astype(np.float32)
+    assert np.array_equal(acc.view(np.uint32), m.normals.view(np.uint32))
+
+
 # ------------------------------------------------------------ CUDA mesher
 
-def _gpu_mesh(field, W, H, C, iso, **kw):
+def _gpu_mesh(fields, W, H, C, iso, halos=None, **kw):
     import torch
     from lenia_b200.mesh import Mesher
-    t = torch.from_numpy(np.ascontiguousarray(field, np.float32).reshape(-1)).cuda()
-    ms = Mesher(W, H, C, iso_value=iso, **kw)
-    ms.run(t)
+    if isinstance(fields, np.ndarray):
+        fields = [fields]
+    ts = [torch.from_numpy(np.ascontiguousarray(f, np.float32).reshape(-1)).cuda() for f in fields]
+    hs = None
+    if halos is not None:
+        hs = [None if h is None else torch.from_numpy(np.ascontiguousarray(h, np.float32).reshape(-1)).cuda()
+              for h in halos]
+    ms = Mesher(W, H, C, iso_value=iso, fields=len(ts), **kw)
+    ms.run(ts, halos=hs)
     torch.cuda.synchronize()
     return ms.arrays(cases=True)
 
@@ -190,7 +225,7 @@ def _assert_same(g, o, label=""):
 
 
 MODES = [dict(slabs=2, share_channels=True), dict(slabs=1, share_channels=False),
-         dict(slabs=3, share_channels=True), dict(slabs=1, share_channels=True, x_offset=112.0)]
+         dict(slabs=3, share_channels=True), dict(slabs=1, share_channels=True, offsets=[(112.0, 0.0, -3.5)])]
 
 
 @pytest.mark.gpu
@@ -218,6 +253,23 @@ def test_gpu_mesh_matches_restatement_shapes(shape):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("nfields", [2, 3])
+def test_gpu_mesh_matches_restatement_fields(nfields):
+    """Fields meshed together (the U and H views), each with its own halo
+    source and offset, in both slab/sharing modes."""
+    W, H, C = 24, 20, 3
+    rng = np.random.default_rng(nfields)
+    fields = [rng.uniform(0, 1, size=(C, W, H, W)).astype(np.float32) for _ in range(nfields)]
+    halos = [None] + [rng.uniform(0, 1, size=(C, W, H, W)).astype(np.float32) for _ in range(nfields - 1)]
+    offs = [(0, 0, 0), (84.0, 0, 0), (0, 0, 84.0)][:nfields]
+    for kw in (dict(slabs=2, share_channels=True), dict(slabs=1, share_channels=False)):
+        o = O.mesh_restated(fields, W, H, C, 0.5, offsets=offs, halos=halos, **kw)
+        g = _gpu_mesh(fields, W, H, C, 0.5, halos=halos, offsets=offs, **kw)
+        assert o.n_triangles > 10000
+        _assert_same(g, o, f"{nfields} {kw}")
+
+
+@pytest.mark.gpu
 def test_gpu_mesh_empty_and_full():
     for value in (0.0, 1.0):
         f = np.full((2, 16, 16, 16), value, np.float32)
@@ -228,41 +280,68 @@ def test_gpu_mesh_empty_and_full():
             assert g.n_triangles == 0 and g.n_vertices == 0
 
 
-@pytest.mark.gpu
-def test_gpu_mesh_of_world_snapshot():
-    """lenia_mesh_world on RBB after steps equals the restatement of the
-    world's grid at that step."""
-    from lenia_b200.mesh import Mesher
+def _world_after(wl, steps):
     from lenia_b200.world import World
-    wl = LC.four_channels()
     w = World(wl.desc, wl.kernels)
     w.set_snapshots(True)
     w.set_state(wl.A0)
-    w.step(3)
-    A = w.get("A")
-    ms = Mesher(32, 32, 4, iso_value=wl.desc.iso_value)
-    ms.run_world(w, "RBB")
+    w.step(steps)
+    return w
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("view", ["NORMAL", "U", "H"])
+def test_gpu_mesh_of_world_views(view):
+    """lenia_mesh_world for each view equals the restatement of the world's
+    snapshots with the reference's halo sources and offsets."""
+    from lenia_b200.mesh import Mesher
+    wl = LC.four_channels()
+    w = _world_after(wl, 3)
+    nf = {"NORMAL": 1, "U": 2, "H": 3}[view]
+    fields = [w.get("RBB"), w.get("U_SUM_RB"), w.get("H_RB")][:nf]
+    halos = [w.get("A"), w.get("U_SUM"), w.get("H")][:nf]
+    ms = Mesher.for_view(view, 32, 32, 4, iso_value=wl.desc.iso_value)
+    ms.run_world(w, view)
     g = ms.arrays(cases=True)
-    o = O.mesh_restated(A, 32, 32, 4, np.float32(wl.desc.iso_value), slabs=2, share_channels=True)
+    o = O.mesh_restated(fields, 32, 32, 4, np.float32(wl.desc.iso_value), offsets=VIEW_OFFSETS[:nf], halos=halos,
+                        slabs=2, share_channels=True)
     assert o.n_triangles > 1000
-    _assert_same(g, o, "world")
+    _assert_same(g, o, view)
 
 
 @pytest.mark.gpu
 def test_gpu_mesh_config1_size():
     """128^3 x 4 channels, the single-world size, after two steps."""
     from lenia_b200.mesh import Mesher
-    from lenia_b200.world import World
     wl = P.config1()
-    w = World(wl.desc, wl.kernels)
-    w.set_snapshots(True)
-    w.set_state(wl.A0)
-    w.step(2)
-    A = w.get("A")
+    w = _world_after(wl, 2)
+    A = w.get("RBB")
     for kw in (dict(slabs=2, share_channels=True), dict(slabs=1, share_channels=False)):
         ms = Mesher(128, 128, 4, iso_value=wl.desc.iso_value, **kw)
-        ms.run_world(w, "RBB")
+        ms.run_world(w, "NORMAL")
         g = ms.arrays(cases=True)
         o = O.mesh_restated(A, 128, 128, 4, np.float32(wl.desc.iso_value), **kw)
         assert o.n_triangles > 10000
         _assert_same(g, o, str(kw))
+
+
+def test_ply_and_obj_dumps(tmp_path):
+    """The PLY/OBJ writers emit every vertex and face of a mesh."""
+    from lenia_b200.mesh import MeshArrays, write_obj, write_ply
+    f, W, H, C = _closed_field(5, W=16, H=16, C=1)
+    o = O.mesh_restated(f, W, H, C, 0.35, slabs=1, share_channels=False)
+    m = MeshArrays(o.positions, o.normals, o.vertex_channel, o.indices.reshape(-1, 3), o.face_normals)
+    ply = tmp_path / "m.ply"
+    write_ply(str(ply), m)
+    data = ply.read_bytes()
+    head, body = data.split(b"end_header\n", 1)
+    assert f"element vertex {m.n_vertices}".encode() in head
+    assert f"element face {m.n_triangles}".encode() in head
+    assert len(body) == m.n_vertices * 25 + m.n_triangles * 13
+    faces = np.frombuffer(body[m.n_vertices * 25:], dtype=[("k", "u1"), ("i", "<u4", 3)])
+    assert (faces["k"] == 3).all() and np.array_equal(faces["i"], m.indices)
+    obj = tmp_path / "m.obj"
+    write_obj(str(obj), m)
+    lines = obj.read_text().splitlines()
+    assert sum(l.startswith("v ") for l in lines) == m.n_vertices
+    assert sum(l.startswith("f ") for l in lines) == m.n_triangles
