@@ -13,19 +13,39 @@
 // Every float operation keeps the reference's order and rounding (this file
 // is compiled with -fmad=false), so outputs match the CPU restatement bit for
 // bit given the same inputs.
+//
+// A block owns a 32 x 8 x kFlowZ tile of cells; per field (SUM, then each H
+// channel) one thread copies the field's tile with its halo into shared
+// memory with a TMA tensor load (zero outside the grid, which is the zero
+// border and the never-written halo edges), double buffered so that field
+// f+1 lands while field f is used; blocks on the grid boundary then patch the
+// torus/wall halo faces.  Each thread walks its z column with the three
+// planes of 3 x 3 values around it in registers.
+#include <cudaTypedefs.h>
+
 #include "lenia_internal.h"
-#include "async_copy.cuh"
+#include "tma.cuh"
 
 namespace lenia {
 
-constexpr int kFX = 32, kFY = 8, kFZ = 4;  // output tile
-constexpr int kSX = kFX + 2, kSY = kFY + 2, kSZ = kFZ + 2;
+#ifndef LENIA_FLOW_Z
+#define LENIA_FLOW_Z 4
+#endif
+#ifndef LENIA_FLOW_MINB
+#define LENIA_FLOW_MINB 3
+#endif
+constexpr int kFX = 32, kFY = 8;          // output tile in x, y (one thread per column)
+constexpr int kFlowZ = LENIA_FLOW_Z;      // output cells per thread along z
+constexpr int kTX = 40, kTY = kFY + 2;    // staged tile: x from x0 - 4 (TMA x must be 16-byte aligned), y halo
+constexpr int kTZ = kFlowZ + 2;
+constexpr int kTile = kTX * kTY * kTZ;    // floats per staged field
+constexpr unsigned kTmaWaitLimit = 1u << 24;
 
 __device__ __forceinline__ float smax(float a, float b) { return a > b ? a : b; }
 __device__ __forceinline__ float smin(float a, float b) { return a < b ? a : b; }
 
-// Source of tile cell (x, y, z) under the gradient halo rules; false when
-// the cell reads 0 (edges, corners, zero faces).
+// Source of cell (x, y, z) under the gradient halo rules; false when the
+// cell reads 0 (edges, corners, zero faces).
 __device__ __forceinline__ bool gb_source(const Dims &d, int border, int &x, int &y, int &z)
 {
     const int ox = (x < 0) | (x >= d.W), oy = (y < 0) | (y >= d.H), oz = (z < 0) | (z >= d.D);
@@ -44,42 +64,61 @@ __device__ __forceinline__ bool gb_source(const Dims &d, int border, int &x, int
     return true;
 }
 
-// Queues the asynchronous copy of one field's tile (with its one-cell halo).
-__device__ __forceinline__ void issue_tile(float *tile, const float *f, const Dims &d, int x0, int y0, int z0,
-                                           int border)
+// Torus/wall halo faces of a staged tile (the TMA copy left zeros there).
+// Only the cells the gradients read are patched: x0-1..x0+32, y0-1..y0+8,
+// z0-1..z0+kFlowZ, with exactly one coordinate one step outside the grid.
+__device__ void patch_faces(float *tile, const float *f, const Dims &d, int border, int x0, int y0, int z0)
 {
     const int tid = threadIdx.x + threadIdx.y * kFX;
-    for (int e = tid; e < kSX * kSY * kSZ; e += kFX * kFY) {
-        const int lx = e % kSX, ly = (e / kSX) % kSY, lz = e / (kSX * kSY);
-        int x = x0 + lx - 1, y = y0 + ly - 1, z = z0 + lz - 1;
-        const bool ok = gb_source(d, border, x, y, z);
-        const float *src = ok ? f + x + y * d.W + z * d.W * d.H : f;
-        cp_async_f32(tile + e, src, ok);
+    constexpr int RX = kFX + 2, RY = kTY, RZ = kTZ;
+    for (int e = tid; e < RX * RY * RZ; e += kFX * kFY) {
+        const int rx = e % RX, ry = (e / RX) % RY, rz = e / (RX * RY);
+        int x = x0 - 1 + rx, y = y0 - 1 + ry, z = z0 - 1 + rz;
+        const int ox = (x < 0) | (x >= d.W), oy = (y < 0) | (y >= d.H), oz = (z < 0) | (z >= d.D);
+        if (ox + oy + oz != 1) continue;
+        if (x < -1 || x > d.W || y < -1 || y > d.H || z < -1 || z > d.D) continue;
+        const int t = (rx + 3) + ry * kTX + rz * kTX * kTY;
+        tile[t] = gb_source(d, border, x, y, z) ? __ldg(f + x + y * d.W + z * d.W * d.H) : 0.0f;
     }
-    cp_async_commit();
 }
 
-// True when any value of the tile is infinite, NaN or so large that a
-// Sobel product could overflow (block-wide); such blocks take the literal
-// 27-tap multiply-then-add path.
+// True when any staged value is infinite, NaN or so large that a Sobel
+// product could overflow (block-wide); such blocks take the literal 27-tap
+// multiply-then-add path.
 __device__ __forceinline__ bool tile_unsafe(const float *tile)
 {
     const int tid = threadIdx.x + threadIdx.y * kFX;
     int bad = 0;
-    for (int e = tid; e < kSX * kSY * kSZ; e += kFX * kFY) bad |= !(fabsf(tile[e]) < 1.0e30f);
+    for (int e = tid; e < kTile; e += kFX * kFY) bad |= !(fabsf(tile[e]) < 1.0e30f);
     return __syncthreads_or(bad) != 0;
 }
 
-__device__ __forceinline__ float sob_w(int dd) { return dd == 0 ? 2.0f : 1.0f; }
+__host__ __device__ constexpr float sob_w(int dd) { return dd == 0 ? 2.0f : 1.0f; }
 
-// Gradient at tile position (lx, ly, lz) (interior coordinates).
-// Literal path (`literal`): every tap as the reference writes it,
-// acc = acc + v * coef.  Fast path: the coefficients are 0, +-1, +-2, +-4, so
-// for finite v of moderate size v * coef is exact and acc + v * coef rounds
-// exactly like fma(v, coef, acc); zero taps leave acc unchanged (acc starts at
-// +0 and never becomes -0).  Both paths give the same bits.
-template <bool LITERAL>
-__device__ __forceinline__ void sobel_taps(const float *tile, int lx, int ly, int lz, float &gx, float &gy, float &gz)
+// The 27-tap gradient as the reference writes it, acc = acc + v * coef, in
+// (dz, dy, dx) order, around tile index c (returned by value: no local
+// variable of the caller has its address taken).
+__device__ __noinline__ float3 sobel_literal(const float *tile, int c)
+{
+    float ax = 0.0f, ay = 0.0f, az = 0.0f;
+    for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+                const float v = tile[c + dx + dy * kTX + dz * kTX * kTY];
+                ax = ax + v * (sob_w(dx) * sob_w(dy) * (float)dz);
+                ay = ay + v * ((float)dx * sob_w(dy) * sob_w(dz));
+                az = az + v * (sob_w(dx) * (float)dy * sob_w(dz));
+            }
+    return make_float3(ax, ay, az);
+}
+
+// The same gradient from three register planes (values v[(dy+1)*3 + dx+1] of
+// z-1, z, z+1).  The coefficients are 0, +-1, +-2, +-4, so for finite values
+// of moderate size v * coef is exact and acc + v * coef rounds exactly like
+// fma(v, coef, acc); zero taps leave acc unchanged (acc starts at +0 and
+// never becomes -0): the same bits as the literal form.
+__device__ __forceinline__ void sobel_window(const float (&pm)[9], const float (&p0)[9], const float (&pp)[9],
+                                             float &gx, float &gy, float &gz)
 {
     float ax = 0.0f, ay = 0.0f, az = 0.0f;
 #pragma unroll
@@ -88,73 +127,135 @@ __device__ __forceinline__ void sobel_taps(const float *tile, int lx, int ly, in
         for (int dy = -1; dy <= 1; dy++)
 #pragma unroll
             for (int dx = -1; dx <= 1; dx++) {
-                const float v = tile[(lx + 1 + dx) + (ly + 1 + dy) * kSX + (lz + 1 + dz) * kSX * kSY];
-                const float cx = sob_w(dx) * sob_w(dy) * (float)dz;
-                const float cy = (float)dx * sob_w(dy) * sob_w(dz);
-                const float cz = sob_w(dx) * (float)dy * sob_w(dz);
-                if (LITERAL) {
-                    ax = ax + v * cx;
-                    ay = ay + v * cy;
-                    az = az + v * cz;
-                } else {
-                    if (dz != 0) ax = __fmaf_rn(v, cx, ax);
-                    if (dx != 0) ay = __fmaf_rn(v, cy, ay);
-                    if (dy != 0) az = __fmaf_rn(v, cz, az);
-                }
+                const int k = (dy + 1) * 3 + dx + 1;
+                const float v = dz < 0 ? pm[k] : (dz == 0 ? p0[k] : pp[k]);
+                if (dz != 0) ax = __fmaf_rn(v, sob_w(dx) * sob_w(dy) * (float)dz, ax);
+                if (dx != 0) ay = __fmaf_rn(v, (float)dx * sob_w(dy) * sob_w(dz), ay);
+                if (dy != 0) az = __fmaf_rn(v, sob_w(dx) * (float)dy * sob_w(dz), az);
             }
     gx = ax;
     gy = ay;
     gz = az;
 }
 
-__device__ __noinline__ void sobel_literal(const float *tile, int lx, int ly, int lz, float &gx, float &gy, float &gz)
+__device__ __forceinline__ void load_plane(const float *tile, int c, float (&v)[9])
 {
-    sobel_taps<true>(tile, lx, ly, lz, gx, gy, gz);
+#pragma unroll
+    for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+        for (int dx = -1; dx <= 1; dx++) v[(dy + 1) * 3 + dx + 1] = tile[c + dx + dy * kTX];
 }
 
-__device__ __forceinline__ void gradient(const float *tile, int lx, int ly, int lz, int sobel, bool literal,
-                                         float &gx, float &gy, float &gz)
+__global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p, FlowBuffers b,
+                                                   const __grid_constant__ CUtensorMap tm_sum,
+                                                   const __grid_constant__ CUtensorMap tm_h)
 {
-    if (sobel) {
-        if (literal) sobel_literal(tile, lx, ly, lz, gx, gy, gz);
-        else sobel_taps<false>(tile, lx, ly, lz, gx, gy, gz);
-    } else {
-        const int c = (lx + 1) + (ly + 1) * kSX + (lz + 1) * kSX * kSY;
-        gx = (tile[c + 1] - tile[c - 1]) * 0.5f;
-        gy = (tile[c + kSX] - tile[c - kSX]) * 0.5f;
-        gz = (tile[c + kSX * kSY] - tile[c - kSX * kSY]) * 0.5f;
-    }
-}
-
-__global__ void __launch_bounds__(kFX *kFY) k_flow(StepParams p, FlowBuffers b)
-{
-    __shared__ float tiles[2][kSX * kSY * kSZ];
+    extern __shared__ __align__(128) float flow_smem[];
+    __shared__ __align__(8) uint64_t bars[2];
+    float *const tiles[2] = {flow_smem, flow_smem + kTile};
     const Dims &d = p.d;
     const int C = p.C;
     const int N = d.N;
     const int tx = threadIdx.x, ty = threadIdx.y;
+    const bool leader = tx == 0 && ty == 0;
     const int tiles_x = (d.W + kFX - 1) / kFX;
     const int x0 = (blockIdx.x % tiles_x) * kFX;
     const int y0 = (blockIdx.x / tiles_x) * kFY;
-    const int z0 = blockIdx.y * kFZ;
+    const int z0 = blockIdx.y * kFlowZ;
     const int x = x0 + tx, y = y0 + ty;
     const bool col_in = x < d.W && y < d.H;
     const int sobel = p.gradient_mode == kGradSobel;
     const float ta = p.theta_a;
+    const bool patch = p.sobel_border != kBorderNone &&
+                       (x0 == 0 || x0 + kFX >= d.W || y0 == 0 || y0 + kFY >= d.H || z0 == 0 || z0 + kFlowZ >= d.D);
 
-    float na[kFZ][3];
-    // field 0 is SUM, field 1 + c is H channel c; field f+1 loads while f computes
-    issue_tile(tiles[0], b.SUM, d, x0, y0, z0, p.sobel_border);
-    for (int f = 0; f <= C; f++) {
+    if (leader) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    // field 0 is SUM, field 1 + c is H channel c
+    auto issue = [&](int f) {
+        if (!leader) return;
+        const int buf = f & 1;
+        fence_proxy_async();
+        mbar_arrive_expect_tx(&bars[buf], kTile * 4);
+        if (f == 0) tma_load_3d(tiles[buf], &tm_sum, x0 - 4, y0 - 1, z0 - 1, &bars[buf]);
+        else tma_load_4d(tiles[buf], &tm_h, x0 - 4, y0 - 1, z0 - 1, f - 1, &bars[buf]);
+    };
+
+    // Waits for field f's tile, patches its faces and decides the path; returns
+    // whether the literal (non-finite) path is needed.
+    auto land = [&](int f) -> bool {
         float *tile = tiles[f & 1];
-        if (f < C) issue_tile(tiles[(f + 1) & 1], b.H + f * N, d, x0, y0, z0, p.sobel_border);
+        if (!mbar_wait(&bars[f & 1], (unsigned)(f >> 1) & 1u, kTmaWaitLimit) && b.err) atomicOr(b.err, 2);
+        __syncthreads();
+        if (patch) {
+            patch_faces(tile, f == 0 ? b.SUM : b.H + (f - 1) * N, d, p.sobel_border, x0, y0, z0);
+            __syncthreads();
+        }
+        return sobel && tile_unsafe(tile);
+    };
+    // the column: tile index of (x, y, z0 + lz) is col + (lz + 1) * plane
+    const int col = (tx + 4) + (ty + 1) * kTX;
+    constexpr int plane = kTX * kTY;
+    // Gradient of output lz of this column; win holds the Sobel planes.
+    auto grad = [&](const float *tile, bool literal, int lz, float (&win)[3][9], float (&g)[3]) {
+        const int cc = col + (lz + 1) * plane;
+        if (sobel) {
+            if (literal) {
+                const float3 r = sobel_literal(tile, cc);
+                g[0] = r.x;
+                g[1] = r.y;
+                g[2] = r.z;
+            } else {
+                if (lz == 0) {
+                    load_plane(tile, col, win[0]);
+                    load_plane(tile, col + plane, win[1]);
+                }
+                load_plane(tile, cc + plane, win[(lz + 2) % 3]);
+                sobel_window(win[lz % 3], win[(lz + 1) % 3], win[(lz + 2) % 3], g[0], g[1], g[2]);
+            }
+        } else {
+            g[0] = (tile[cc + 1] - tile[cc - 1]) * 0.5f;
+            g[1] = (tile[cc + kTX] - tile[cc - kTX]) * 0.5f;
+            g[2] = (tile[cc + plane] - tile[cc - plane]) * 0.5f;
+        }
+    };
+
+    // field 0: the gradient of SUM (NA), kept in registers for every channel
+    float na[kFlowZ][3];
+    issue(0);
+    issue(1);
+    {
+        const bool literal = land(0);
+        float win[3][9];
+#pragma unroll
+        for (int lz = 0; lz < kFlowZ; lz++) {
+            grad(tiles[0], literal, lz, win, na[lz]);
+            const int z = z0 + lz;
+            if (b.NA && col_in && z < d.D) {
+                const int i = x + y * d.W + z * d.W * d.H;
+                b.NA[i] = na[lz][0];
+                b.NA[N + i] = na[lz][1];
+                b.NA[2 * N + i] = na[lz][2];
+            }
+        }
+        fence_proxy_async();
+        __syncthreads();
+    }
+    // fields 1..C: the gradient of H channel c = f - 1 and the flow epilogue
+    for (int f = 1; f <= C; f++) {
+        float *tile = tiles[f & 1];
+        if (f < C) issue(f + 1);
         // per-cell inputs of this channel, loaded while the tile lands
-        float v3[3][kFZ], gal[kFZ];
+        float v3[3][kFlowZ], gal[kFlowZ];
         unsigned gvalid = 0;  // bit lz: the alpha source of cell lz was written
         const int c = f - 1;
-        if (f > 0 && col_in) {
+        if (col_in) {
 #pragma unroll
-            for (int lz = 0; lz < kFZ; lz++) {
+            for (int lz = 0; lz < kFlowZ; lz++) {
                 const int z = z0 + lz;
                 if (z >= d.D) continue;
                 const int i = x + y * d.W + z * d.W * d.H;
@@ -175,102 +276,127 @@ __global__ void __launch_bounds__(kFX *kFY) k_flow(StepParams p, FlowBuffers b)
                 gvalid |= (valid ? 1u : 0u) << lz;
             }
         }
-        if (f < C) cp_async_wait<1>();
-        else cp_async_wait<0>();
-        __syncthreads();
-        const bool literal = sobel && tile_unsafe(tile);
-        if (f == 0) {
+        const bool literal = land(f);
+        float win[3][9];
 #pragma unroll
-            for (int lz = 0; lz < kFZ; lz++) gradient(tile, tx, ty, lz, sobel, literal, na[lz][0], na[lz][1], na[lz][2]);
-            if (b.NA && col_in) {
-#pragma unroll
-                for (int lz = 0; lz < kFZ; lz++) {
-                    const int z = z0 + lz;
-                    if (z >= d.D) continue;
-                    const int i = x + y * d.W + z * d.W * d.H;
-                    b.NA[i] = na[lz][0];
-                    b.NA[N + i] = na[lz][1];
-                    b.NA[2 * N + i] = na[lz][2];
+        for (int lz = 0; lz < kFlowZ; lz++) {
+            float g[3];
+            grad(tile, literal, lz, win, g);
+            const int z = z0 + lz;
+            if (!col_in || z >= d.D) continue;
+            const int i = x + y * d.W + z * d.W * d.H;
+            const int ci = c * N + i;
+            float alpha;
+            {
+                const float gv = gal[lz];
+                if (!((gvalid >> lz) & 1u)) {
+                    alpha = 0.0f;
+                } else {
+                    float pg = gv / ta;
+                    pg = pg * pg;
+                    alpha = smin(smax(pg, 0.0f), 1.0f);
                 }
             }
-        } else if (col_in) {
-#pragma unroll
-            for (int lz = 0; lz < kFZ; lz++) {
-                const int z = z0 + lz;
-                if (z >= d.D) continue;
-                const int i = x + y * d.W + z * d.W * d.H;
-                const int ci = c * N + i;
-                float nu[3];
-                gradient(tile, tx, ty, lz, sobel, literal, nu[0], nu[1], nu[2]);
-                float alpha;
-                {
-                    const float g = gal[lz];
-                    if (!((gvalid >> lz) & 1u)) {
-                        alpha = 0.0f;
-                    } else {
-                        float pg = g / ta;
-                        pg = pg * pg;
-                        alpha = smin(smax(pg, 0.0f), 1.0f);
-                    }
-                }
-                if (b.PREALPHA) b.PREALPHA[ci] = alpha;
-                if (b.NU) {
-                    b.NU[ci] = nu[0];
-                    b.NU[C * N + ci] = nu[1];
-                    b.NU[2LL * C * N + ci] = nu[2];
-                }
-                if (b.ALPHA) {
-                    // ALPHA = |GRID - GA| with GA read at c*P + i (Q20)
-                    // (GA blocks past the last channel are never written: 0)
-                    const float g = __ldg(b.A + ci);
-                    const int fi = p.alpha_index_fix ? ci : c * d.P + i;
-                    const float ga = fi < C * N ? __ldg(b.GA + fi) : 0.0f;
-                    b.ALPHA[ci] = fabsf(g - ga);
-                }
-                const float a1 = 1.0f - alpha;
-                float f3[3];
-#pragma unroll
-                for (int q = 0; q < 3; q++) f3[q] = nu[q] * a1 - na[lz][q] * alpha;
-                if (b.F) {
-#pragma unroll
-                    for (int q = 0; q < 3; q++) b.F[q * C * N + ci] = f3[q];
-                }
-                float vv[3] = {v3[0][lz], v3[1][lz], v3[2][lz]};
-                const float pos[3] = {(float)x + 0.5f, (float)y + 0.5f, (float)z + 0.5f};
-                if (p.mu_vel) {
-#pragma unroll
-                    for (int q = 0; q < 3; q++) vv[q] = (vv[q] + f3[q]) * p.v_damp;
-                }
-#pragma unroll
-                for (int q = 0; q < 3; q++) {
-                    float m = (p.mu_vel ? vv[q] : f3[q]) * p.timestep;
-                    m = smax(m, -p.ma);
-                    m = smin(m, p.ma);
-                    m = pos[q] + m;
-                    if (p.border == kBorderWall) {
-                        m = smax(m, p.sigma);
-                        m = smin(m, q == 1 ? p.ghs : p.gws);
-                    }
-                    b.MU[q * C * N + ci] = m;
-                }
-                if (!p.mu_vel) {
-#pragma unroll
-                    for (int q = 0; q < 3; q++) vv[q] = (vv[q] + f3[q]) * p.v_damp;
-                }
-#pragma unroll
-                for (int q = 0; q < 3; q++) b.V[q * C * N + ci] = vv[q];
+            if (b.PREALPHA) b.PREALPHA[ci] = alpha;
+            if (b.NU) {
+                b.NU[ci] = g[0];
+                b.NU[C * N + ci] = g[1];
+                b.NU[2LL * C * N + ci] = g[2];
             }
+            if (b.ALPHA) {
+                // ALPHA = |GRID - GA| with GA read at c*P + i (Q20)
+                // (GA blocks past the last channel are never written: 0)
+                const float ga_g = __ldg(b.A + ci);
+                const int fi = p.alpha_index_fix ? ci : c * d.P + i;
+                const float ga = fi < C * N ? __ldg(b.GA + fi) : 0.0f;
+                b.ALPHA[ci] = fabsf(ga_g - ga);
+            }
+            const float a1 = 1.0f - alpha;
+            float f3[3];
+#pragma unroll
+            for (int q = 0; q < 3; q++) f3[q] = g[q] * a1 - na[lz][q] * alpha;
+            if (b.F) {
+#pragma unroll
+                for (int q = 0; q < 3; q++) b.F[q * C * N + ci] = f3[q];
+            }
+            float vv[3] = {v3[0][lz], v3[1][lz], v3[2][lz]};
+            const float pos[3] = {(float)x + 0.5f, (float)y + 0.5f, (float)z + 0.5f};
+            if (p.mu_vel) {
+#pragma unroll
+                for (int q = 0; q < 3; q++) vv[q] = (vv[q] + f3[q]) * p.v_damp;
+            }
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                float m = (p.mu_vel ? vv[q] : f3[q]) * p.timestep;
+                m = smax(m, -p.ma);
+                m = smin(m, p.ma);
+                m = pos[q] + m;
+                if (p.border == kBorderWall) {
+                    m = smax(m, p.sigma);
+                    m = smin(m, q == 1 ? p.ghs : p.gws);
+                }
+                b.MU[q * C * N + ci] = m;
+            }
+            if (!p.mu_vel) {
+#pragma unroll
+                for (int q = 0; q < 3; q++) vv[q] = (vv[q] + f3[q]) * p.v_damp;
+            }
+#pragma unroll
+            for (int q = 0; q < 3; q++) b.V[q * C * N + ci] = vv[q];
         }
+        // every thread is done with this buffer (including its generic writes)
+        // before the next TMA copy into it
+        fence_proxy_async();
         __syncthreads();
     }
 }
 
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+}
+
+cudaError_t encode_tensor_map(CUtensorMap *map, const float *base, int rank, const unsigned long long *dims,
+                              const unsigned *box)
+{
+    if (!g_encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
+        g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    cuuint64_t gdim[5], gstride[4];
+    cuuint32_t bdim[5], estride[5];
+    unsigned long long stride = sizeof(float);
+    for (int i = 0; i < rank; i++) {
+        gdim[i] = dims[i];
+        bdim[i] = box[i];
+        estride[i] = 1;
+        if (i > 0) gstride[i - 1] = stride;
+        stride *= dims[i];
+    }
+    const CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, (void *)base, gdim, gstride,
+                                bdim, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 cudaError_t launch_flow(const StepParams &p, const FlowBuffers &b, cudaStream_t st)
 {
-    const int tiles_x = (p.d.W + kFX - 1) / kFX, tiles_y = (p.d.H + kFY - 1) / kFY;
-    dim3 grid(tiles_x * tiles_y, (p.d.D + kFZ - 1) / kFZ);
+    const Dims &d = p.d;
+    CUtensorMap tm_sum, tm_h;
+    const unsigned long long dsum[3] = {(unsigned long long)d.W, (unsigned long long)d.H, (unsigned long long)d.D};
+    const unsigned long long dh[4] = {(unsigned long long)d.W, (unsigned long long)d.H, (unsigned long long)d.D,
+                                      (unsigned long long)p.C};
+    const unsigned box[4] = {kTX, kTY, kTZ, 1};
+    cudaError_t e = encode_tensor_map(&tm_sum, b.SUM, 3, dsum, box);
+    if (e == cudaSuccess) e = encode_tensor_map(&tm_h, b.H, 4, dh, box);
+    if (e != cudaSuccess) return e;
+    const int tiles_x = (d.W + kFX - 1) / kFX, tiles_y = (d.H + kFY - 1) / kFY;
+    dim3 grid(tiles_x * tiles_y, (d.D + kFlowZ - 1) / kFlowZ);
     dim3 block(kFX, kFY);
-    k_flow<<<grid, block, 0, st>>>(p, b);
+    const size_t smem = 2 * kTile * sizeof(float);
+    k_flow<<<grid, block, smem, st>>>(p, b, tm_sum, tm_h);
     return cudaGetLastError();
 }
 

@@ -546,6 +546,7 @@ lenia_status stage_flow(lenia_world *w)
     b.MU = w->MU;
     b.F = (w->debug || needs_F(w->desc)) ? w->F : nullptr;
     b.ALPHA = (w->debug || w->desc.osc_div_flow) ? w->ALPHA : nullptr;
+    b.err = w->err_flag;
     if (w->debug) {
         b.NA = w->NA;
         b.NU = w->NU;
@@ -880,6 +881,7 @@ lenia_status lenia_sync(lenia_world *w)
     if (e != cudaSuccess) return cuda_fail(w, e, "sync");
     if (flag) {
         cudaMemset(w->err_flag, 0, sizeof(int));
+        if (flag & 2) return fail(w, LENIA_ERR_TIMEOUT, "a tile copy of the flow stage did not complete in time");
         return fail(w, LENIA_ERR_NONFINITE, "non-finite u met in the growth table lookup");
     }
     return LENIA_OK;

@@ -93,6 +93,7 @@ struct FlowBuffers {
     float *F;            // 3*C*N or null
     float *ALPHA;        // C*N or null
     float *NA, *NU, *PREALPHA;  // debug outputs or null (PREALPHA: 4*N flat)
+    int *err;            // bit 2 set when a tile copy did not complete in time
 };
 
 struct TransportBuffers {
