@@ -11,7 +11,7 @@
 // Float operation order and rounding are the reference's (-fmad=false).
 #include "lenia_internal.h"
 #include "growth_common.cuh"
-#include "async_copy.cuh"
+#include "tma.cuh"
 
 namespace lenia {
 
@@ -234,15 +234,20 @@ __global__ void __launch_bounds__(256) k_transport(StepParams p, TransportBuffer
 
 // ------------------------------------------------------------------
 // RT / SRT as a tiled destination gather.  A block owns 32 x 8 x TZ cells
-// (thread = one x, y column of TZ cells).  Per channel the block stages MU and
-// ARR of its cells plus a DD-cell halo (the reference's halo rules applied at
-// load time) in shared memory, then walks the source layers z' upward: the x
+// (thread = one x, y column of TZ cells).  Per channel one thread copies MU
+// and ARR of the block's cells plus a DD-cell halo into shared memory with
+// four TMA tensor loads (zero outside the grid; double buffered across
+// channels); blocks on the grid boundary then patch the DD periodic face
+// layers (transpose_borders copies them whatever the border setting; edges
+// and corners stay 0).  The thread walks the source layers z' upward: the x
 // and y overlap factors of a source depend only on the thread's column, so
 // they are computed once and reused for the (up to 2 DD + 1) destinations of
 // the column that the source reaches.  Each destination still receives its
 // contributions in the reference's (dz, dy, dx) order, with the reference's
 // float operations, so the result is bit-identical.
 constexpr int kTX = 32, kTY = 8, kTZ = 4;
+constexpr int kTBoxX = 40;  // staged x range x0 - 4 .. x0 + 35 (TMA x must be 16-byte aligned)
+constexpr unsigned kTmaWaitLimitT = 1u << 24;
 
 // min(max(si - |d|, 0), clip).  With clip == 1 the clamp is a saturating
 // add: identical for every input (NaN and negative values give +0 either
@@ -274,15 +279,30 @@ __device__ __forceinline__ bool tb_source(const Dims &d, int dd, int &x, int &y,
     return true;
 }
 
+#ifndef LENIA_TRANSPORT_BUFS
+#define LENIA_TRANSPORT_BUFS 1
+#endif
+#ifndef LENIA_TRANSPORT_MINB
+#define LENIA_TRANSPORT_MINB 4
+#endif
+// 1 buffer and 4 blocks per SM measured faster than 2 buffers and 2 blocks
+// (121 vs 157 us at 128^3 x 4 channels): other blocks cover the copy.
+constexpr int kTBufs = LENIA_TRANSPORT_BUFS;  // 2: channel c + 1 lands while c is used
+
 template <int DD, bool TORUS, bool CLIP1>
-__global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, TransportBuffers b)
+__global__ void __launch_bounds__(kTX *kTY, LENIA_TRANSPORT_MINB) k_transport_tiled(StepParams p, TransportBuffers b,
+                                                              const __grid_constant__ CUtensorMap tm_mu,
+                                                              const __grid_constant__ CUtensorMap tm_arr)
 {
-    constexpr int SX = kTX + 2 * DD, SY = kTY + 2 * DD, SZ = kTZ + 2 * DD, SV = SX * SY * SZ;
-    extern __shared__ float tiles[];  // [2 buffers][MU_x, MU_y, MU_z, ARR][SV]
+    constexpr int SX = kTBoxX, SY = kTY + 2 * DD, SZ = kTZ + 2 * DD, SV = SX * SY * SZ;
+    constexpr int OX = 4 - DD;  // staged x of source offset -DD from the tile's first column
+    extern __shared__ __align__(128) float tiles[];  // [kTBufs buffers][MU_x, MU_y, MU_z, ARR][SV]
+    __shared__ __align__(8) uint64_t bars[2];
     const Dims &d = p.d;
     const long long N = d.N;
     const int C = p.C;
     const int tx = threadIdx.x, ty = threadIdx.y;
+    const bool leader = tx == 0 && ty == 0;
     const int tiles_x = (d.W + kTX - 1) / kTX;
     const int x0 = (blockIdx.x % tiles_x) * kTX;
     const int y0 = (blockIdx.x / tiles_x) * kTY;
@@ -292,25 +312,60 @@ __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, Tran
     const bool srt = p.mode_type == kModeSRT;
     const int crt = p.rt_all_channels ? C : (C < 3 ? C : 3);
     const int tid = tx + ty * kTX;
+    const bool patch = x0 - DD < 0 || x0 + kTX + DD > d.W || y0 - DD < 0 || y0 + kTY + DD > d.H || z0 - DD < 0 ||
+                       z0 + kTZ + DD > d.D;
 
-    // queues channel c's MU and ARR tiles (cells plus a DD halo) into buffer c & 1
+    if (leader) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    // queues channel c's MU and ARR tiles (cells plus a DD halo) into buffer c % kTBufs
     auto issue = [&](int c) {
-        float *buf = tiles + (c & 1) * 4 * SV;
-        const float *mux = b.MU + (long long)c * N;
-        const float *muy = b.MU + (long long)(C + c) * N;
-        const float *muz = b.MU + (long long)(2 * C + c) * N;
-        const float *arr = b.ARR + (long long)c * N;
-        for (int e = tid; e < SV; e += kTX * kTY) {
-            const int lx = e % SX, ly = (e / SX) % SY, lz = e / (SX * SY);
-            int gx = x0 + lx - DD, gy = y0 + ly - DD, gz = z0 + lz - DD;
-            const bool ok = tb_source(d, p.dd, gx, gy, gz);
-            const int o = ok ? gx + gy * d.W + gz * d.W * d.H : 0;
-            cp_async_f32(buf + e, mux + o, ok);
-            cp_async_f32(buf + SV + e, muy + o, ok);
-            cp_async_f32(buf + 2 * SV + e, muz + o, ok);
-            cp_async_f32(buf + 3 * SV + e, arr + o, ok);
-        }
-        cp_async_commit();
+        if (!leader) return;
+        float *buf = tiles + (c % kTBufs) * 4 * SV;
+        uint64_t *bar = &bars[c % kTBufs];
+        fence_proxy_async();
+        mbar_arrive_expect_tx(bar, 4 * SV * 4);
+        const int gx = x0 - 4, gy = y0 - DD, gz = z0 - DD;
+        tma_load_4d(buf, &tm_mu, gx, gy, gz, c, bar);
+        tma_load_4d(buf + SV, &tm_mu, gx, gy, gz, C + c, bar);
+        tma_load_4d(buf + 2 * SV, &tm_mu, gx, gy, gz, 2 * C + c, bar);
+        tma_load_4d(buf + 3 * SV, &tm_arr, gx, gy, gz, c, bar);
+    };
+    // the periodic face layers of channel c's tiles: for each grid face the
+    // tile crosses, the cells of its DD layers whose other coordinates are in
+    // the grid (edges and corners keep the copy's zeros)
+    auto patch_faces = [&](int c, float *buf) {
+        const float *src[4] = {b.MU + (long long)c * N, b.MU + (long long)(C + c) * N,
+                               b.MU + (long long)(2 * C + c) * N, b.ARR + (long long)c * N};
+        const int lo[3] = {x0 - DD, y0 - DD, z0 - DD};
+        const int hi[3] = {x0 + kTX + DD, y0 + kTY + DD, z0 + kTZ + DD};
+        const int ext[3] = {d.W, d.H, d.D};
+        for (int a = 0; a < 3; a++)
+            for (int side = 0; side < 2; side++) {
+                const int flo = side == 0 ? lo[a] : (ext[a] > lo[a] ? ext[a] : lo[a]);
+                const int fhi = side == 0 ? (hi[a] < 0 ? hi[a] : 0) : hi[a];
+                if (flo >= fhi) continue;
+                const int a1 = (a + 1) % 3, a2 = (a + 2) % 3;
+                const int l1 = lo[a1] > 0 ? lo[a1] : 0, h1 = hi[a1] < ext[a1] ? hi[a1] : ext[a1];
+                const int l2 = lo[a2] > 0 ? lo[a2] : 0, h2 = hi[a2] < ext[a2] ? hi[a2] : ext[a2];
+                const int nl = fhi - flo, n1 = h1 - l1, n2 = h2 - l2;
+                if (n1 <= 0 || n2 <= 0) continue;
+                for (int e = tid; e < nl * n1 * n2; e += kTX * kTY) {
+                    int g[3];
+                    g[a] = flo + e % nl;
+                    g[a1] = l1 + (e / nl) % n1;
+                    g[a2] = l2 + e / (nl * n1);
+                    const int t = (g[0] - x0 + 4) + (g[1] - y0 + DD) * SX + (g[2] - z0 + DD) * SX * SY;
+                    int gx = g[0], gy = g[1], gz = g[2];
+                    const bool ok = tb_source(d, p.dd, gx, gy, gz);
+                    const long long o = gx + (long long)gy * d.W + (long long)gz * d.W * d.H;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) buf[q * SV + t] = ok ? __ldg(src[q] + o) : 0.0f;
+                }
+            }
     };
 
     float tt[kMaxChannels][kTZ];
@@ -321,21 +376,22 @@ __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, Tran
 
     if (crt > 0) issue(0);
     for (int c = 0; c < crt; c++) {
-        if (c + 1 < crt) {
-            issue(c + 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
+        if (kTBufs == 2 && c + 1 < crt) issue(c + 1);
+        float *buf = tiles + (c % kTBufs) * 4 * SV;
+        if (!mbar_wait(&bars[c % kTBufs], (unsigned)(c / kTBufs) & 1u, kTmaWaitLimitT) && b.err) atomicOr(b.err, 2);
         __syncthreads();
-        const float *tmx = tiles + (c & 1) * 4 * SV, *tmy = tmx + SV, *tmz = tmx + 2 * SV, *tar = tmx + 3 * SV;
+        if (patch) {
+            patch_faces(c, buf);
+            __syncthreads();
+        }
+        const float *tmx = buf, *tmy = buf + SV, *tmz = buf + 2 * SV, *tar = buf + 3 * SV;
         float acc[kTZ];
 #pragma unroll
         for (int j = 0; j < kTZ; j++) acc[j] = 0.0f;
         if (srt) {
 #pragma unroll
             for (int j = 0; j < kTZ; j++) {
-                const int e = (tx + DD) + (ty + DD) * SX + (j + DD) * SX * SY;
+                const int e = (tx + OX + DD) + (ty + DD) * SX + (j + DD) * SX * SY;
                 const float pz = (float)(z0 + j) + 0.5f;
                 float mx = fabsf(px - tmx[e]), my = fabsf(py - tmy[e]), mz = fabsf(pz - tmz[e]);
                 mx = tmin(tmax(p.si - mx, 0.0f), p.clip);
@@ -354,7 +410,7 @@ __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, Tran
                 for (int oy = -DD; oy <= DD; oy++) {
 #pragma unroll
                     for (int ox = -DD; ox <= DD; ox++) {
-                        const int e = (tx + DD + ox) + (ty + DD + oy) * SX + lz * SX * SY;
+                        const int e = (tx + OX + DD + ox) + (ty + DD + oy) * SX + lz * SX * SY;
                         const float mx = overlap<TORUS, CLIP1>(px - tmx[e], p.si, p.clip, d.W);
                         const float my = overlap<TORUS, CLIP1>(py - tmy[e], p.si, p.clip, d.H);
                         const float am = tar[e] * mx;
@@ -379,7 +435,10 @@ __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, Tran
             if (cc == c)
 #pragma unroll
                 for (int j = 0; j < kTZ; j++) tt[cc][j] = acc[j];
-        __syncthreads();  // buffer c & 1 is refilled by issue(c + 2)
+        // buffer c % kTBufs (and its generic patch writes) is done before it is refilled
+        fence_proxy_async();
+        __syncthreads();
+        if (kTBufs == 1 && c + 1 < crt) issue(c + 1);
     }
     if (x >= d.W || y >= d.H) return;
 
@@ -398,16 +457,27 @@ __global__ void __launch_bounds__(kTX *kTY) k_transport_tiled(StepParams p, Tran
 
 cudaError_t launch_transport(const StepParams &p, const TransportBuffers &b, cudaStream_t st)
 {
-    if ((p.mode_type == kModeRT || p.mode_type == kModeSRT) && p.dd >= 1 && p.dd <= 2) {
-        const int tiles_x = (p.d.W + kTX - 1) / kTX, tiles_y = (p.d.H + kTY - 1) / kTY;
-        dim3 grid(tiles_x * tiles_y, (p.d.D + kTZ - 1) / kTZ), block(kTX, kTY);
+    const int crt = p.rt_all_channels ? p.C : (p.C < 3 ? p.C : 3);
+    if ((p.mode_type == kModeRT || p.mode_type == kModeSRT) && p.dd >= 1 && p.dd <= 2 && crt > 0) {
+        const Dims &d = p.d;
+        const int tiles_x = (d.W + kTX - 1) / kTX, tiles_y = (d.H + kTY - 1) / kTY;
+        dim3 grid(tiles_x * tiles_y, (d.D + kTZ - 1) / kTZ), block(kTX, kTY);
         const bool torus = p.border == kBorderTorus;
+        const unsigned long long dmu[4] = {(unsigned long long)d.W, (unsigned long long)d.H,
+                                           (unsigned long long)d.D, 3ull * p.C};
+        const unsigned long long darr[4] = {(unsigned long long)d.W, (unsigned long long)d.H,
+                                            (unsigned long long)d.D, (unsigned long long)p.C};
         auto go = [&](auto kern, int dd) -> cudaError_t {
-            const int sv = (kTX + 2 * dd) * (kTY + 2 * dd) * (kTZ + 2 * dd);
-            const size_t smem = 2 * 4 * (size_t)sv * sizeof(float);
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            const unsigned box[4] = {(unsigned)kTBoxX, (unsigned)(kTY + 2 * dd), (unsigned)(kTZ + 2 * dd), 1u};
+            CUtensorMap tm_mu, tm_arr;
+            cudaError_t e = encode_tensor_map(&tm_mu, b.MU, 4, dmu, box);
+            if (e == cudaSuccess) e = encode_tensor_map(&tm_arr, b.ARR, 4, darr, box);
             if (e != cudaSuccess) return e;
-            kern<<<grid, block, smem, st>>>(p, b);
+            const int sv = kTBoxX * (kTY + 2 * dd) * (kTZ + 2 * dd);
+            const size_t smem = kTBufs * 4 * (size_t)sv * sizeof(float);
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            kern<<<grid, block, smem, st>>>(p, b, tm_mu, tm_arr);
             return cudaGetLastError();
         };
         const bool c1 = p.clip == 1.0f;

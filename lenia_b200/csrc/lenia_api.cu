@@ -581,6 +581,7 @@ lenia_status stage_transport(lenia_world *w)
     b.SUM = w->SUM;
     b.BACK = w->BACK;
     b.TT = w->debug ? w->TT : nullptr;
+    b.err = w->err_flag;
     cudaError_t e;
     {
         ProfScope ps(w, KID_TRANSPORT);
@@ -881,7 +882,7 @@ lenia_status lenia_sync(lenia_world *w)
     if (e != cudaSuccess) return cuda_fail(w, e, "sync");
     if (flag) {
         cudaMemset(w->err_flag, 0, sizeof(int));
-        if (flag & 2) return fail(w, LENIA_ERR_TIMEOUT, "a tile copy of the flow stage did not complete in time");
+        if (flag & 2) return fail(w, LENIA_ERR_TIMEOUT, "a tile copy of the flow or transport stage did not complete in time");
         return fail(w, LENIA_ERR_NONFINITE, "non-finite u met in the growth table lookup");
     }
     return LENIA_OK;

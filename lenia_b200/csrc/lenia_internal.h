@@ -109,6 +109,7 @@ struct TransportBuffers {
     float *SUM;          // N
     float *BACK;         // C*N (transposition soft clip)
     float *TT;           // debug: pre-clamp TT, or null
+    int *err;            // bit 2 set when a tile copy did not complete in time
 };
 
 // Launch wrappers (kernels_*.cu); all are asynchronous on `st`.
