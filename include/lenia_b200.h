@@ -199,6 +199,40 @@ const char *lenia_kernel_name(int kid);
 lenia_status lenia_convolve_noalloc(int width, int height, const float *field, const LeniaKernelParams *kernel,
                                     float *u_out, void *stream);
 
+/* ---- Batches of worlds -------------------------------------------------
+ *
+ * Many independent worlds (any mix of sizes, channels, kernel sets and
+ * modes) stepped together: the reference has no counterpart beyond calling
+ * its step once per world.  Each world keeps only the fields that live from
+ * step to step (A, V, GA, SUM); the buffers of one step belong to a lane, a
+ * stream whose worlds run one after another, and lanes run concurrently.  One
+ * step of every world is captured once into a CUDA graph and replayed, so a
+ * batch step is one graph launch.  Every world computes exactly what a world
+ * of lenia_create computes (bit-identical fields). */
+typedef struct lenia_batch lenia_batch;
+
+/* descs[n_worlds]; kernels: every world's kernels one after another,
+ * kernel_counts[i] of them for world i; lanes: concurrent streams (0 = up to
+ * 64).  Worlds start at 0, like lenia_create's. */
+lenia_status lenia_batch_create(const LeniaWorldDesc *descs, const LeniaKernelParams *kernels,
+                                const int *kernel_counts, int n_worlds, int lanes, lenia_batch **out);
+lenia_status lenia_batch_destroy(lenia_batch *b);
+int lenia_batch_size(const lenia_batch *b);
+/* Field copies of world `world` (A, V, GA or SUM; as lenia_set_field /
+ * lenia_get_field), ordered with the steps on the batch's stream. */
+lenia_status lenia_batch_set_field(lenia_batch *b, int world, int field, const float *src, size_t count,
+                                   int on_device);
+lenia_status lenia_batch_get_field(lenia_batch *b, int world, int field, float *dst, size_t count, int on_device);
+/* n_steps graph launches on the batch's stream; returns when queued. */
+lenia_status lenia_batch_step(lenia_batch *b, int n_steps);
+/* Uses `stream` (a cudaStream_t) for later steps and copies. */
+lenia_status lenia_batch_set_stream(lenia_batch *b, void *stream);
+/* Waits for the batch and reports the first world's device-side error. */
+lenia_status lenia_batch_sync(lenia_batch *b);
+/* Kernel launches one batch step contains (all worlds). */
+int lenia_batch_launches_per_step(const lenia_batch *b);
+const char *lenia_batch_last_error(const lenia_batch *b);
+
 /* ---- Marching cubes --------------------------------------------------
  *
  * Replaces generate_mesh_v1/v2/v3 (mesh.cpp:34-431, 434-1109, 1115-2037)

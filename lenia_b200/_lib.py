@@ -131,6 +131,20 @@ def load() -> ctypes.CDLL:
         "lenia_kernel_name": ([ctypes.c_int], ctypes.c_char_p),
         "lenia_convolve_noalloc": ([ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(LeniaKernelParams),
                                     ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+        "lenia_batch_create": ([ctypes.POINTER(LeniaWorldDesc), ctypes.POINTER(LeniaKernelParams),
+                                ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
+                                ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+        "lenia_batch_destroy": ([P], ctypes.c_int),
+        "lenia_batch_size": ([P], ctypes.c_int),
+        "lenia_batch_set_field": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int],
+                                  ctypes.c_int),
+        "lenia_batch_get_field": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int],
+                                  ctypes.c_int),
+        "lenia_batch_step": ([P, ctypes.c_int], ctypes.c_int),
+        "lenia_batch_set_stream": ([P, ctypes.c_void_p], ctypes.c_int),
+        "lenia_batch_sync": ([P], ctypes.c_int),
+        "lenia_batch_launches_per_step": ([P], ctypes.c_int),
+        "lenia_batch_last_error": ([P], ctypes.c_char_p),
         "lenia_mesher_create": ([ctypes.POINTER(LeniaMeshDesc), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
         "lenia_mesher_destroy": ([P], ctypes.c_int),
         "lenia_mesher_run": ([P, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p,

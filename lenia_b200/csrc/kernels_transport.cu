@@ -199,6 +199,11 @@ __global__ void __launch_bounds__(256) k_transport(StepParams p, TransportBuffer
         const float *vel = p.adv_vel ? b.V : b.F;
         const float ext[3] = {(float)d.W, (float)d.H, (float)d.W};
         const float pos[3] = {px, py, pz};
+        // With |ma| < 1, X = (pos - 0.5) - v + ext lies in (ext - 1, 2 ext):
+        // floorf(X / ext) is 1 exactly when X >= ext (a float X below ext gives
+        // a quotient at most 1 - 2^-24, and X / ext < 2 - 2^-9 for ext <= 256),
+        // so the comparison replaces the division with the same result.
+        const bool one_wrap = fabsf(p.ma) < 1.0f;
         for (int c = 0; c < C; c++) {
             int i0[3];
             float fr[3];
@@ -208,7 +213,8 @@ __global__ void __launch_bounds__(256) k_transport(StepParams p, TransportBuffer
                 v = tmin(tmax(v, -p.ma), p.ma);
                 float X = (pos[q] - 0.5f) - v;
                 X = X + ext[q];
-                X = X - floorf(X / ext[q]) * ext[q];
+                const float k = one_wrap ? (X >= ext[q] ? 1.0f : 0.0f) : floorf(X / ext[q]);
+                X = X - k * ext[q];
                 const float X0 = floorf(X);
                 i0[q] = (int)X0;
                 fr[q] = X - X0;
@@ -217,14 +223,37 @@ __global__ void __launch_bounds__(256) k_transport(StepParams p, TransportBuffer
             const float fx = fr[0], fy = fr[1], fz = fr[2];
             const float nfx = 1.0f - fx, nfy = 1.0f - fy, nfz = 1.0f - fz;
             const int x0 = i0[0], y0 = i0[1], z0 = i0[2];
-            float s = tb_read(arr, d, dd, x0, y0, z0) * nfx * nfy * nfz;
-            s = s + tb_read(arr, d, dd, x0 + 1, y0, z0) * fx * nfy * nfz;
-            s = s + tb_read(arr, d, dd, x0, y0 + 1, z0) * nfx * fy * nfz;
-            s = s + tb_read(arr, d, dd, x0 + 1, y0 + 1, z0) * fx * fy * nfz;
-            s = s + tb_read(arr, d, dd, x0, y0, z0 + 1) * nfx * nfy * fz;
-            s = s + tb_read(arr, d, dd, x0 + 1, y0, z0 + 1) * fx * nfy * fz;
-            s = s + tb_read(arr, d, dd, x0, y0 + 1, z0 + 1) * nfx * fy * fz;
-            s = s + tb_read(arr, d, dd, x0 + 1, y0 + 1, z0 + 1) * fx * fy * fz;
+            float a[8];
+            if (x0 >= 0 && y0 >= 0 && z0 >= 0 && x0 + 1 < d.W && y0 + 1 < d.H && z0 + 1 < d.D) {
+                // all eight corners inside the grid: plain loads
+                const float *q0 = arr + x0 + (long long)y0 * d.W + (long long)z0 * d.W * d.H;
+                const long long sy = d.W, sz = (long long)d.W * d.H;
+                a[0] = __ldg(q0);
+                a[1] = __ldg(q0 + 1);
+                a[2] = __ldg(q0 + sy);
+                a[3] = __ldg(q0 + sy + 1);
+                a[4] = __ldg(q0 + sz);
+                a[5] = __ldg(q0 + sz + 1);
+                a[6] = __ldg(q0 + sz + sy);
+                a[7] = __ldg(q0 + sz + sy + 1);
+            } else {
+                a[0] = tb_read(arr, d, dd, x0, y0, z0);
+                a[1] = tb_read(arr, d, dd, x0 + 1, y0, z0);
+                a[2] = tb_read(arr, d, dd, x0, y0 + 1, z0);
+                a[3] = tb_read(arr, d, dd, x0 + 1, y0 + 1, z0);
+                a[4] = tb_read(arr, d, dd, x0, y0, z0 + 1);
+                a[5] = tb_read(arr, d, dd, x0 + 1, y0, z0 + 1);
+                a[6] = tb_read(arr, d, dd, x0, y0 + 1, z0 + 1);
+                a[7] = tb_read(arr, d, dd, x0 + 1, y0 + 1, z0 + 1);
+            }
+            float s = a[0] * nfx * nfy * nfz;
+            s = s + a[1] * fx * nfy * nfz;
+            s = s + a[2] * nfx * fy * nfz;
+            s = s + a[3] * fx * fy * nfz;
+            s = s + a[4] * nfx * nfy * fz;
+            s = s + a[5] * fx * nfy * fz;
+            s = s + a[6] * nfx * fy * fz;
+            s = s + a[7] * fx * fy * fz;
             tt[c] = s;
         }
     }

@@ -103,6 +103,7 @@ struct lenia_world {
     cudaStream_t own_stream = nullptr;  // created by lenia_create
     int device = 0;
     bool debug = false, snapshots = false;
+    bool shared_scratch = false;  // the per-step buffers belong to a batch lane (see lenia_batch)
     int launches = 0;
     std::string err;
     // device state
@@ -373,16 +374,26 @@ out:
 
 void free_world(lenia_world *w)
 {
-    float *fs[] = {w->A, w->A_next, w->V, w->GA, w->SUM, w->H, w->H_RB, w->U_SUM, w->U_SUM_RB, w->BACK, w->MU,
-                   w->F, w->ALPHA, w->U_S, w->SUM_S, w->RBB, w->NA, w->NU, w->PREALPHA, w->TT, w->U, w->Kc,
-                   w->blur_hat, w->lut_rows, w->ksum};
+    float *fs[] = {w->A, w->A_next, w->V, w->GA, w->SUM, w->H_RB, w->U_SUM_RB, w->RBB, w->NA, w->NU, w->PREALPHA,
+                   w->TT, w->U, w->Kc, w->blur_hat, w->lut_rows, w->ksum};
     for (float *p : fs)
         if (p) cudaFree(p);
-    void *vs[] = {w->XS, w->S, w->lut_base, w->kp_dev, w->tw_x_fwd, w->tw_x_inv, w->tw_y_fwd, w->tw_y_inv,
-                  w->err_flag};
+    void *vs[] = {w->lut_base, w->kp_dev, w->tw_x_fwd, w->tw_x_inv, w->tw_y_fwd, w->tw_y_inv, w->err_flag};
     for (void *p : vs)
         if (p) cudaFree(p);
+    if (!w->shared_scratch) {
+        void *sc[] = {w->H, w->U_SUM, w->BACK, w->MU, w->F, w->ALPHA, w->U_S, w->SUM_S, w->XS, w->S};
+        for (void *p : sc)
+            if (p) cudaFree(p);
+    }
 }
+
+// Per-step buffers a batch lane lends to its worlds (they run one after
+// another on the lane's stream).
+struct WorldScratch {
+    float *H, *U_SUM, *BACK, *MU, *F, *ALPHA, *U_S, *SUM_S;
+    float2 *XS, *S;
+};
 
 // ---------------------------------------------------------------- stages
 
@@ -632,14 +643,10 @@ float *field_ptr(lenia_world *w, int field, size_t *count)
     }
 }
 
-}  // namespace
-
-extern "C" {
-
-const char *lenia_version(void) { return "lenia_b200 0.1 (sm_100a)"; }
-
-lenia_status lenia_create(const LeniaWorldDesc *desc, const LeniaKernelParams *kernels, int n_kernels,
-                          lenia_world **out)
+// A world; with `shared`, the per-step buffers are the lane's and the
+// kernels are built on `stream` (which the world then uses).
+lenia_status create_world(const LeniaWorldDesc *desc, const LeniaKernelParams *kernels, int n_kernels,
+                          const WorldScratch *shared, cudaStream_t stream, lenia_world **out)
 {
     if (!out) return LENIA_ERR_INVALID_ARG;
     *out = nullptr;
@@ -684,16 +691,30 @@ lenia_status lenia_create(const LeniaWorldDesc *desc, const LeniaKernelParams *k
     w->V = dalloc<float>(3 * CN, e);
     w->GA = dalloc<float>(CN, e);
     w->SUM = dalloc<float>(N, e);
-    w->H = dalloc<float>(CN, e);
-    w->H_RB = dalloc<float>(CN, e);
-    w->U_SUM = dalloc<float>(CN, e);
-    w->U_SUM_RB = dalloc<float>(CN, e);
-    w->BACK = dalloc<float>(CN, e);
-    w->MU = dalloc<float>(3 * CN, e);
-    w->U_S = dalloc<float>(CN, e);
-    w->SUM_S = dalloc<float>(N, e);
-    w->XS = dalloc<float2>((size_t)(w->C + 1) * d.HS, e);
-    w->S = dalloc<float2>((size_t)std::max(w->K, w->C + 1) * d.HS, e);
+    if (shared) {
+        w->shared_scratch = true;
+        w->H = shared->H;
+        w->U_SUM = shared->U_SUM;
+        w->BACK = shared->BACK;
+        w->MU = shared->MU;
+        w->F = shared->F;
+        w->ALPHA = shared->ALPHA;
+        w->U_S = shared->U_S;
+        w->SUM_S = shared->SUM_S;
+        w->XS = shared->XS;
+        w->S = shared->S;
+    } else {
+        w->H = dalloc<float>(CN, e);
+        w->H_RB = dalloc<float>(CN, e);
+        w->U_SUM = dalloc<float>(CN, e);
+        w->U_SUM_RB = dalloc<float>(CN, e);
+        w->BACK = dalloc<float>(CN, e);
+        w->MU = dalloc<float>(3 * CN, e);
+        w->U_S = dalloc<float>(CN, e);
+        w->SUM_S = dalloc<float>(N, e);
+        w->XS = dalloc<float2>((size_t)(w->C + 1) * d.HS, e);
+        w->S = dalloc<float2>((size_t)std::max(w->K, w->C + 1) * d.HS, e);
+    }
     const size_t kh = (size_t)d.KX * (d.D / 2 + 1) * (d.H / 2 + 1);
     w->Kc = dalloc<float>(std::max(w->K, 1) * kh, e);
     w->blur_hat = dalloc<float>(kh, e);
@@ -713,8 +734,12 @@ lenia_status lenia_create(const LeniaWorldDesc *desc, const LeniaKernelParams *k
         if (e == cudaSuccess) e = cudaMemcpy(w->tw_y_fwd, c.data(), sizeof(float2) * d.H, cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(w->tw_y_inv, dd.data(), sizeof(float2) * d.H, cudaMemcpyHostToDevice);
     }
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&w->own_stream, cudaStreamNonBlocking);
-    w->stream = w->own_stream;
+    if (shared) {
+        w->stream = stream;
+    } else {
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&w->own_stream, cudaStreamNonBlocking);
+        w->stream = w->own_stream;
+    }
     if (e != cudaSuccess) {
         s = e == cudaErrorMemoryAllocation ? LENIA_ERR_OOM : LENIA_ERR_CUDA;
         fprintf(stderr, "lenia_create: %s\n", cudaGetErrorString(e));
@@ -731,6 +756,18 @@ lenia_status lenia_create(const LeniaWorldDesc *desc, const LeniaKernelParams *k
     }
     *out = w;
     return LENIA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *lenia_version(void) { return "lenia_b200 0.1 (sm_100a)"; }
+
+lenia_status lenia_create(const LeniaWorldDesc *desc, const LeniaKernelParams *kernels, int n_kernels,
+                          lenia_world **out)
+{
+    return create_world(desc, kernels, n_kernels, nullptr, nullptr, out);
 }
 
 lenia_status lenia_destroy(lenia_world *w)
@@ -957,5 +994,291 @@ const char *lenia_kernel_name(int kid) { return kid >= 0 && kid < KID_MAX ? kKer
 int lenia_launches_per_step(const lenia_world *w) { return w ? w->launches : 0; }
 
 const char *lenia_last_error(const lenia_world *w) { return w ? w->err.c_str() : "null world"; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- batches
+//
+// Many independent worlds stepped together.  Each world keeps only what
+// lives from step to step (A, V, GA, SUM, its kernel spectra and growth-table
+// rows); the buffers a step produces and consumes (H, U_SUM, BACK, MU, U_S,
+// SUM_S, F, ALPHA and the half spectra) belong to a lane, a stream whose
+// worlds run one after another.  Lanes run concurrently.  One step of every
+// world is captured into a CUDA graph once and replayed: two graphs, since a
+// step swaps each world's A and A_next.  Every world runs the single-world
+// code above, so its fields are bit-identical to a world stepped alone.
+
+struct BatchLane {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t join = nullptr;
+    WorldScratch sc = {};
+    std::vector<int> worlds;
+};
+
+struct lenia_batch {
+    std::vector<lenia_world *> worlds;
+    std::vector<BatchLane> lanes;
+    cudaStream_t stream = nullptr;  // graph launches, field copies
+    cudaStream_t own_stream = nullptr;
+    cudaEvent_t fork = nullptr;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    int parity = 0;
+    std::string err;
+};
+
+namespace {
+
+lenia_status bfail(lenia_batch *b, lenia_status s, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (b) b->err = buf;
+    return s;
+}
+
+void free_batch(lenia_batch *b)
+{
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (cudaGraphExec_t &g : b->exec)
+        if (g) cudaGraphExecDestroy(g);
+    for (lenia_world *w : b->worlds) {
+        free_world(w);
+        delete w;
+    }
+    for (BatchLane &l : b->lanes) {
+        if (l.stream) cudaStreamSynchronize(l.stream);
+        void *sc[] = {l.sc.H, l.sc.U_SUM, l.sc.BACK, l.sc.MU, l.sc.F, l.sc.ALPHA, l.sc.U_S, l.sc.SUM_S, l.sc.XS, l.sc.S};
+        for (void *p : sc)
+            if (p) cudaFree(p);
+        if (l.join) cudaEventDestroy(l.join);
+        if (l.stream) cudaStreamDestroy(l.stream);
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->own_stream) cudaStreamDestroy(b->own_stream);
+}
+
+// One step of a world on its current stream (lenia_step without snapshots).
+lenia_status step_once(lenia_world *w)
+{
+    lenia_status s;
+    w->launches = 0;
+    if ((s = stage_growth(w)) != LENIA_OK) return s;
+    if ((s = stage_blur(w)) != LENIA_OK) return s;
+    if ((s = stage_flow(w)) != LENIA_OK) return s;
+    return stage_transport(w);
+}
+
+// Captures one step of every world, lanes forked from and joined to the
+// batch stream, into exec[which].
+lenia_status capture_step(lenia_batch *b, int which)
+{
+    cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) return bfail(b, LENIA_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
+    lenia_status s = LENIA_OK;
+    e = cudaEventRecord(b->fork, b->stream);
+    for (size_t l = 0; l < b->lanes.size() && e == cudaSuccess && s == LENIA_OK; l++) {
+        BatchLane &lane = b->lanes[l];
+        e = cudaStreamWaitEvent(lane.stream, b->fork, 0);
+        for (int i : lane.worlds) {
+            if (e != cudaSuccess || s != LENIA_OK) break;
+            lenia_world *w = b->worlds[i];
+            w->stream = lane.stream;
+            s = step_once(w);
+            if (s != LENIA_OK) b->err = "world " + std::to_string(i) + ": " + w->err;
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(lane.join, lane.stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, lane.join, 0);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(b->stream, &graph);
+    for (lenia_world *w : b->worlds) w->stream = b->stream;
+    if (s != LENIA_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return s;
+    }
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec[which], graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return bfail(b, LENIA_ERR_CUDA, "capturing the batch step: %s", cudaGetErrorString(e));
+    return LENIA_OK;
+}
+
+bool batch_field_ok(int field)
+{
+    return field == LENIA_FIELD_A || field == LENIA_FIELD_V || field == LENIA_FIELD_GA || field == LENIA_FIELD_SUM;
+}
+
+}  // namespace
+
+extern "C" {
+
+lenia_status lenia_batch_create(const LeniaWorldDesc *descs, const LeniaKernelParams *kernels,
+                                const int *kernel_counts, int n_worlds, int lanes, lenia_batch **out)
+{
+    if (!descs || !kernel_counts || !out || n_worlds < 1 || lanes < 0) return LENIA_ERR_INVALID_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return LENIA_ERR_NO_DEVICE;
+    }
+    for (int i = 0; i < n_worlds; i++) {
+        const LeniaWorldDesc &d = descs[i];
+        if (d.width < 8 || d.width > 256 || d.height < 8 || d.height > 256 || d.channels < 1 ||
+            d.channels > LENIA_MAX_CHANNELS || kernel_counts[i] < 0 || kernel_counts[i] > LENIA_MAX_KERNELS)
+            return LENIA_ERR_INVALID_ARG;
+    }
+    lenia_batch *b = new lenia_batch();
+    const int L = std::max(1, std::min(lanes == 0 ? 64 : lanes, n_worlds));
+    b->lanes.resize(L);
+    // longest processing time first: the largest world to the lightest lane
+    std::vector<int> order(n_worlds);
+    for (int i = 0; i < n_worlds; i++) order[i] = i;
+    auto cells = [&](int i) {
+        return (long long)descs[i].width * descs[i].height * descs[i].width * descs[i].channels *
+               (1 + kernel_counts[i]);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return cells(a) > cells(c); });
+    std::vector<long long> load(L, 0);
+    for (int i : order) {
+        const int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        b->lanes[l].worlds.push_back(i);
+        load[l] += cells(i);
+    }
+    std::vector<size_t> koff(n_worlds + 1, 0);
+    for (int i = 0; i < n_worlds; i++) koff[i + 1] = koff[i] + kernel_counts[i];
+    b->worlds.assign(n_worlds, nullptr);
+    cudaError_t e = cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking);
+    b->stream = b->own_stream;
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    lenia_status s = LENIA_OK;
+    for (BatchLane &lane : b->lanes) {
+        if (e != cudaSuccess || s != LENIA_OK) break;
+        std::sort(lane.worlds.begin(), lane.worlds.end());
+        e = cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&lane.join, cudaEventDisableTiming);
+        // scratch sized for the lane's largest needs
+        size_t cn = 0, n = 0, xs = 0, sk = 0;
+        bool need_f = false, need_alpha = false;
+        for (int i : lane.worlds) {
+            const LeniaWorldDesc &d = descs[i];
+            const size_t N = (size_t)d.width * d.height * d.width;
+            const size_t hs = (size_t)(d.width / 2 + 1) * d.width * d.height;
+            cn = std::max(cn, (size_t)d.channels * N);
+            n = std::max(n, N);
+            xs = std::max(xs, (size_t)(d.channels + 1) * hs);
+            sk = std::max(sk, (size_t)std::max(kernel_counts[i], d.channels + 1) * hs);
+            need_f = need_f || needs_F(d);
+            need_alpha = need_alpha || d.osc_div_flow;
+        }
+        WorldScratch &sc = lane.sc;
+        sc.H = dalloc<float>(cn, e);
+        sc.U_SUM = dalloc<float>(cn, e);
+        sc.BACK = dalloc<float>(cn, e);
+        sc.MU = dalloc<float>(3 * cn, e);
+        sc.U_S = dalloc<float>(cn, e);
+        sc.SUM_S = dalloc<float>(n, e);
+        sc.F = need_f ? dalloc<float>(3 * cn, e) : nullptr;
+        sc.ALPHA = need_alpha ? dalloc<float>(cn, e) : nullptr;
+        sc.XS = dalloc<float2>(xs, e);
+        sc.S = dalloc<float2>(sk, e);
+        for (int i : lane.worlds) {
+            if (e != cudaSuccess || s != LENIA_OK) break;
+            s = create_world(&descs[i], kernels ? kernels + koff[i] : nullptr, kernel_counts[i], &sc, lane.stream,
+                             &b->worlds[i]);
+            if (s != LENIA_OK) bfail(b, s, "world %d could not be created", i);
+        }
+    }
+    if (e == cudaSuccess && s == LENIA_OK) {
+        for (BatchLane &lane : b->lanes)
+            if (e == cudaSuccess) e = cudaStreamSynchronize(lane.stream);
+        for (lenia_world *w : b->worlds) w->stream = b->stream;
+    }
+    if (e != cudaSuccess && s == LENIA_OK) s = e == cudaErrorMemoryAllocation ? LENIA_ERR_OOM : LENIA_ERR_CUDA;
+    if (s == LENIA_OK) s = capture_step(b, 0);
+    if (s == LENIA_OK) s = capture_step(b, 1);
+    if (s != LENIA_OK) {
+        fprintf(stderr, "lenia_batch_create: %s\n", b->err.empty() ? cudaGetErrorString(e) : b->err.c_str());
+        b->worlds.erase(std::remove(b->worlds.begin(), b->worlds.end(), nullptr), b->worlds.end());
+        free_batch(b);
+        delete b;
+        return s;
+    }
+    *out = b;
+    return LENIA_OK;
+}
+
+lenia_status lenia_batch_destroy(lenia_batch *b)
+{
+    if (!b) return LENIA_ERR_INVALID_ARG;
+    free_batch(b);
+    delete b;
+    return LENIA_OK;
+}
+
+int lenia_batch_size(const lenia_batch *b) { return b ? (int)b->worlds.size() : 0; }
+
+lenia_status lenia_batch_set_stream(lenia_batch *b, void *stream)
+{
+    if (!b) return LENIA_ERR_INVALID_ARG;
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return bfail(b, LENIA_ERR_CUDA, "set_stream: %s", cudaGetErrorString(e));
+    b->stream = (cudaStream_t)stream;
+    for (lenia_world *w : b->worlds) w->stream = b->stream;
+    return LENIA_OK;
+}
+
+lenia_status lenia_batch_set_field(lenia_batch *b, int world, int field, const float *src, size_t count, int on_device)
+{
+    if (!b || world < 0 || world >= (int)b->worlds.size()) return LENIA_ERR_INVALID_ARG;
+    if (!batch_field_ok(field)) return bfail(b, LENIA_ERR_INVALID_ARG, "a batch world keeps only A, V, GA and SUM");
+    const lenia_status s = lenia_set_field(b->worlds[world], field, src, count, on_device);
+    if (s != LENIA_OK) b->err = b->worlds[world]->err;
+    return s;
+}
+
+lenia_status lenia_batch_get_field(lenia_batch *b, int world, int field, float *dst, size_t count, int on_device)
+{
+    if (!b || world < 0 || world >= (int)b->worlds.size()) return LENIA_ERR_INVALID_ARG;
+    if (!batch_field_ok(field)) return bfail(b, LENIA_ERR_INVALID_ARG, "a batch world keeps only A, V, GA and SUM");
+    const lenia_status s = lenia_get_field(b->worlds[world], field, dst, count, on_device);
+    if (s != LENIA_OK) b->err = b->worlds[world]->err;
+    return s;
+}
+
+lenia_status lenia_batch_step(lenia_batch *b, int n_steps)
+{
+    if (!b || n_steps < 0) return LENIA_ERR_INVALID_ARG;
+    for (int i = 0; i < n_steps; i++) {
+        const cudaError_t e = cudaGraphLaunch(b->exec[b->parity], b->stream);
+        if (e != cudaSuccess) return bfail(b, LENIA_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
+        for (lenia_world *w : b->worlds) std::swap(w->A, w->A_next);
+        b->parity ^= 1;
+    }
+    return LENIA_OK;
+}
+
+lenia_status lenia_batch_sync(lenia_batch *b)
+{
+    if (!b) return LENIA_ERR_INVALID_ARG;
+    for (size_t i = 0; i < b->worlds.size(); i++) {
+        const lenia_status s = lenia_sync(b->worlds[i]);
+        if (s != LENIA_OK) return bfail(b, s, "world %zu: %s", i, b->worlds[i]->err.c_str());
+    }
+    return LENIA_OK;
+}
+
+int lenia_batch_launches_per_step(const lenia_batch *b)
+{
+    if (!b) return 0;
+    int n = 0;
+    for (const lenia_world *w : b->worlds) n += w->launches;
+    return n;
+}
+
+const char *lenia_batch_last_error(const lenia_batch *b) { return b ? b->err.c_str() : "null batch"; }
 
 }  // extern "C"

@@ -174,3 +174,27 @@ def config1(seed: int = 1, width: int = 128, mode: int = MODE_RT, radius: int = 
     ks = sample_kernels(rng, 4, radius=radius)
     A0 = seed_cube(rng, desc, width // 2)
     return Workload(desc, ks, A0)
+
+
+CONFIG3_SIZES = (24, 32, 36, 44, 48, 64, 96)
+
+
+def config3(n_worlds: int = 4096, seed: int = 3, sizes: Sequence[int] = CONFIG3_SIZES) -> List[Workload]:
+    """Batched worlds: per world a side drawn uniformly from `sizes` (cubic),
+    3 channels, 9 kernels (one per channel pair) of radius side / 4 drawn as
+    in config 0, central differences with periodic borders, RT or advection
+    reintegration by a fair coin, and its own seeded U(0,1) cube of half the
+    side.  World i draws from default_rng((seed, i))."""
+    out = []
+    for i in range(n_worlds):
+        rng = np.random.default_rng((seed, i))
+        w = int(sizes[int(rng.integers(0, len(sizes)))])
+        mode = MODE_RT if rng.integers(0, 2) == 0 else MODE_ADV
+        desc = WorldDesc(width=w, height=w, channels=3, timestep=0.2, theta_a=2.0,
+                         sigma=0.65, dd=1.0, growth_type=GROWTH_RT, mode_type=mode,
+                         sobel_border=BORDER_TORUS, border=BORDER_TORUS,
+                         gradient_mode=GRADIENT_CENTRAL_DIFF, blur_central_diff=False,
+                         mu_vel=False, adv_vel=True, asymptotic=(False,) * 4, soft_clip=(False,) * 4)
+        ks = sample_kernels(rng, 3, radius=max(2, w // 4))
+        out.append(Workload(desc, ks, seed_cube(rng, desc, w // 2)))
+    return out

@@ -1,0 +1,118 @@
+"""Batches of worlds: bit-identity with worlds stepped alone (GPU), and the
+partition of a batch across ranks (CPU, gloo)."""
+from __future__ import annotations
+
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from lenia_b200 import params as P
+from lenia_b200.batch import shard_worlds, world_cost
+
+
+def test_config3_draws_every_size_and_mode():
+    wls = P.config3(64, seed=1)
+    assert {wl.desc.width for wl in wls} == set(P.CONFIG3_SIZES)
+    assert {wl.desc.mode_type for wl in wls} == {P.MODE_RT, P.MODE_ADV}
+    again = P.config3(3, seed=1)
+    assert all(np.array_equal(a.A0, b.A0) for a, b in zip(wls[:3], again))
+
+
+def test_shard_worlds_partitions_and_balances():
+    wls = P.config3(200, seed=2)
+    costs = [world_cost(wl.desc, len(wl.kernels)) for wl in wls]
+    for n in (1, 2, 3, 8):
+        parts = shard_worlds(costs, n)
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(costs)))
+        loads = [sum(costs[i] for i in p) for p in parts]
+        # LPT bound: no rank exceeds the mean by more than the largest world
+        assert max(loads) - sum(loads) / n <= max(costs)
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world_size, port, n_worlds, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world_size)
+    try:
+        wls = P.config3(n_worlds, seed=5)
+        costs = [world_cost(wl.desc, len(wl.kernels)) for wl in wls]
+        mine = shard_worlds(costs, world_size)[rank]
+        every = [None] * world_size
+        dist.all_gather_object(every, mine)
+        import torch
+        t = torch.tensor([float(sum(costs[i] for i in mine)), float(len(mine))], dtype=torch.float64)
+        dist.all_reduce(t)
+        q.put((rank, every, float(t[0]), int(t[1]), float(sum(costs))))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_shards_over_gloo_ranks():
+    """Two gloo ranks compute the same partition independently; the shards
+    are disjoint and cover the batch, and the reduced totals match."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, 40, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    res.sort()
+    every0, every1 = res[0][1], res[1][1]
+    assert every0 == every1
+    assert sorted(i for part in every0 for i in part) == list(range(40))
+    assert not set(every0[0]) & set(every0[1])
+    assert res[0][2] == res[0][4] and res[0][3] == 40
+
+
+@pytest.mark.gpu
+def test_batch_matches_worlds_stepped_alone():
+    from lenia_b200.batch import Batch
+    from lenia_b200.world import World
+    wls = P.config3(7, seed=11, sizes=(24, 32, 36, 48))
+    b = Batch([wl.desc for wl in wls], [wl.kernels for wl in wls], lanes=3)
+    for i, wl in enumerate(wls):
+        b.set_state(i, wl.A0)
+    alone = []
+    for wl in wls:
+        w = World(wl.desc, wl.kernels)
+        w.set_state(wl.A0.ravel())
+        alone.append(w)
+    for steps in (3, 2):   # an odd count first: the batch alternates its two graphs
+        b.step(steps)
+        for w in alone:
+            w.step(steps)
+        b.sync()
+        for i, w in enumerate(alone):
+            for name in ("A", "V", "GA", "SUM"):
+                got, want = b.get(i, name), w.get(name)
+                assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (i, name, steps)
+    assert b.launches_per_step() >= 6 * len(wls)
+    for w in alone:
+        w.close()
+    b.close()
+
+
+@pytest.mark.gpu
+def test_batch_rejects_scratch_fields():
+    from lenia_b200.batch import Batch
+    from lenia_b200._lib import LeniaError
+    wls = P.config3(2, seed=12, sizes=(24,))
+    b = Batch([wl.desc for wl in wls], [wl.kernels for wl in wls], lanes=2)
+    with pytest.raises(LeniaError):
+        b._check(b._lib.lenia_batch_get_field(b._h, 0, 4, None, 0, 0))  # H lives in the lane
+    b.close()
