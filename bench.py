@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--width", type=int, default=128)
     ap.add_argument("--mode", default="rt", choices=["rt", "adv"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-worlds", type=int, default=512,
+                    help="worlds of the batched measurement (config 3 mix; 0 = skip)")
     return ap.parse_args()
 
 
@@ -242,6 +244,64 @@ def run_reference(args):
     return 0
 
 
+# ------------------------------------------------------------ batches
+def batch_measure(args, rank, n, stream, barrier, max_over_ranks):
+    """World-steps/s of a batch of independent worlds (the config 3 mix:
+    sides 24-96, 3 channels, 9 kernels, RT or advection per world), sharded
+    across the ranks by cost with no exchange while stepping; beside it the
+    plain loop (each world its own World, stepped one after another) over a
+    subset of this rank's worlds."""
+    import torch
+    from lenia_b200 import params as P
+    from lenia_b200.batch import Batch, shard_worlds, world_cost
+    from lenia_b200.world import World
+    wls = P.config3(args.batch_worlds, seed=3)
+    mine = shard_worlds([world_cost(wl.desc, len(wl.kernels)) for wl in wls], n)[rank]
+    sub = [wls[i] for i in mine]
+    b = Batch([wl.desc for wl in sub], [wl.kernels for wl in sub], lanes=64)
+    for i, wl in enumerate(sub):
+        b.set_state(i, wl.A0)
+    b.set_stream(stream.cuda_stream)
+    b.step(3)
+    steps = 10
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.step(steps)
+    e1.record(stream)
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1)) / steps
+    b.sync()
+    launches = b.launches_per_step()
+    b.close()
+    plain = sub[:min(64, len(sub))]
+    ws = []
+    for wl in plain:
+        w = World(wl.desc, wl.kernels)
+        w.set_stream(stream.cuda_stream)
+        w.set_state(wl.A0.ravel())
+        w.step(2)
+        ws.append(w)
+    barrier()
+    e0.record(stream)
+    for _ in range(3):
+        for w in ws:
+            w.step(1)
+    e1.record(stream)
+    barrier()
+    plain_ms = e0.elapsed_time(e1) / 3
+    for w in ws:
+        w.close()
+    cells = sum(wl.desc.width ** 3 * wl.desc.channels for wl in wls)
+    return {"workload": f"{args.batch_worlds} worlds, sides 24-96 (config 3 mix), 3 channels, 9 kernels, "
+                        f"RT or advection per world, sharded over {n} GPU(s)",
+            "world_steps_per_s": args.batch_worlds / (ms / 1000.0), "ms_per_step": ms,
+            "cell_updates_per_s": cells / (ms / 1000.0), "graph_launches_per_step": 1,
+            "gpu_launches_per_step": launches,
+            "plain_world_steps_per_s_per_gpu": len(ws) / (plain_ms / 1000.0),
+            "plain_sample_worlds": len(ws)}
+
+
 # ------------------------------------------------------------ GPU arm
 def run_ours(args):
     import numpy as np
@@ -354,6 +414,8 @@ def run_ours(args):
             "vertices": mesher.n_vertices, "triangles": mesher.n_triangles, "gpu_launches_per_mesh": 5}
     mesher.close()
 
+    batched = batch_measure(args, rank, n, stream, barrier, max_over_ranks) if args.batch_worlds > 0 else None
+
     line = None
     if rank == 0:
         line = {
@@ -375,6 +437,8 @@ def run_ours(args):
             "kernels": kernels_table,
             "mesh": mesh,
         }
+        if batched is not None:
+            line["batched"] = batched
         if n == 1 and not args.no_cpu_baseline:
             rate, dt = cpu_port_rate(wl, 2, 1)
             line["cpu_baseline"] = {
