@@ -27,6 +27,8 @@
 
 #include <stdint.h>
 
+#include <vector>
+
 #include "../restate/oracle_api.h"
 
 /* ---- globals normally defined by main.cpp / render.cpp ---------------- */
@@ -105,6 +107,18 @@ extern float BELL_LUT[BELL_LUT_SIZE];
 
 /* The kernel-preview mesh is rendering only (render.cpp:216-352). */
 void rebuild_kernel_mesh(Vertex *v) { (void)v; }
+
+/* rand()/srand() of the reference's platform (the MSVC C runtime): the linear
+ * congruential generator x = 214013 x + 2531011 (mod 2^32), returning bits
+ * 16..30.  Defined here with protected visibility so that the reference's
+ * calls in this library bind to it instead of the C library's generator. */
+static unsigned g_rand_state = 1;
+extern "C" __attribute__((visibility("protected"))) void srand(unsigned seed) noexcept { g_rand_state = seed; }
+extern "C" __attribute__((visibility("protected"))) int rand(void) noexcept
+{
+    g_rand_state = g_rand_state * 214013u + 2531011u;
+    return (int)((g_rand_state >> 16) & 0x7fff);
+}
 
 /* Corner positions of a cube in the order mesh.cpp:19-32 samples them. */
 static const int kCorner[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 0, 1}, {0, 0, 1},
@@ -471,6 +485,36 @@ int ref_get_padded(int field, float *out)
     }
     memcpy(out, src, sizeof(float) * GRID_PADDED * blocks);
     return GRID_PADDED * blocks;
+}
+
+/* generate_random (lenia.cpp:370-429) after srand(seed), with the channel
+ * count set by ref_set_params: writes the kernels it draws (up to max_k) and
+ * the neighbourhood; the seeded grid (seed_grid_gaussian) is then in GRID
+ * (ref_get_field A).  Returns kernel_count. */
+int ref_generate_random(unsigned seed, ora_kernel *out, int max_k, float *neighborhood_out)
+{
+    static std::vector<char> kverts;
+    static IDirect3DVertexBuffer9 kvb;
+    kverts.resize((size_t)GRID_SIZE * 6 * MAX_KERNELS * sizeof(Vertex));
+    kvb.mem = kverts.data();
+    kvb.bytes = kverts.size();
+    kernel_verts = &kvb;
+    srand(seed);
+    generate_random();
+    for (int i = 0; i < kernel_count && i < max_k; i++) {
+        const Kernel &k = kernels[i];
+        out[i].radius = k.radius;
+        out[i].beta_size = k.beta_size;
+        for (int e = 0; e < 12; e++) out[i].b[e] = e < k.beta_size ? k.b[e] : 0.0f;
+        out[i].r_a = k.r_a;
+        out[i].m = k.m;
+        out[i].s = k.s;
+        out[i].h = k.h;
+        out[i].c0 = k.c0;
+        out[i].c1 = k.c1;
+    }
+    *neighborhood_out = neighborhood;
+    return kernel_count;
 }
 
 /* Spectrum T[c] (complex, N entries). */
