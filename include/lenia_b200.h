@@ -233,6 +233,19 @@ lenia_status lenia_batch_sync(lenia_batch *b);
 int lenia_batch_launches_per_step(const lenia_batch *b);
 const char *lenia_batch_last_error(const lenia_batch *b);
 
+/* ---- Statistics for labelling runs --------------------------------------
+ *
+ * No counterpart in the reference.  Per channel of the grid A, in double
+ * precision with a fixed summation order (identical on every run):
+ *   0 mass sum a;  1-6 sum a cos(2 pi x / W), sum a sin(2 pi x / W), the same
+ *   for y (H) and z (W) - the torus-aware centroid and spread;  7 max a;
+ *   8 number of cells with a > fill_threshold. */
+#define LENIA_STATS 9
+/* out: channels x LENIA_STATS doubles (host memory).  Synchronises. */
+lenia_status lenia_world_stats(lenia_world *w, float fill_threshold, double *out);
+/* out: every world's channels x LENIA_STATS doubles, in world order (host). */
+lenia_status lenia_batch_stats(lenia_batch *b, float fill_threshold, double *out);
+
 /* ---- Marching cubes --------------------------------------------------
  *
  * Replaces generate_mesh_v1/v2/v3 (mesh.cpp:34-431, 434-1109, 1115-2037)

@@ -144,6 +144,8 @@ def load() -> ctypes.CDLL:
         "lenia_batch_set_stream": ([P, ctypes.c_void_p], ctypes.c_int),
         "lenia_batch_sync": ([P], ctypes.c_int),
         "lenia_batch_launches_per_step": ([P], ctypes.c_int),
+        "lenia_world_stats": ([P, ctypes.c_float, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+        "lenia_batch_stats": ([P, ctypes.c_float, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
         "lenia_batch_last_error": ([P], ctypes.c_char_p),
         "lenia_mesher_create": ([ctypes.POINTER(LeniaMeshDesc), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
         "lenia_mesher_destroy": ([P], ctypes.c_int),

@@ -103,5 +103,17 @@ class Batch:
     def sync(self) -> None:
         self._check(self._lib.lenia_batch_sync(self._h))
 
+    def stats(self, fill_threshold: float = 0.1) -> List[np.ndarray]:
+        """Grid statistics of every world (channels x 9 doubles each)."""
+        total = sum(d.channels for d in self.descs) * 9
+        out = np.zeros(total, dtype=np.float64)
+        self._check(self._lib.lenia_batch_stats(self._h, ctypes.c_float(fill_threshold),
+                                                out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        res, off = [], 0
+        for d in self.descs:
+            res.append(out[off:off + 9 * d.channels].reshape(d.channels, 9))
+            off += 9 * d.channels
+        return res
+
     def launches_per_step(self) -> int:
         return int(self._lib.lenia_batch_launches_per_step(self._h))

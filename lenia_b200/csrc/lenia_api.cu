@@ -121,6 +121,7 @@ struct lenia_world {
     LeniaKernelParams *kp_dev = nullptr;
     float2 *tw_x_fwd = nullptr, *tw_x_inv = nullptr, *tw_y_fwd = nullptr, *tw_y_inv = nullptr;
     int *err_flag = nullptr;
+    double *stats_trig = nullptr, *stats_partial = nullptr;  // lenia_world_stats buffers (allocated on first use)
     int lut_base_host[kMaxKernels];
     bool blur_valid = false;  // U_S / SUM_S hold a blur result
     // profiling
@@ -378,7 +379,8 @@ void free_world(lenia_world *w)
                    w->TT, w->U, w->Kc, w->blur_hat, w->lut_rows, w->ksum};
     for (float *p : fs)
         if (p) cudaFree(p);
-    void *vs[] = {w->lut_base, w->kp_dev, w->tw_x_fwd, w->tw_x_inv, w->tw_y_fwd, w->tw_y_inv, w->err_flag};
+    void *vs[] = {w->lut_base, w->kp_dev, w->tw_x_fwd, w->tw_x_inv, w->tw_y_fwd, w->tw_y_inv, w->err_flag,
+                  w->stats_trig, w->stats_partial};
     for (void *p : vs)
         if (p) cudaFree(p);
     if (!w->shared_scratch) {
@@ -386,6 +388,34 @@ void free_world(lenia_world *w)
         for (void *p : sc)
             if (p) cudaFree(p);
     }
+}
+
+// Grid statistics of the world's current A into dst (device, C x kStats
+// doubles), on the world's stream.
+lenia_status world_stats_async(lenia_world *w, float fill, double *dst)
+{
+    cudaError_t e = cudaSuccess;
+    if (!w->stats_trig) {
+        const int W = w->d.W, H = w->d.H;
+        std::vector<double> t(2 * (size_t)W + 2 * (size_t)H);
+        const double pi = 3.14159265358979323846;
+        for (int x = 0; x < W; x++) {
+            t[x] = cos(2.0 * pi * x / W);
+            t[W + x] = sin(2.0 * pi * x / W);
+        }
+        for (int y = 0; y < H; y++) {
+            t[2 * W + y] = cos(2.0 * pi * y / H);
+            t[2 * W + H + y] = sin(2.0 * pi * y / H);
+        }
+        w->stats_trig = dalloc<double>(t.size(), e);
+        w->stats_partial = dalloc<double>((size_t)w->C * kStatBlocks * kStats, e);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(w->stats_trig, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_fail(w, e, "statistics buffers");
+    }
+    e = launch_stats(w->A, w->d, w->C, w->stats_trig, fill, w->stats_partial, kStatBlocks, dst, w->stream);
+    if (e != cudaSuccess) return cuda_fail(w, e, "statistics");
+    return LENIA_OK;
 }
 
 // Per-step buffers a batch lane lends to its worlds (they run one after
@@ -989,6 +1019,24 @@ lenia_status lenia_mesh_world(lenia_world *w, int view, lenia_mesher *m, long lo
     return LENIA_OK;
 }
 
+lenia_status lenia_world_stats(lenia_world *w, float fill_threshold, double *out)
+{
+    if (!w || !out) return LENIA_ERR_INVALID_ARG;
+    double *dev = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&dev, sizeof(double) * w->C * kStats, w->stream);
+    if (e != cudaSuccess) return cuda_fail(w, e, "statistics");
+    lenia_status s = world_stats_async(w, fill_threshold, dev);
+    if (s == LENIA_OK) {
+        e = cudaMemcpyAsync(out, dev, sizeof(double) * w->C * kStats, cudaMemcpyDeviceToHost, w->stream);
+        if (e == cudaSuccess) e = cudaFreeAsync(dev, w->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+        if (e != cudaSuccess) s = cuda_fail(w, e, "statistics");
+    } else {
+        cudaFreeAsync(dev, w->stream);
+    }
+    return s;
+}
+
 const char *lenia_kernel_name(int kid) { return kid >= 0 && kid < KID_MAX ? kKernelNames[kid] : nullptr; }
 
 int lenia_launches_per_step(const lenia_world *w) { return w ? w->launches : 0; }
@@ -1268,6 +1316,31 @@ lenia_status lenia_batch_sync(lenia_batch *b)
         const lenia_status s = lenia_sync(b->worlds[i]);
         if (s != LENIA_OK) return bfail(b, s, "world %zu: %s", i, b->worlds[i]->err.c_str());
     }
+    return LENIA_OK;
+}
+
+lenia_status lenia_batch_stats(lenia_batch *b, float fill_threshold, double *out)
+{
+    if (!b || !out) return LENIA_ERR_INVALID_ARG;
+    size_t total = 0;
+    for (const lenia_world *w : b->worlds) total += (size_t)w->C * kStats;
+    double *dev = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&dev, sizeof(double) * total, b->stream);
+    if (e != cudaSuccess) return bfail(b, LENIA_ERR_CUDA, "statistics: %s", cudaGetErrorString(e));
+    size_t off = 0;
+    for (size_t i = 0; i < b->worlds.size(); i++) {
+        lenia_world *w = b->worlds[i];
+        const lenia_status s = world_stats_async(w, fill_threshold, dev + off);
+        if (s != LENIA_OK) {
+            cudaFreeAsync(dev, b->stream);
+            return bfail(b, s, "world %zu: %s", i, w->err.c_str());
+        }
+        off += (size_t)w->C * kStats;
+    }
+    e = cudaMemcpyAsync(out, dev, sizeof(double) * total, cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaFreeAsync(dev, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return bfail(b, LENIA_ERR_CUDA, "statistics: %s", cudaGetErrorString(e));
     return LENIA_OK;
 }
 

@@ -142,6 +142,13 @@ cudaError_t launch_growth_rows_fast(const Dims &d, const float2 *tw_x_inv, const
                                     float *U_dbg, int *err_flag, cudaStream_t st);
 cudaError_t launch_blur_rows_fast(const Dims &d, const float2 *tw_x_inv, const BlurJobs &jobs, cudaStream_t st);
 
+// Grid statistics for labelling (kernels_stats.cu): per channel kStats
+// doubles; trig holds cos, sin of 2 pi x / W (W each) then of 2 pi y / H.
+constexpr int kStats = 9;
+constexpr int kStatBlocks = 64;
+cudaError_t launch_stats(const float *A, const Dims &d, int C, const double *trig, float fill, double *partial,
+                         int nblk, double *out, cudaStream_t st);
+
 // Host FFT plans and twiddle tables (lenia_api.cu).
 int fft_factor(int n, int *radix);
 

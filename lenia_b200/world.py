@@ -144,6 +144,13 @@ class World:
                 out[name] = (float(ms[i]), int(cnt[i]))
         return out
 
+    def stats(self, fill_threshold: float = 0.1) -> np.ndarray:
+        """Grid statistics (channels x 9 doubles, see lenia_world_stats)."""
+        out = np.zeros((self.C, 9), dtype=np.float64)
+        self._check(self._lib.lenia_world_stats(self._h, ctypes.c_float(fill_threshold),
+                                                out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
     @property
     def launches_per_step(self) -> int:
         return int(self._lib.lenia_launches_per_step(self._h))
