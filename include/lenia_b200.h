@@ -199,6 +199,20 @@ const char *lenia_kernel_name(int kid);
 lenia_status lenia_convolve_noalloc(int width, int height, const float *field, const LeniaKernelParams *kernel,
                                     float *u_out, void *stream);
 
+/* ---- Checkpoints --------------------------------------------------------
+ *
+ * The save/load that config.cpp:75-262 sketches (commented out in the
+ * reference): the parameters, the kernels and every field that carries over
+ * between steps (A, V, GA, SUM), as a versioned little-endian binary with a
+ * CRC-32 trailer.  desc and kernels are the world's (the caller's copies);
+ * step is a counter stored alongside. */
+lenia_status lenia_save(lenia_world *w, const LeniaWorldDesc *desc, const LeniaKernelParams *kernels, int n_kernels,
+                        unsigned long long step, const char *path);
+/* Creates a world on the current device from a checkpoint; a wrong magic,
+ * checksum or field size gives LENIA_ERR_INVALID_ARG, another version
+ * LENIA_ERR_UNSUPPORTED.  step (optional) receives the stored counter. */
+lenia_status lenia_load(const char *path, lenia_world **out, unsigned long long *step);
+
 /* ---- Batches of worlds -------------------------------------------------
  *
  * Many independent worlds (any mix of sizes, channels, kernel sets and

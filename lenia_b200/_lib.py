@@ -131,6 +131,10 @@ def load() -> ctypes.CDLL:
         "lenia_kernel_name": ([ctypes.c_int], ctypes.c_char_p),
         "lenia_convolve_noalloc": ([ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(LeniaKernelParams),
                                     ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+        "lenia_save": ([P, ctypes.POINTER(LeniaWorldDesc), ctypes.POINTER(LeniaKernelParams), ctypes.c_int,
+                        ctypes.c_ulonglong, ctypes.c_char_p], ctypes.c_int),
+        "lenia_load": ([ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_ulonglong)],
+                       ctypes.c_int),
         "lenia_batch_create": ([ctypes.POINTER(LeniaWorldDesc), ctypes.POINTER(LeniaKernelParams),
                                 ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
                                 ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),

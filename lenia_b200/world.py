@@ -144,6 +144,31 @@ class World:
                 out[name] = (float(ms[i]), int(cnt[i]))
         return out
 
+    def save(self, path: str, step: int = 0) -> None:
+        """Checkpoint (lenia_save): parameters, kernels, A, V, GA, SUM."""
+        self._check(self._lib.lenia_save(self._h, ctypes.byref(self._cdesc), self._ckern, len(self.kernels),
+                                         ctypes.c_ulonglong(step), path.encode()))
+
+    @classmethod
+    def load(cls, path: str):
+        """(World, step) from a checkpoint written by save()."""
+        from .params import KernelParams, WorldDesc
+        lib = _lib.load()
+        h = ctypes.c_void_p()
+        step = ctypes.c_ulonglong()
+        st = lib.lenia_load(path.encode(), ctypes.byref(h), ctypes.byref(step))
+        if st != _lib.LENIA_OK:
+            raise _lib.LeniaError(st, f"lenia_load({path!r}) failed")
+        w = cls.__new__(cls)
+        w._lib = lib
+        w._h = h
+        hdr = read_checkpoint_header(path)
+        w.desc = hdr["desc"]
+        w.kernels = hdr["kernels"]
+        w._cdesc = _lib.to_c_desc(w.desc)
+        w._ckern = _lib.to_c_kernels(w.kernels)
+        return w, int(step.value)
+
     def stats(self, fill_threshold: float = 0.1) -> np.ndarray:
         """Grid statistics (channels x 9 doubles, see lenia_world_stats)."""
         out = np.zeros((self.C, 9), dtype=np.float64)
@@ -154,3 +179,38 @@ class World:
     @property
     def launches_per_step(self) -> int:
         return int(self._lib.lenia_launches_per_step(self._h))
+
+
+def read_checkpoint_header(path: str) -> dict:
+    """The parameters, kernels and step of a checkpoint file (the layout is
+    documented in lenia_b200/csrc/checkpoint.cu)."""
+    import struct
+    from .params import KernelParams, WorldDesc
+    data = open(path, "rb").read()
+    if data[:8] != b"LENIACKP":
+        raise ValueError(f"{path} is not a checkpoint")
+    version, _flags, nwords = struct.unpack_from("<III", data, 8)
+    off = 20
+    raw = data[off:off + 4 * nwords]
+    off += 4 * nwords
+    cdesc = _lib.LeniaWorldDesc.from_buffer_copy(raw)
+    d = {}
+    for name, ctype in _lib.LeniaWorldDesc._fields_:
+        v = getattr(cdesc, name)
+        d[name] = tuple(bool(x) for x in v) if name in ("asymptotic", "soft_clip") else v
+    desc = WorldDesc(**{k: (bool(v) if isinstance(getattr(WorldDesc(), k), bool) else v) for k, v in d.items()})
+    (nk,) = struct.unpack_from("<I", data, off)
+    off += 4
+    kernels = []
+    for _ in range(nk):
+        radius, beta = struct.unpack_from("<ii", data, off)
+        off += 8
+        b = list(struct.unpack_from("<12f", data, off))
+        off += 48
+        r_a, m, s, h = struct.unpack_from("<4f", data, off)
+        off += 16
+        c0, c1 = struct.unpack_from("<ii", data, off)
+        off += 8
+        kernels.append(KernelParams(radius=radius, beta_size=beta, b=b[:beta], r_a=r_a, m=m, s=s, h=h, c0=c0, c1=c1))
+    (step,) = struct.unpack_from("<Q", data, off)
+    return {"version": version, "desc": desc, "kernels": kernels, "step": step}
