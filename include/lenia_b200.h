@@ -260,6 +260,33 @@ lenia_status lenia_world_stats(lenia_world *w, float fill_threshold, double *out
 /* out: every world's channels x LENIA_STATS doubles, in world order (host). */
 lenia_status lenia_batch_stats(lenia_batch *b, float fill_threshold, double *out);
 
+/* ---- Proposal network ----------------------------------------------------
+ *
+ * No counterpart in the reference.  A multilayer perceptron n_in -> hidden ->
+ * hidden -> hidden -> 1 with GELU, trained and evaluated by this library's
+ * own kernels: weights and activations enter each matrix product rounded to
+ * bfloat16, products accumulate in float32, the loss is binary cross-entropy
+ * on the logit, and Adam updates float32 master weights.  Parameters are laid
+ * out layer by layer, W (out x in, row-major) then b. */
+typedef struct lenia_mlp lenia_mlp;
+lenia_status lenia_mlp_create(int n_in, int hidden, unsigned long long seed, lenia_mlp **out);
+lenia_status lenia_mlp_destroy(lenia_mlp *m);
+long long lenia_mlp_param_count(const lenia_mlp *m);
+lenia_status lenia_mlp_get_params(lenia_mlp *m, float *out, size_t n);
+lenia_status lenia_mlp_set_params(lenia_mlp *m, const float *src, size_t n);
+/* Gradients of the last lenia_mlp_gradients / lenia_mlp_train_step. */
+lenia_status lenia_mlp_get_grads(lenia_mlp *m, float *out, size_t n);
+/* x: B x n_in (device, row-major); logits: B floats (device); on `stream`. */
+lenia_status lenia_mlp_forward(lenia_mlp *m, const float *x, int B, float *logits, void *stream);
+/* Loss (mean binary cross-entropy, host) and gradients of a batch; y: B
+ * targets in {0, 1} (device).  Synchronises the stream. */
+lenia_status lenia_mlp_gradients(lenia_mlp *m, const float *x, const float *y, int B, float *loss_out, void *stream);
+/* lenia_mlp_gradients, then one Adam step (0.9, 0.999, 1e-8) with learning
+ * rate lr and decoupled weight decay wd. */
+lenia_status lenia_mlp_train_step(lenia_mlp *m, const float *x, const float *y, int B, float lr, float wd,
+                                  float *loss_out, void *stream);
+const char *lenia_mlp_last_error(const lenia_mlp *m);
+
 /* ---- Marching cubes --------------------------------------------------
  *
  * Replaces generate_mesh_v1/v2/v3 (mesh.cpp:34-431, 434-1109, 1115-2037)

@@ -135,6 +135,19 @@ def load() -> ctypes.CDLL:
                         ctypes.c_ulonglong, ctypes.c_char_p], ctypes.c_int),
         "lenia_load": ([ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_ulonglong)],
                        ctypes.c_int),
+        "lenia_mlp_create": ([ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_void_p)],
+                             ctypes.c_int),
+        "lenia_mlp_destroy": ([P], ctypes.c_int),
+        "lenia_mlp_param_count": ([P], ctypes.c_longlong),
+        "lenia_mlp_get_params": ([P, ctypes.c_void_p, ctypes.c_size_t], ctypes.c_int),
+        "lenia_mlp_set_params": ([P, ctypes.c_void_p, ctypes.c_size_t], ctypes.c_int),
+        "lenia_mlp_get_grads": ([P, ctypes.c_void_p, ctypes.c_size_t], ctypes.c_int),
+        "lenia_mlp_forward": ([P, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+        "lenia_mlp_gradients": ([P, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
+                                 ctypes.c_void_p], ctypes.c_int),
+        "lenia_mlp_train_step": ([P, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                  ctypes.POINTER(ctypes.c_float), ctypes.c_void_p], ctypes.c_int),
+        "lenia_mlp_last_error": ([P], ctypes.c_char_p),
         "lenia_batch_create": ([ctypes.POINTER(LeniaWorldDesc), ctypes.POINTER(LeniaKernelParams),
                                 ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
                                 ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
