@@ -13,10 +13,12 @@ axis; max; cells above a fill threshold) this module derives
     squares,
   - the centroid velocity between two observations (torus-wrapped),
 and labels a run at its final observation:
-  dead        total mass below 1 % of the initial mass, or max below 0.05;
+  dead        total mass below a quarter of the initial mass, or max below
+              0.05;
   exploding   non-finite statistics, more than half of the cells above the
-              fill threshold, or a spread above a quarter of the side;
+              fill threshold, or a spread above a fifth of the side;
   persistent  otherwise (alive and bounded).
+The thresholds are this project's choice (the reference defines no labels).
 """
 from __future__ import annotations
 
@@ -99,9 +101,9 @@ def label(s_final: Summary, initial_mass: float, width: int) -> str:
     vals = np.concatenate([s_final.mass, s_final.max, [s_final.total, s_final.fill]])
     if not np.all(np.isfinite(vals)):
         return "exploding"
-    if s_final.total < 0.01 * initial_mass or s_final.max.max() < 0.05:
+    if s_final.total < 0.25 * initial_mass or s_final.max.max() < 0.05:
         return "dead"
-    if s_final.fill > 0.5 or s_final.spread[-1] > 0.25 * width:
+    if s_final.fill > 0.5 or s_final.spread[-1] > 0.2 * width:
         return "exploding"
     return "persistent"
 

@@ -3,7 +3,8 @@ sampling.
 
 Candidates are kernel sets drawn as in config 0 (one kernel per channel pair,
 1-3 shells, b ~ U(0,1), m ~ U(0.1,0.5), s ~ U(0.01,0.18), h ~ U(0.01,1)) on
-cubic worlds with 3 channels and a seeded cube.  A run is a *hit* when its
+cubic worlds with 3 channels and a seeded cube, run as mass-conserving Flow
+Lenia (see `candidates`).  A run is a *hit* when its
 label at the final step is "persistent" (alive and bounded, lenia_b200.labels).
 
   uniform  every candidate runs to the final step;
@@ -31,14 +32,21 @@ N_KERNELS = 9
 KERNEL_FEATURES = 7  # b0, b1, b2, m, s, h, r_a
 
 
-def candidates(n: int, seed: int, width: int = 32) -> List[P.Workload]:
+def candidates(n: int, seed: int, width: int = 32, asymptotic: bool = False,
+               growth_type: int = P.GROWTH_NOGROWTH, sigma: float = 0.5) -> List[P.Workload]:
+    """n candidate worlds, mass-conserving Flow Lenia by default: sigma 0.5
+    (the reference's reintegration spreads (2 sigma)^3 / (4 sigma^2) of a
+    cell's mass per step with S_NORM 0, exactly 1 only at sigma 0.5; at the
+    benchmark's 0.65 every world fills the grid) and no growth (with the
+    reference's growth, h bell >= 0, every random kernel set fills the grid;
+    asymptotic channels fill most of it)."""
     out = []
     for i in range(n):
         rng = np.random.default_rng((seed, i))
-        desc = P.WorldDesc(width=width, height=width, channels=3, timestep=0.2, theta_a=2.0, sigma=0.65, dd=1.0,
-                           growth_type=P.GROWTH_RT, mode_type=P.MODE_RT, sobel_border=P.BORDER_TORUS,
+        desc = P.WorldDesc(width=width, height=width, channels=3, timestep=0.2, theta_a=2.0, sigma=sigma, dd=1.0,
+                           growth_type=growth_type, mode_type=P.MODE_RT, sobel_border=P.BORDER_TORUS,
                            border=P.BORDER_TORUS, gradient_mode=P.GRADIENT_CENTRAL_DIFF, blur_central_diff=False,
-                           mu_vel=False, asymptotic=(False,) * 4, soft_clip=(False,) * 4)
+                           mu_vel=False, asymptotic=(asymptotic,) * 4, soft_clip=(False,) * 4)
         ks = P.sample_kernels(rng, 3, radius=max(2, width // 4))
         out.append(P.Workload(desc, ks, P.seed_cube(rng, desc, width // 2)))
     return out
