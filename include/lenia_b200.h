@@ -187,6 +187,22 @@ int lenia_profile_read(lenia_world *w, double *ms, long long *launches, int n);
 /* Name of kernel id `kid` of lenia_profile_read (NULL past the last). */
 const char *lenia_kernel_name(int kid);
 
+/* ------------------------------------------------------- convolution modes
+ * How the growth stage computes u_k = K_k (*) A_c0 (the reference: FFTW,
+ * lenia.cpp:435-491).  LENIA_CONV_FFT is the half-spectrum FP32 FFT path.
+ * The direct modes run the same periodic convolution in the spatial domain on
+ * the tcgen05 tensor cores with FP32 accumulation: DIRECT_BF16 rounds grid
+ * and kernel taps to BF16; DIRECT_BF16X3 splits each into hi + lo BF16 parts
+ * and sums hi*hi + hi*lo + lo*hi.  Direct modes need every kernel's
+ * radius * r_a <= 64 and keep u_k of every kernel in HBM (K x N floats). */
+enum { LENIA_CONV_FFT = 0, LENIA_CONV_DIRECT_BF16 = 1, LENIA_CONV_DIRECT_BF16X3 = 2 };
+/* Selects the convolution mode (rebuilds the kernel tables; synchronous). */
+lenia_status lenia_set_conv_mode(lenia_world *w, int mode);
+int lenia_get_conv_mode(lenia_world *w);
+/* Tensor multiply-adds one direct convolution issues and the useful ones
+ * (nonzero taps x cells x products per tap); both 0 in FFT mode. */
+lenia_status lenia_conv_macs(lenia_world *w, double *issued, double *useful);
+
 /* No counterpart in the reference.  u_out = Re(IFFT(FFT(field) * K^))/N for
  * one field and one kernel, computed exactly as a world's growth stage computes
  * u for that kernel, for callers that cannot allocate device memory: every

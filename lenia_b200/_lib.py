@@ -27,6 +27,7 @@ FIELD = {
     "U": 16, "H_RB": 17, "U_SUM_RB": 18, "RBB": 19,
 }
 STAGE = {"GROWTH": 0, "BLUR": 1, "FLOW": 2, "TRANSPORT": 3, "SNAPSHOT": 4}
+CONV = {"FFT": 0, "DIRECT_BF16": 1, "DIRECT_BF16X3": 2}
 
 
 class LeniaWorldDesc(ctypes.Structure):
@@ -123,6 +124,9 @@ def load() -> ctypes.CDLL:
         "lenia_set_stream": ([P, ctypes.c_void_p], ctypes.c_int),
         "lenia_sync": ([P], ctypes.c_int),
         "lenia_set_debug": ([P, ctypes.c_int], ctypes.c_int),
+        "lenia_set_conv_mode": ([P, ctypes.c_int], ctypes.c_int),
+        "lenia_get_conv_mode": ([P], ctypes.c_int),
+        "lenia_conv_macs": ([P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
         "lenia_set_snapshots": ([P, ctypes.c_int], ctypes.c_int),
         "lenia_launches_per_step": ([P], ctypes.c_int),
         "lenia_set_profiling": ([P, ctypes.c_int], ctypes.c_int),

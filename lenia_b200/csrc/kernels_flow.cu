@@ -355,8 +355,8 @@ namespace {
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 }
 
-cudaError_t encode_tensor_map(CUtensorMap *map, const float *base, int rank, const unsigned long long *dims,
-                              const unsigned *box)
+cudaError_t encode_tensor_map_typed(CUtensorMap *map, const void *base, int dtype, int elem_bytes, int rank,
+                                    const unsigned long long *dims, const unsigned *box)
 {
     if (!g_encode) {
         void *fn = nullptr;
@@ -367,7 +367,7 @@ cudaError_t encode_tensor_map(CUtensorMap *map, const float *base, int rank, con
     }
     cuuint64_t gdim[5], gstride[4];
     cuuint32_t bdim[5], estride[5];
-    unsigned long long stride = sizeof(float);
+    unsigned long long stride = (unsigned long long)elem_bytes;
     for (int i = 0; i < rank; i++) {
         gdim[i] = dims[i];
         bdim[i] = box[i];
@@ -375,10 +375,16 @@ cudaError_t encode_tensor_map(CUtensorMap *map, const float *base, int rank, con
         if (i > 0) gstride[i - 1] = stride;
         stride *= dims[i];
     }
-    const CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, (void *)base, gdim, gstride,
-                                bdim, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+    const CUresult r = g_encode(map, (CUtensorMapDataType)dtype, (cuuint32_t)rank, (void *)base, gdim, gstride, bdim,
+                                estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+cudaError_t encode_tensor_map(CUtensorMap *map, const float *base, int rank, const unsigned long long *dims,
+                              const unsigned *box)
+{
+    return encode_tensor_map_typed(map, base, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (int)sizeof(float), rank, dims, box);
 }
 
 cudaError_t launch_flow(const StepParams &p, const FlowBuffers &b, cudaStream_t st)

@@ -19,6 +19,7 @@
 #include <utility>
 #include <vector>
 
+#include "direct_conv.h"
 #include "lenia_internal.h"
 
 using namespace lenia;
@@ -81,12 +82,16 @@ enum KernelId {
     KID_BLUR_ROWS,
     KID_FLOW,
     KID_TRANSPORT,
+    KID_DIRECT_PAD,
+    KID_DIRECT_CONV,
+    KID_GROWTH_U,
     KID_MAX
 };
 const char *const kKernelNames[KID_MAX] = {"fwd_rows",          "planes_fwd",          "planes_inv",
                                            "growth_rows",       "blur_fwd_rows",       "blur_planes_fwd",
                                            "blur_planes_inv",   "blur_rows",           "flow",
-                                           "transport"};
+                                           "transport",         "direct_pad",          "direct_conv",
+                                           "growth_u"};
 
 struct ProfRec {
     int kid;
@@ -124,6 +129,8 @@ struct lenia_world {
     double *stats_trig = nullptr, *stats_partial = nullptr;  // lenia_world_stats buffers (allocated on first use)
     int lut_base_host[kMaxKernels];
     bool blur_valid = false;  // U_S / SUM_S hold a blur result
+    int conv_mode = LENIA_CONV_FFT;
+    DirectConv *dconv = nullptr;  // plan of the direct convolution modes
     // profiling
     bool profile = false;
     std::vector<ProfRec> prof_pending;
@@ -314,6 +321,16 @@ lenia_status build_kernels(lenia_world *w)
     e = cudaMallocAsync((void **)&grids, ng * sizeof(float), st);
     if (e != cudaSuccess) return cuda_fail(w, e, "kernel grid scratch");
     if ((e = launch_kernel_grids(d, w->kp_dev, K, grids, w->ksum, st)) != cudaSuccess) goto out;
+    if (w->dconv) {
+        direct_destroy(w->dconv);
+        w->dconv = nullptr;
+    }
+    if (w->conv_mode != LENIA_CONV_FFT) {
+        if (!w->U && K > 0) w->U = dalloc<float>((size_t)K * d.N, e);
+        if (e != cudaSuccess) goto out;
+        if ((e = direct_create(d, w->C, w->kernels.data(), K, w->conv_mode, &w->dconv)) != cudaSuccess) goto out;
+        if ((e = direct_build(w->dconv, grids, st)) != cudaSuccess) goto out;
+    }
     for (int k0 = 0; k0 < K; k0 += 2 * kMaxPairs) {
         FwdRowJobs fj;
         memset(&fj, 0, sizeof(fj));
@@ -383,6 +400,8 @@ void free_world(lenia_world *w)
                   w->stats_trig, w->stats_partial};
     for (void *p : vs)
         if (p) cudaFree(p);
+    direct_destroy(w->dconv);
+    w->dconv = nullptr;
     if (!w->shared_scratch) {
         void *sc[] = {w->H, w->U_SUM, w->BACK, w->MU, w->F, w->ALPHA, w->U_S, w->SUM_S, w->XS, w->S};
         for (void *p : sc)
@@ -436,6 +455,46 @@ lenia_status stage_growth(lenia_world *w)
         std::swap(w->H, w->H_RB);
         std::swap(w->U_SUM, w->U_SUM_RB);
     }
+    GrowthJobs gj;
+    memset(&gj, 0, sizeof(gj));
+    gj.K = w->K;
+    gj.C = w->C;
+    for (int k = 0; k < w->K; k++) {
+        gj.spec[k] = w->S + (size_t)k * d.HS;
+        gj.c1[k] = w->kernels[k].c1;
+        gj.h[k] = w->kernels[k].h;
+        gj.lut_base[k] = w->lut_base_host[k];
+    }
+    for (int c = 0; c < kMaxChannels; c++) {
+        gj.asymptotic[c] = w->desc.asymptotic[c];
+        gj.soft_clip[c] = w->desc.soft_clip[c];
+    }
+    gj.growth_rt = w->desc.growth_type == LENIA_GROWTH_RT;
+    gj.timestep = w->desc.timestep;
+    if (w->conv_mode != LENIA_CONV_FFT) {
+        // direct convolution on the tensor cores, then the growth from u_k
+        if (!w->dconv && w->K > 0) return fail(w, LENIA_ERR_INVALID_ARG, "direct convolution has no plan");
+        if (w->dconv) {
+            {
+                ProfScope ps(w, KID_DIRECT_PAD);
+                if ((e = direct_pad(w->dconv, w->A, st)) != cudaSuccess) return cuda_fail(w, e, "direct_pad");
+            }
+            {
+                ProfScope ps(w, KID_DIRECT_CONV);
+                if ((e = direct_convolve(w->dconv, w->U, w->err_flag, st)) != cudaSuccess)
+                    return cuda_fail(w, e, "direct_conv");
+            }
+            w->launches += 2;
+        }
+        {
+            ProfScope ps(w, KID_GROWTH_U);
+            if ((e = launch_growth_from_u(d, gj, w->lut_rows, w->U, w->A, w->H, w->U_SUM, w->BACK, w->err_flag, st)) !=
+                cudaSuccess)
+                return cuda_fail(w, e, "growth_u");
+        }
+        w->launches++;
+        return LENIA_OK;
+    }
     // forward transforms of the grid channels, packed in pairs
     FwdRowJobs fj;
     memset(&fj, 0, sizeof(fj));
@@ -478,22 +537,6 @@ lenia_status stage_growth(lenia_world *w)
             return cuda_fail(w, e, "planes (inverse)");
         w->launches++;
     }
-    GrowthJobs gj;
-    memset(&gj, 0, sizeof(gj));
-    gj.K = w->K;
-    gj.C = w->C;
-    for (int k = 0; k < w->K; k++) {
-        gj.spec[k] = w->S + (size_t)k * d.HS;
-        gj.c1[k] = w->kernels[k].c1;
-        gj.h[k] = w->kernels[k].h;
-        gj.lut_base[k] = w->lut_base_host[k];
-    }
-    for (int c = 0; c < kMaxChannels; c++) {
-        gj.asymptotic[c] = w->desc.asymptotic[c];
-        gj.soft_clip[c] = w->desc.soft_clip[c];
-    }
-    gj.growth_rt = w->desc.growth_type == LENIA_GROWTH_RT;
-    gj.timestep = w->desc.timestep;
     {
         ProfScope ps(w, KID_GROWTH_ROWS);
         if ((e = launch_growth_rows(d, w->px, w->tw_x_inv, gj, w->lut_rows, w->A, w->H, w->U_SUM, w->BACK,
@@ -960,6 +1003,41 @@ lenia_status lenia_set_debug(lenia_world *w, int on)
     if (!w) return LENIA_ERR_INVALID_ARG;
     w->debug = on != 0;
     return ensure_optional(w);
+}
+
+lenia_status lenia_set_conv_mode(lenia_world *w, int mode)
+{
+    if (!w) return LENIA_ERR_INVALID_ARG;
+    if (mode < LENIA_CONV_FFT || mode > LENIA_CONV_DIRECT_BF16X3)
+        return fail(w, LENIA_ERR_INVALID_ARG, "unknown convolution mode %d", mode);
+    if (mode != LENIA_CONV_FFT)
+        for (const LeniaKernelParams &k : w->kernels)
+            if ((float)k.radius * k.r_a > 64.0f)
+                return fail(w, LENIA_ERR_UNSUPPORTED, "direct convolution needs radius * r_a <= 64");
+    cudaError_t e = cudaStreamSynchronize(w->stream);
+    if (e != cudaSuccess) return cuda_fail(w, e, "set_conv_mode");
+    const int old = w->conv_mode;
+    w->conv_mode = mode;
+    lenia_status s = build_kernels(w);
+    if (s != LENIA_OK && old != mode) {
+        const std::string why = w->err;
+        w->conv_mode = old;
+        build_kernels(w);
+        w->err = why;
+    }
+    return s;
+}
+
+int lenia_get_conv_mode(lenia_world *w) { return w ? w->conv_mode : -1; }
+
+lenia_status lenia_conv_macs(lenia_world *w, double *issued, double *useful)
+{
+    if (!w) return LENIA_ERR_INVALID_ARG;
+    double a = 0.0, b = 0.0;
+    if (w->dconv) direct_counts(w->dconv, &a, &b);
+    if (issued) *issued = a;
+    if (useful) *useful = b;
+    return LENIA_OK;
 }
 
 lenia_status lenia_set_snapshots(lenia_world *w, int on)

@@ -78,4 +78,9 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
 cudaError_t encode_tensor_map(CUtensorMap *map, const float *base, int rank, const unsigned long long *dims,
                               const unsigned *box);
 
+// Host: the same for elements of driver type `dtype` (a CUtensorMapDataType)
+// and `elem_bytes` bytes each.
+cudaError_t encode_tensor_map_typed(CUtensorMap *map, const void *base, int dtype, int elem_bytes, int rank,
+                                    const unsigned long long *dims, const unsigned *box);
+
 }  // namespace lenia

@@ -115,6 +115,22 @@ class World:
     def set_snapshots(self, on: bool = True) -> None:
         self._check(self._lib.lenia_set_snapshots(self._h, int(on)))
 
+    def set_conv_mode(self, mode: str) -> None:
+        """'FFT' (FP32 spectral path), 'DIRECT_BF16' or 'DIRECT_BF16X3'
+        (spatial convolution on the tensor cores, FP32 accumulation)."""
+        self._check(self._lib.lenia_set_conv_mode(self._h, _lib.CONV[mode]))
+
+    @property
+    def conv_mode(self) -> str:
+        m = int(self._lib.lenia_get_conv_mode(self._h))
+        return {v: k for k, v in _lib.CONV.items()}[m]
+
+    def conv_macs(self) -> tuple:
+        """(issued, useful) tensor multiply-adds of one direct convolution."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self._lib.lenia_conv_macs(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def set_stream(self, stream_ptr: int) -> None:
         self._check(self._lib.lenia_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
 
