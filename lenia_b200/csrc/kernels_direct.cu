@@ -720,7 +720,9 @@ cudaError_t direct_create(const Dims &d, int C, const LeniaKernelParams *kernels
             cudaSuccess)
             goto fail;
     }
-    if ((e = cudaFuncSetAttribute(k_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dc->smem)) !=
+    // the attribute is per function and shared by every plan: the limit
+    // itself, so that plans of other worlds launch with their own sizes
+    if ((e = cudaFuncSetAttribute(k_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimit)) !=
         cudaSuccess)
         goto fail;
     *out = dc;

@@ -99,6 +99,69 @@ __global__ void __launch_bounds__(kPlaneThreads) k_planes(Dims d, FftPlan py, Ff
     for (int e = threadIdx.x; e < D * H; e += blockDim.x) dst[e] = buf[e];
 }
 
+// Planes larger than shared memory: the same two line transforms as
+// k_planes, each as its own pass through global memory.  Pass y transforms
+// TZ consecutive z-lines of one kx plane (after the optional kernel product);
+// pass z transforms TY consecutive y-columns.  Every line goes through the
+// same 1-D transform as in k_planes, so results are identical.
+__global__ void __launch_bounds__(kPlaneThreads) k_plane_lines_y(Dims d, FftPlan py, const float2 *__restrict__ tw_y,
+                                                                 PlaneJobs jobs, int sign, int TZ)
+{
+    extern __shared__ float2 smem[];
+    const int H = d.H, D = d.D;
+    float2 *twy = smem;
+    float2 *buf = smem + H;
+    const int kx = blockIdx.x;
+    const int z0 = blockIdx.y * TZ;
+    const int job = blockIdx.z;
+    const long long base = ((long long)kx * D + z0) * H;
+    const float2 *src = jobs.src[job] + base;
+    float2 *dst = jobs.dst[job] + base;
+    const float *kc = jobs.kc[job];
+    for (int i = threadIdx.x; i < H; i += blockDim.x) twy[i] = tw_y[i];
+    const int KZ = D / 2 + 1, KY = H / 2 + 1;
+    if (kc) {
+        const float *kp = kc + (long long)kx * KZ * KY;
+        for (int e = threadIdx.x; e < TZ * H; e += blockDim.x) {
+            const int z = z0 + e / H, y = e % H;
+            const int oz = z <= D - z ? z : D - z;
+            const int oy = y <= H - y ? y : H - y;
+            const float k = kp[oz * KY + oy];
+            const float2 t = src[e];
+            buf[e] = make_float2(t.x * k, t.y * k);
+        }
+    } else {
+        for (int e = threadIdx.x; e < TZ * H; e += blockDim.x) buf[e] = src[e];
+    }
+    __syncthreads();
+    fft_lines<kPlaneCap>(buf, py, TZ, 1, H, twy, sign, false);
+    for (int e = threadIdx.x; e < TZ * H; e += blockDim.x) dst[e] = buf[e];
+}
+
+__global__ void __launch_bounds__(kPlaneThreads) k_plane_lines_z(Dims d, FftPlan pz, const float2 *__restrict__ tw_z,
+                                                                 PlaneJobs jobs, int sign, int TY)
+{
+    extern __shared__ float2 smem[];
+    const int H = d.H, D = d.D;
+    float2 *twz = smem;
+    float2 *buf = smem + D;
+    const int kx = blockIdx.x;
+    const int y0 = blockIdx.y * TY;
+    const int job = blockIdx.z;
+    float2 *dst = jobs.dst[job] + (long long)kx * D * H + y0;
+    for (int i = threadIdx.x; i < D; i += blockDim.x) twz[i] = tw_z[i];
+    for (int e = threadIdx.x; e < D * TY; e += blockDim.x) {
+        const int z = e / TY, t = e % TY;
+        buf[e] = dst[(long long)z * H + t];
+    }
+    __syncthreads();
+    fft_lines<kPlaneCap>(buf, pz, TY, TY, 1, twz, sign, true);
+    for (int e = threadIdx.x; e < D * TY; e += blockDim.x) {
+        const int z = e / TY, t = e % TY;
+        dst[(long long)z * H + t] = buf[e];
+    }
+}
+
 // ------------------------------------------------- inverse rows: growth
 
 // Builds the packed row spectrum of kernels (s0, s1) for one row tile.
@@ -360,6 +423,26 @@ int row_tile(const Dims &d, const FftPlan &px)
     return 0;
 }
 
+constexpr long long kPlaneSmem = 200 * 1024;
+
+// Lines per block of the split plane passes (0: none fits).
+static int split_tile(int n_lines, int n, const FftPlan &p, int other)
+{
+    for (int t = 64; t >= 1; t /= 2)
+        if (n_lines % t == 0 && fits(p, t, kPlaneThreads, kPlaneCap) &&
+            (long long)t * n * 8 + (long long)other * 8 <= kPlaneSmem)
+            return t;
+    return 0;
+}
+
+bool plane_fits(const Dims &d, const FftPlan &py, const FftPlan &pz);
+
+// Whether the plane transforms run, in one pass or in two.
+bool planes_supported(const Dims &d, const FftPlan &py, const FftPlan &pz)
+{
+    return plane_fits(d, py, pz) || (split_tile(d.D, d.H, py, d.H) > 0 && split_tile(d.H, d.D, pz, d.D) > 0);
+}
+
 bool plane_fits(const Dims &d, const FftPlan &py, const FftPlan &pz)
 {
     return (long long)d.D * d.H * 8 + (d.H + d.D) * 8 <= 200 * 1024 && fits(py, d.D, kPlaneThreads, kPlaneCap) &&
@@ -390,7 +473,17 @@ cudaError_t launch_planes(const Dims &d, const FftPlan &py, const FftPlan &pz, c
                           const float2 *tw_z, const PlaneJobs &jobs, int sign, cudaStream_t st)
 {
     if (fast_supported(d)) return launch_planes_fast(d, tw_y, tw_z, jobs, sign, st);
-    if (!plane_fits(d, py, pz)) return cudaErrorInvalidValue;
+    if (!plane_fits(d, py, pz)) {
+        const int TZ = split_tile(d.D, d.H, py, d.H), TY = split_tile(d.H, d.D, pz, d.D);
+        if (TZ == 0 || TY == 0) return cudaErrorInvalidValue;
+        const size_t sy = ((size_t)TZ * d.H + d.H) * sizeof(float2), sz = ((size_t)d.D * TY + d.D) * sizeof(float2);
+        cudaError_t e = set_smem((const void *)k_plane_lines_y, sy);
+        if (e == cudaSuccess) e = set_smem((const void *)k_plane_lines_z, sz);
+        if (e != cudaSuccess) return e;
+        k_plane_lines_y<<<dim3(d.KX, d.D / TZ, jobs.njobs), kPlaneThreads, sy, st>>>(d, py, tw_y, jobs, sign, TZ);
+        k_plane_lines_z<<<dim3(d.KX, d.H / TY, jobs.njobs), kPlaneThreads, sz, st>>>(d, pz, tw_z, jobs, sign, TY);
+        return cudaGetLastError();
+    }
     const size_t smem = (size_t)(d.H + d.D + (long long)d.D * d.H) * sizeof(float2);
     cudaError_t e = set_smem((const void *)k_planes, smem);
     if (e != cudaSuccess) return e;

@@ -27,6 +27,7 @@ using namespace lenia;
 namespace lenia {
 int row_tile(const Dims &d, const FftPlan &px);
 bool plane_fits(const Dims &d, const FftPlan &py, const FftPlan &pz);
+bool planes_supported(const Dims &d, const FftPlan &py, const FftPlan &pz);
 
 int fft_factor(int n, int *radix)
 {
@@ -752,7 +753,7 @@ lenia_status create_world(const LeniaWorldDesc *desc, const LeniaKernelParams *k
     w->px.nstages = fft_factor(d.W, w->px.radix);
     w->py.n = d.H;
     w->py.nstages = fft_factor(d.H, w->py.radix);
-    if (row_tile(d, w->px) == 0 || !plane_fits(d, w->py, w->px)) {
+    if (row_tile(d, w->px) == 0 || !planes_supported(d, w->py, w->px)) {
         delete w;
         return LENIA_ERR_UNSUPPORTED;
     }

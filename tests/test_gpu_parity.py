@@ -109,6 +109,18 @@ def test_stages_bit_exact_non_cubic(cuda_lib, oracle_built, shape):
     assert not problems, "\n".join(problems[:12])
 
 
+def test_stages_bit_exact_split_planes(cuda_lib, oracle_built):
+    """A kx plane of 100 x 256 complex values (200 KB) does not fit the
+    one-pass plane transform: the y and z line transforms run as separate
+    passes and stay bit-exact."""
+    wl = variant("sobel_torus", seed=356, width=100)
+    wl.desc.height = 256
+    rng = np.random.default_rng(356)
+    wl.A0 = P.seed_cube(rng, wl.desc, 32)
+    problems = run_staged(wl, steps=1)
+    assert not problems, "\n".join(problems[:12])
+
+
 def test_trajectory_bit_exact_cfg0(cuda_lib, oracle_built):
     """Whole steps (the production path, no debug outputs) stay bit-exact over
     100 steps of the 32^3 plain-step configuration."""
