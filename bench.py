@@ -14,6 +14,11 @@ With N > 1 (torchrun, one process per GPU) every rank advances its own world
 sum over ranks divided by the slowest rank's time.  `--impl reference` times
 the CPU restatement of the reference's step (oracle, complex-to-complex
 spectral structure like the reference's FFTW path) on the host cores.
+
+Beside the headline (N = 1 only): `batched` (config 3 mix as one batch) and
+`conv_modes`: the growth stage of the 256^3, radius-20 precision workload in
+each convolution mode (FP32 FFT, direct BF16 and BF16x3 on the tensor cores,
+with the direct kernel's tensor roofline) and the autotuner's choice.
 """
 from __future__ import annotations
 
@@ -45,6 +50,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-worlds", type=int, default=512,
                     help="worlds of the batched measurement (config 3 mix; 0 = skip)")
+    ap.add_argument("--conv-width", type=int, default=256,
+                    help="side of the convolution-mode measurement (config 2 workload; 0 = skip)")
     return ap.parse_args()
 
 
@@ -183,6 +190,58 @@ def ncu_traffic(kernel: str):
     except OSError:
         pass
     return None
+
+
+def measured_tensor_peak():
+    """Dense BF16 tensor peak in TFLOP/s: the sustained figure (the direct
+    convolution runs for tens of milliseconds per launch)."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        j = json.load(open(p))
+        return float(j["bf16_tflops_sustained"]), "measured sustained"
+    except Exception:
+        return 1400.0, "fallback sustained"
+
+
+def conv_measure(args):
+    """The growth stage (convolution and growth table) of the precision
+    workload (width^3, 3 channels, 9 kernels of radius 20) in every
+    convolution mode, per-kernel device times from the library's profiler;
+    the direct modes against the tensor-core peak (issued and useful
+    multiply-adds); and the autotuner's choice for that world."""
+    from lenia_b200.world import World
+    wl = P.config2(width=args.conv_width, radius=20)
+    peak, peak_kind = measured_tensor_peak()
+    out = {"workload": f"{args.conv_width}^3 x 3 channels, 9 kernels R=20, growth stage (config 2)", "modes": {}}
+    reps = 3
+    for mode in ("FFT", "DIRECT_BF16", "DIRECT_BF16X3"):
+        w = World(wl.desc, wl.kernels)
+        w.set_conv_mode(mode)
+        w.set_state(wl.A0.ravel())
+        w.stage("GROWTH")
+        w.sync()
+        w.set_profiling(True)
+        for _ in range(reps):
+            w.stage("GROWTH")
+        w.sync()
+        prof = w.profile_read()
+        r = {"growth_stage_ms": sum(v[0] for v in prof.values()) / reps,
+             "kernels_ms": {k: v[0] / v[1] for k, v in prof.items()}}
+        if mode != "FFT":
+            issued, useful = w.conv_macs()
+            conv_s = prof["direct_conv"][0] / prof["direct_conv"][1] / 1000.0
+            r["tensor_roofline"] = {"bound": "tensor", "kernel": "direct_conv", "unit": "TFLOP/s",
+                                    "achieved": 2 * issued / conv_s / 1e12, "peak": peak, "peak_kind": peak_kind,
+                                    "frac": 2 * issued / conv_s / 1e12 / peak,
+                                    "useful_tflops": 2 * useful / conv_s / 1e12,
+                                    "issued_over_useful": issued / useful}
+        out["modes"][mode] = r
+        w.close()
+    w = World(wl.desc, wl.kernels)
+    w.set_state(wl.A0.ravel())
+    out["autotune"] = w.autotune()
+    w.close()
+    return out
 
 
 def measured_peaks():
@@ -415,6 +474,7 @@ def run_ours(args):
     mesher.close()
 
     batched = batch_measure(args, rank, n, stream, barrier, max_over_ranks) if args.batch_worlds > 0 else None
+    conv = conv_measure(args) if (args.conv_width > 0 and n == 1) else None
 
     line = None
     if rank == 0:
@@ -439,6 +499,8 @@ def run_ours(args):
         }
         if batched is not None:
             line["batched"] = batched
+        if conv is not None:
+            line["conv_modes"] = conv
         if n == 1 and not args.no_cpu_baseline:
             rate, dt = cpu_port_rate(wl, 2, 1)
             line["cpu_baseline"] = {

@@ -121,7 +121,7 @@ typedef enum LeniaField {
     LENIA_FIELD_TT = 13,       /* C*N (debug: TT before the transposition epilogue) */
     LENIA_FIELD_U_S = 14,      /* C*N (central difference) */
     LENIA_FIELD_SUM_S = 15,    /* N (central difference) */
-    LENIA_FIELD_U = 16,        /* K*N: u_k = Re(IFFT)/N per kernel (debug) */
+    LENIA_FIELD_U = 16,        /* K*N: u_k per kernel (debug, or a direct convolution mode) */
     LENIA_FIELD_H_RB = 17,     /* C*N: H of the previous step */
     LENIA_FIELD_U_SUM_RB = 18, /* C*N: U_SUM of the previous step */
     LENIA_FIELD_RBB = 19       /* C*N: grid snapshot for meshing */
@@ -157,7 +157,10 @@ lenia_status lenia_set_kernels(lenia_world *w, const LeniaKernelParams *kernels,
 
 /* Copies `count` floats into / out of a field.  `on_device` = 1 means the
  * pointer is device memory; 0 means host memory (pageable or pinned).
- * Field sizes are listed at LeniaField; count must match. */
+ * Field sizes are listed at LeniaField; count must match.  Device copies are
+ * queued on the world's stream and return at once: order other streams'
+ * use of the pointer after them (lenia_sync, or events).  Host copies
+ * return when done. */
 lenia_status lenia_set_field(lenia_world *w, int field, const float *src, size_t count, int on_device);
 lenia_status lenia_get_field(lenia_world *w, int field, float *dst, size_t count, int on_device);
 /* Number of floats of a field (0 if the field does not exist). */
@@ -202,6 +205,19 @@ int lenia_get_conv_mode(lenia_world *w);
 /* Tensor multiply-adds one direct convolution issues and the useful ones
  * (nonzero taps x cells x products per tap); both 0 in FFT mode. */
 lenia_status lenia_conv_macs(lenia_world *w, double *issued, double *useful);
+
+/* No counterpart in the reference.  Measures the growth stage on this world's
+ * stream for every convolution mode whose bit is set in `modes` (bit i = mode
+ * i; LENIA_CONV_FFT and LENIA_CONV_DIRECT_BF16X3 give FP32-level results,
+ * DIRECT_BF16 does not), and for the FFT path every row tile its
+ * runtime-sized kernels take (grids without size-specialised kernels), then
+ * keeps the fastest.  The grid state is left as it was.  Synchronous. */
+typedef struct LeniaTuneResult {
+    int conv_mode;  /* the mode kept */
+    int row_tile;   /* rows per block of the FFT row transforms (0: built-in choice) */
+    float ms[3];    /* growth-stage milliseconds per mode, best tile; -1: not measured */
+} LeniaTuneResult;
+lenia_status lenia_autotune(lenia_world *w, int modes, LeniaTuneResult *out);
 
 /* No counterpart in the reference.  u_out = Re(IFFT(FFT(field) * K^))/N for
  * one field and one kernel, computed exactly as a world's growth stage computes
@@ -259,6 +275,11 @@ lenia_status lenia_batch_step(lenia_batch *b, int n_steps);
 lenia_status lenia_batch_set_stream(lenia_batch *b, void *stream);
 /* Waits for the batch and reports the first world's device-side error. */
 lenia_status lenia_batch_sync(lenia_batch *b);
+/* No counterpart in the reference.  lenia_autotune (above) on the
+ * first world of every grid shape in the batch, its choice (convolution mode,
+ * row tile) applied to every world of that shape, then the batch's step graphs
+ * captured again.  per_world: n_worlds results, or NULL.  Synchronous. */
+lenia_status lenia_batch_autotune(lenia_batch *b, int modes, LeniaTuneResult *per_world);
 /* Kernel launches one batch step contains (all worlds). */
 int lenia_batch_launches_per_step(const lenia_batch *b);
 const char *lenia_batch_last_error(const lenia_batch *b);

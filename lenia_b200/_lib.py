@@ -30,6 +30,10 @@ STAGE = {"GROWTH": 0, "BLUR": 1, "FLOW": 2, "TRANSPORT": 3, "SNAPSHOT": 4}
 CONV = {"FFT": 0, "DIRECT_BF16": 1, "DIRECT_BF16X3": 2}
 
 
+class LeniaTuneResult(ctypes.Structure):
+    _fields_ = [("conv_mode", ctypes.c_int), ("row_tile", ctypes.c_int), ("ms", ctypes.c_float * 3)]
+
+
 class LeniaWorldDesc(ctypes.Structure):
     _fields_ = [
         ("width", ctypes.c_int), ("height", ctypes.c_int), ("channels", ctypes.c_int),
@@ -127,6 +131,7 @@ def load() -> ctypes.CDLL:
         "lenia_set_conv_mode": ([P, ctypes.c_int], ctypes.c_int),
         "lenia_get_conv_mode": ([P], ctypes.c_int),
         "lenia_conv_macs": ([P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+        "lenia_autotune": ([P, ctypes.c_int, ctypes.POINTER(LeniaTuneResult)], ctypes.c_int),
         "lenia_set_snapshots": ([P, ctypes.c_int], ctypes.c_int),
         "lenia_launches_per_step": ([P], ctypes.c_int),
         "lenia_set_profiling": ([P, ctypes.c_int], ctypes.c_int),
@@ -164,6 +169,7 @@ def load() -> ctypes.CDLL:
         "lenia_batch_step": ([P, ctypes.c_int], ctypes.c_int),
         "lenia_batch_set_stream": ([P, ctypes.c_void_p], ctypes.c_int),
         "lenia_batch_sync": ([P], ctypes.c_int),
+        "lenia_batch_autotune": ([P, ctypes.c_int, ctypes.POINTER(LeniaTuneResult)], ctypes.c_int),
         "lenia_batch_launches_per_step": ([P], ctypes.c_int),
         "lenia_world_stats": ([P, ctypes.c_float, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
         "lenia_batch_stats": ([P, ctypes.c_float, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),

@@ -103,6 +103,20 @@ class Batch:
     def sync(self) -> None:
         self._check(self._lib.lenia_batch_sync(self._h))
 
+    def autotune(self, modes=("FFT", "DIRECT_BF16X3")) -> List[dict]:
+        """lenia_batch_autotune: per grid shape, the convolution mode and FFT
+        row tile that time fastest on its first world, applied to every world
+        of that shape; returns each world's choice."""
+        mask = 0
+        for m in modes:
+            mask |= 1 << _lib.CONV[m]
+        n = len(self.descs)
+        res = (_lib.LeniaTuneResult * n)()
+        self._check(self._lib.lenia_batch_autotune(self._h, mask, res))
+        names = {v: k for k, v in _lib.CONV.items()}
+        return [{"conv_mode": names[r.conv_mode], "row_tile": r.row_tile,
+                 "ms": {names[i]: (float(r.ms[i]) if r.ms[i] >= 0 else None) for i in range(3)}} for r in res]
+
     def stats(self, fill_threshold: float = 0.1) -> List[np.ndarray]:
         """Grid statistics of every world (channels x 9 doubles each)."""
         total = sum(d.channels for d in self.descs) * 9

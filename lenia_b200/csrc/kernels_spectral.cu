@@ -418,6 +418,7 @@ static bool fits(const FftPlan &p, int nlines, int threads, int cap)
 
 int row_tile(const Dims &d, const FftPlan &px)
 {
+    if (d.ty > 0 && d.H % d.ty == 0 && fits(px, d.ty, kRowThreads, kRowCap)) return d.ty;
     for (int ty = 32; ty >= 1; ty /= 2)
         if (d.H % ty == 0 && fits(px, ty, kRowThreads, kRowCap)) return ty;
     return 0;

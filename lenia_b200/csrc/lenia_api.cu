@@ -1031,6 +1031,84 @@ lenia_status lenia_set_conv_mode(lenia_world *w, int mode)
 
 int lenia_get_conv_mode(lenia_world *w) { return w ? w->conv_mode : -1; }
 
+// Times the growth stage (the convolution and the growth table) for every
+// allowed convolution mode and, on the FFT path's runtime-sized kernels, every
+// row tile that fits; keeps the fastest.  The grid state is untouched: the
+// growth stage only writes H, U_SUM and BACK, which the next step recomputes
+// (the mesh snapshot pair is not rotated while timing).
+lenia_status lenia_autotune(lenia_world *w, int modes, LeniaTuneResult *out)
+{
+    if (!w || !out) return LENIA_ERR_INVALID_ARG;
+    if ((modes & ~7) || !(modes & 7)) return fail(w, LENIA_ERR_INVALID_ARG, "autotune: mode mask %d", modes);
+    cudaError_t e = cudaStreamSynchronize(w->stream);
+    if (e != cudaSuccess) return cuda_fail(w, e, "autotune");
+    memset(out, 0, sizeof(*out));
+    for (int i = 0; i < 3; i++) out->ms[i] = -1.0f;
+    const bool snaps = w->snapshots;
+    const int launches = w->launches;
+    const int mode0 = w->conv_mode, ty0 = w->d.ty;
+    w->snapshots = false;
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    std::vector<int> tiles = {0};
+    if (!fast_supported(w->d)) {
+        tiles.clear();
+        for (int ty = 32; ty >= 1; ty /= 2) {
+            Dims t = w->d;
+            t.ty = ty;
+            if (row_tile(t, w->px) == ty) tiles.push_back(ty);
+        }
+    }
+    int best_mode = -1, best_ty = 0;
+    float best = 1e30f;
+    lenia_status s = LENIA_OK;
+    for (int mode = 0; mode < 3 && s == LENIA_OK; mode++) {
+        if (!((modes >> mode) & 1)) continue;
+        if (w->conv_mode != mode) {
+            w->conv_mode = mode;
+            if (build_kernels(w) != LENIA_OK) continue;  // e.g. a radius the direct modes do not take
+        }
+        const std::vector<int> cand = mode == LENIA_CONV_FFT ? tiles : std::vector<int>{ty0};
+        for (int ty : cand) {
+            w->d.ty = ty;
+            if ((s = stage_growth(w)) != LENIA_OK) break;  // warm-up
+            cudaEventRecord(a, w->stream);
+            for (int r = 0; r < 3 && s == LENIA_OK; r++) s = stage_growth(w);
+            cudaEventRecord(b, w->stream);
+            if (s != LENIA_OK) break;
+            if ((e = cudaEventSynchronize(b)) != cudaSuccess) {
+                s = cuda_fail(w, e, "autotune timing");
+                break;
+            }
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, a, b);
+            ms /= 3.0f;
+            if (out->ms[mode] < 0.0f || ms < out->ms[mode]) out->ms[mode] = ms;
+            if (ms < best) {
+                best = ms;
+                best_mode = mode;
+                best_ty = ty;
+            }
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    w->snapshots = snaps;
+    w->launches = launches;
+    if (s == LENIA_OK && best_mode < 0) s = fail(w, LENIA_ERR_UNSUPPORTED, "autotune: no allowed mode runs");
+    const int keep_mode = s == LENIA_OK ? best_mode : mode0;
+    w->d.ty = s == LENIA_OK ? best_ty : ty0;
+    if (w->conv_mode != keep_mode) {
+        w->conv_mode = keep_mode;
+        const lenia_status s2 = build_kernels(w);
+        if (s == LENIA_OK) s = s2;
+    }
+    out->conv_mode = w->conv_mode;
+    out->row_tile = w->d.ty;
+    return s;
+}
+
 lenia_status lenia_conv_macs(lenia_world *w, double *issued, double *useful)
 {
     if (!w) return LENIA_ERR_INVALID_ARG;
@@ -1396,6 +1474,44 @@ lenia_status lenia_batch_sync(lenia_batch *b)
         if (s != LENIA_OK) return bfail(b, s, "world %zu: %s", i, b->worlds[i]->err.c_str());
     }
     return LENIA_OK;
+}
+
+// Per grid shape (width, height): lenia_autotune on the first world of that
+// shape, its choice applied to every world of the shape; then both step
+// graphs are captured again.
+lenia_status lenia_batch_autotune(lenia_batch *b, int modes, LeniaTuneResult *per_world)
+{
+    if (!b) return LENIA_ERR_INVALID_ARG;
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return bfail(b, LENIA_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+    std::vector<int> done(b->worlds.size(), 0);
+    for (size_t i = 0; i < b->worlds.size(); i++) {
+        if (done[i]) continue;
+        lenia_world *rep = b->worlds[i];
+        LeniaTuneResult r;
+        lenia_status s = lenia_autotune(rep, modes, &r);
+        if (s != LENIA_OK) return bfail(b, s, "world %zu: %s", i, rep->err.c_str());
+        for (size_t j = i; j < b->worlds.size(); j++) {
+            lenia_world *w = b->worlds[j];
+            if (done[j] || w->d.W != rep->d.W || w->d.H != rep->d.H) continue;
+            done[j] = 1;
+            w->d.ty = r.row_tile;
+            if (w->conv_mode != r.conv_mode) {
+                w->conv_mode = r.conv_mode;
+                if ((s = build_kernels(w)) != LENIA_OK) return bfail(b, s, "world %zu: %s", j, w->err.c_str());
+            }
+            w->stream = b->stream;
+            if (per_world) per_world[j] = r;
+        }
+    }
+    for (cudaGraphExec_t &g : b->exec)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    lenia_status s = capture_step(b, 0);
+    if (s == LENIA_OK) s = capture_step(b, 1);
+    return s;
 }
 
 lenia_status lenia_batch_stats(lenia_batch *b, float fill_threshold, double *out)

@@ -29,6 +29,7 @@ struct Dims {
     int KX;       // W/2 + 1
     long long HS; // KX * D * H complex entries of a half spectrum
     long long P;  // (W+8)(H+8)(W+8): the reference's padded block (Q20)
+    int ty = 0;   // row tile of the runtime-sized row transforms (0: the largest that fits)
 };
 
 // Forward row pass: up to kMaxPairs pairs of real fields -> half spectra.

@@ -176,6 +176,22 @@ def config1(seed: int = 1, width: int = 128, mode: int = MODE_RT, radius: int = 
     return Workload(desc, ks, A0)
 
 
+def config2(seed: int = 2, width: int = 256, radius: int = 20) -> Workload:
+    """Precision workload: a width^3 grid with the plain step's modes
+    (3 channels, 9 kernels drawn as in config 0 but of the given radius,
+    central differences, RT with sigma 0.65, periodic borders) from the plain
+    step's seeded U(0,1) cube scaled to half the side."""
+    rng = np.random.default_rng(seed)
+    desc = WorldDesc(width=width, height=width, channels=3, timestep=0.2, theta_a=2.0,
+                     sigma=0.65, dd=1.0, growth_type=GROWTH_RT, mode_type=MODE_RT,
+                     sobel_border=BORDER_TORUS, border=BORDER_TORUS,
+                     gradient_mode=GRADIENT_CENTRAL_DIFF, blur_central_diff=False,
+                     mu_vel=False, asymptotic=(False,) * 4, soft_clip=(False,) * 4)
+    ks = sample_kernels(rng, 3, radius=radius)
+    A0 = seed_cube(rng, desc, width // 2)
+    return Workload(desc, ks, A0)
+
+
 CONFIG3_SIZES = (24, 32, 36, 44, 48, 64, 96)
 
 

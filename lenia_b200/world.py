@@ -64,12 +64,18 @@ class World:
 
     # --------------------------------------------------------------- fields
     def set(self, name: str, value) -> None:
-        """Writes a field from a numpy array (host) or a CUDA torch tensor."""
+        """Writes a field from a numpy array (host) or a CUDA torch tensor.
+        The device copy runs on the world's stream; with a tensor this call
+        first waits for the device's pending work (the tensor's producer may
+        run on another stream) and returns once the copy is done."""
         n = self.field_size(name) if name not in ("U_S", "SUM_S") else None
         if hasattr(value, "is_cuda") and value.is_cuda:
+            import torch
             t = value.contiguous()
+            torch.cuda.synchronize(t.device)
             self._check(self._lib.lenia_set_field(self._h, _lib.FIELD[name], ctypes.c_void_p(t.data_ptr()),
                                                   t.numel(), 1))
+            torch.cuda.synchronize(t.device)
             return
         a = np.ascontiguousarray(value, dtype=np.float32).ravel()
         self._check(self._lib.lenia_set_field(self._h, _lib.FIELD[name], a.ctypes.data_as(ctypes.c_void_p),
@@ -77,13 +83,17 @@ class World:
         del n
 
     def get(self, name: str, out=None):
-        """Reads a field into a new numpy array, or into `out` (numpy or CUDA tensor)."""
+        """Reads a field into a new numpy array, or into `out` (numpy or CUDA
+        tensor).  Into a tensor the copy runs on the world's stream and this
+        call returns once it is done, so `out` is ready on any stream."""
         n = self.field_size(name)
         if n == 0:
             raise _lib.LeniaError(1, f"field {name} is not available (enable debug or snapshots)")
         if out is not None and hasattr(out, "is_cuda") and out.is_cuda:
+            import torch
             self._check(self._lib.lenia_get_field(self._h, _lib.FIELD[name], ctypes.c_void_p(out.data_ptr()),
                                                   out.numel(), 1))
+            torch.cuda.synchronize(out.device)
             return out
         a = np.empty(n, dtype=np.float32) if out is None else out
         self._check(self._lib.lenia_get_field(self._h, _lib.FIELD[name], a.ctypes.data_as(ctypes.c_void_p),
@@ -130,6 +140,18 @@ class World:
         a, b = ctypes.c_double(), ctypes.c_double()
         self._check(self._lib.lenia_conv_macs(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def autotune(self, modes=("FFT", "DIRECT_BF16X3")) -> dict:
+        """Times the growth stage per allowed convolution mode (and the FFT
+        path's row tiles) and keeps the fastest (lenia_autotune)."""
+        mask = 0
+        for m in modes:
+            mask |= 1 << _lib.CONV[m]
+        r = _lib.LeniaTuneResult()
+        self._check(self._lib.lenia_autotune(self._h, mask, ctypes.byref(r)))
+        names = {v: k for k, v in _lib.CONV.items()}
+        return {"conv_mode": names[r.conv_mode], "row_tile": r.row_tile,
+                "ms": {names[i]: (float(r.ms[i]) if r.ms[i] >= 0 else None) for i in range(3)}}
 
     def set_stream(self, stream_ptr: int) -> None:
         self._check(self._lib.lenia_set_stream(self._h, ctypes.c_void_p(stream_ptr)))

@@ -38,14 +38,8 @@ MODES = ("FFT", "DIRECT_BF16", "DIRECT_BF16X3")
 
 def workload(width: int, radius: int, seed: int):
     from lenia_b200 import params as P
-    rng = np.random.default_rng(seed)
-    desc = P.WorldDesc(width=width, height=width, channels=3, timestep=0.2, theta_a=2.0, sigma=0.65, dd=1.0,
-                       growth_type=P.GROWTH_RT, mode_type=P.MODE_RT, sobel_border=P.BORDER_TORUS,
-                       border=P.BORDER_TORUS, gradient_mode=P.GRADIENT_CENTRAL_DIFF, blur_central_diff=False,
-                       mu_vel=False, asymptotic=(False,) * 4, soft_clip=(False,) * 4)
-    ks = P.sample_kernels(rng, 3, radius=radius)
-    A0 = P.seed_cube(rng, desc, width // 2)
-    return desc, ks, A0
+    wl = P.config2(seed=seed, width=width, radius=radius)
+    return wl.desc, wl.kernels, wl.A0
 
 
 def _err(x, ref):

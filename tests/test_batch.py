@@ -108,6 +108,45 @@ def test_batch_matches_worlds_stepped_alone():
 
 
 @pytest.mark.gpu
+def test_batch_autotune_then_matches_worlds_with_the_same_choice():
+    """After lenia_batch_autotune every world of a grid shape carries the
+    shape's choice, and the batch (graphs captured again) still matches
+    worlds stepped alone with that choice bit for bit."""
+    from lenia_b200.batch import Batch
+    from lenia_b200.world import World
+    wls = P.config3(6, seed=13, sizes=(24, 36, 48))
+    b = Batch([wl.desc for wl in wls], [wl.kernels for wl in wls], lanes=2)
+    for i, wl in enumerate(wls):
+        b.set_state(i, wl.A0)
+    b.step(1)
+    res = b.autotune()
+    print(res)
+    by_shape = {}
+    for wl, r in zip(wls, res):
+        key = (wl.desc.width, wl.desc.height)
+        assert by_shape.setdefault(key, (r["conv_mode"], r["row_tile"])) == (r["conv_mode"], r["row_tile"])
+        assert r["ms"]["FFT"] is not None and r["ms"]["DIRECT_BF16X3"] is not None
+    alone = []
+    for wl, r in zip(wls, res):
+        w = World(wl.desc, wl.kernels)
+        w.set_conv_mode(r["conv_mode"])
+        w.set_state(wl.A0.ravel())
+        w.step(1)
+        alone.append(w)
+    b.step(3)
+    for w in alone:
+        w.step(3)
+    b.sync()
+    for i, w in enumerate(alone):
+        for name in ("A", "V", "GA", "SUM"):
+            got, want = b.get(i, name), w.get(name)
+            assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (i, name)
+    for w in alone:
+        w.close()
+    b.close()
+
+
+@pytest.mark.gpu
 def test_batch_rejects_scratch_fields():
     from lenia_b200.batch import Batch
     from lenia_b200._lib import LeniaError

@@ -172,3 +172,35 @@ def test_mode_switch_and_errors(cuda_lib):
     st = w2._lib.lenia_set_conv_mode(w2.handle, _lib.CONV["DIRECT_BF16"])
     assert st == 7  # LENIA_ERR_UNSUPPORTED: radius * r_a above 64
     assert w2.conv_mode == "FFT"
+
+
+@pytest.mark.parametrize("shape", [(32, 32), (40, 24)])
+def test_autotune_keeps_state_and_picks_fastest(cuda_lib, shape):
+    """The autotuner times FFT (every row tile of the runtime-sized kernels
+    for a non-cubic grid) against BF16X3 and keeps the fastest; the grid state
+    is untouched and a tuned FFT world steps bit-identically to an untuned
+    one."""
+    from lenia_b200.world import World
+    w_, h_ = shape
+    wl = P.config0(seed=8, width=w_)
+    wl.desc.height = h_
+    wl.A0 = P.seed_cube(np.random.default_rng(8), wl.desc, min(w_, h_) // 2)
+    a, b = World(wl.desc, wl.kernels), World(wl.desc, wl.kernels)
+    for w in (a, b):
+        w.set_state(wl.A0.ravel())
+        w.step(2)
+    before = {n: a.get(n).copy() for n in ("A", "V", "GA", "SUM")}
+    r = a.autotune()
+    print(shape, r)
+    ms = {k: v for k, v in r["ms"].items() if v is not None}
+    assert set(ms) == {"FFT", "DIRECT_BF16X3"}
+    assert r["conv_mode"] == min(ms, key=ms.get) and a.conv_mode == r["conv_mode"]
+    for n, v in before.items():
+        assert np.array_equal(a.get(n).view(np.uint32), v.view(np.uint32)), n
+    if r["conv_mode"] == "FFT":
+        a.step(3)
+        b.step(3)
+        for n in ("A", "V", "GA", "SUM"):
+            assert np.array_equal(a.get(n).view(np.uint32), b.get(n).view(np.uint32)), n
+    with pytest.raises(Exception):
+        a.autotune(modes=())
