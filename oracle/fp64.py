@@ -147,10 +147,15 @@ class State:
 
 class Fp64Step:
     """One world of the float64 oracle.  After step(): .U (K, D, H, W),
-    .F (3, C, D, H, W), .H, .BACK, and the new state."""
+    .F (3, C, D, H, W), .H, .BACK, and the new state.
 
-    def __init__(self, desc, kernels, xp: Xp = None):
+    exact_bell=False keeps the reference's growth table (truncating index of
+    u into bell values on a 1/255 grid); True evaluates the growth as the
+    continuous bell(u, m, s) in double, the function the table samples."""
+
+    def __init__(self, desc, kernels, xp: Xp = None, exact_bell: bool = False):
         self.xp = xp or Xp()
+        self.exact_bell = exact_bell
         self.desc = desc
         self.kernels = list(kernels)
         d = desc
@@ -182,8 +187,13 @@ class Fp64Step:
 
     # ------------------------------------------------------------ growth
     def _growth_value(self, k, u):
-        """Entry of the growth table at the truncating index of u (double)."""
+        """Entry of the growth table at the truncating index of u (double),
+        or the exact bell of u."""
         xp = self.xp
+        if self.exact_bell:
+            kp = self.kernels[k]
+            q = (u - float(_f32(kp.m))) / float(_f32(kp.s))
+            return xp.exp(-(q * q) / 2.0)
         ui = xp.trunc_int(u * 255.0)
         f = ui + self.lut_base[k]
         valid = (f >= 0) & (f < (1 << 24))

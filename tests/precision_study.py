@@ -11,10 +11,12 @@ next to oracle/fp64.py on the same GPU in float64.  Per step and per mode:
   F     the same for the flow field F (3 x C x N)
   mass  max over channels of |sum A - sum A64| / sum A64
 
-Two regimes: "trajectory" (every path runs its own steps from the same
-start; errors include divergence of the dynamics) and "one-step" (before
-each step every world is reset to the oracle's state, so the errors are
-those of one step's arithmetic).
+Regimes: "trajectory" (every path runs its own steps from the same start;
+errors include divergence of the dynamics), "one-step" (before each step
+every world is reset to the oracle's state, so the errors are those of one
+step's arithmetic) and "one-step-exact" (the same against the oracle with
+the exact bell in place of the growth table: the table's quantisation then
+counts as error).
 
   python tests/precision_study.py --width 256 --radius 20 --steps 100 \
       --json out.json --md summary.md
@@ -55,7 +57,7 @@ def run(width=256, radius=20, steps=100, seed=2, regime="trajectory", modes=MODE
     dev = torch.device("cuda")
     desc, ks, A0 = workload(width, radius, seed)
     C, K, N = desc.channels, len(ks), desc.cells
-    ref = fp64.Fp64Step(desc, ks, fp64.Xp(dev))
+    ref = fp64.Fp64Step(desc, ks, fp64.Xp(dev), exact_bell=regime == "one-step-exact")
     ref.set_state(A0)
     worlds = {}
     for m in modes:
@@ -69,7 +71,7 @@ def run(width=256, radius=20, steps=100, seed=2, regime="trajectory", modes=MODE
     bufA = torch.empty(C * N, dtype=torch.float32, device=dev)
     rows = []
     for s in range(steps):
-        if regime == "one-step":
+        if regime.startswith("one-step"):
             st = ref.state
             for w in worlds.values():
                 for name, v in (("A", st.A), ("V", st.V), ("GA", st.GA), ("SUM", st.SUM)):

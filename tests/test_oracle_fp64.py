@@ -55,3 +55,21 @@ def test_rejects_other_modes():
     wl = P.config1(seed=1, width=32)
     with pytest.raises(NotImplementedError):
         fp64.Fp64Step(wl.desc, wl.kernels)
+
+
+def test_exact_bell_differs_only_by_table_quantisation(oracle_built):
+    """The exact-bell variant agrees with the table variant on u (the
+    convolution is the same) and its growth differs by at most one table
+    step of the bell."""
+    from oracle import fp64
+    wl = P.config0(seed=5)
+    a = fp64.Fp64Step(wl.desc, wl.kernels)
+    b = fp64.Fp64Step(wl.desc, wl.kernels, exact_bell=True)
+    for f in (a, b):
+        f.set_state(wl.A0)
+        f.step()
+    for ua, ub in zip(a.U, b.U):
+        assert np.array_equal(ua, ub)
+    hsum = sum(float(np.float32(k.h)) for k in wl.kernels)
+    for ha, hb in zip(a.H, b.H):
+        assert 0 < np.abs(ha - hb).max() <= hsum * 0.2
