@@ -209,6 +209,7 @@ def conv_measure(args):
     convolution mode, per-kernel device times from the library's profiler;
     the direct modes against the tensor-core peak (issued and useful
     multiply-adds); and the autotuner's choice for that world."""
+    from lenia_b200 import params as P
     from lenia_b200.world import World
     wl = P.config2(width=args.conv_width, radius=20)
     peak, peak_kind = measured_tensor_peak()

@@ -1509,8 +1509,10 @@ lenia_status lenia_batch_autotune(lenia_batch *b, int modes, LeniaTuneResult *pe
             cudaGraphExecDestroy(g);
             g = nullptr;
         }
-    lenia_status s = capture_step(b, 0);
-    if (s == LENIA_OK) s = capture_step(b, 1);
+    // the worlds' host pointers hold the current grid: the graph of the
+    // current parity is captured first (each capture swaps A and A_next)
+    lenia_status s = capture_step(b, b->parity);
+    if (s == LENIA_OK) s = capture_step(b, b->parity ^ 1);
     return s;
 }
 
