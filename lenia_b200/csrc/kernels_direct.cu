@@ -32,7 +32,9 @@
 // Input layout: P[part][c][zp][yp][xp] bf16, the grid padded periodically by R
 // cells on each side of every axis (zp = z + R, yp = y + R, xp = x + R; the
 // x extent rounded up to 8).  Output rows of a tile are consecutive padded
-// rows r = zp Hp + yp; rows in the y padding are computed and dropped.
+// rows r = zp Hp + yp, either running on across planes (rows in the y
+// padding are computed and dropped) or, when that needs fewer tiles, 128
+// rows y0..y0+127 of one plane.
 //
 // The tensor cores' accumulation adds each MMA's products into the FP32
 // accumulator with a rounding bias that grows with the number of MMAs per
@@ -97,6 +99,7 @@ struct DirGroup {
 struct DirLaunch {
     int W, H, D, C, R, Hp, rows_s, Kw, x3, ns;
     int seg_every;        // dz-runs between accumulator drains (0: one drain)
+    int nby;              // tiles per plane (0: tiles run on across planes)
     long long N;
     unsigned data_bytes;  // shared-memory bytes of one input tile slot
     unsigned data_tx;     // bytes TMA delivers into it
@@ -222,7 +225,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_direct(DirLaunch p, const __gri
 
     const DirGroup g = p.groups[blockIdx.z];
     const int tile_x = blockIdx.y * kTileX;
-    const long long row0 = (long long)p.R * p.Hp + (long long)blockIdx.x * kTileRows;
+    // padded row of the tile's first output row
+    const long long row0 =
+        p.nby > 0 ? (long long)(blockIdx.x / p.nby + p.R) * p.Hp + p.R + (long long)(blockIdx.x % p.nby) * kTileRows
+                  : (long long)p.R * p.Hp + (long long)blockIdx.x * kTileRows;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned ncols = g.nk <= 1 ? 128u : g.nk <= 2 ? 256u : 512u;
     const int npass = p.x3 ? 2 : 1;
@@ -563,6 +569,8 @@ struct DirectConv {
     size_t smem = 0;
     unsigned data_bytes = 0, data_tx = 0, strip_bytes = 0, stage_bytes = 0;
     int seg_every = 0;  // dz-runs per accumulator drain (0: one drain)
+    int nby = 0;        // tiles per plane (0: tiles run on across planes)
+    long long nb = 0;   // row tiles
     std::vector<DirGroup> groups;
     std::vector<DirPair> pairs;
     DirGroup *groups_dev = nullptr;
@@ -638,7 +646,12 @@ cudaError_t direct_create(const Dims &d, int C, const LeniaKernelParams *kernels
     }
     int strip0 = 0;
     const int nx = (d.W + kTileX - 1) / kTileX;
-    const long long nb = ((long long)d.D * dc->Hp + kTileRows - 1) / kTileRows;
+    // row tiles: across planes, or per plane when that takes fewer
+    const long long nb_flat = ((long long)d.D * dc->Hp + kTileRows - 1) / kTileRows;
+    const int nby = (d.H + kTileRows - 1) / kTileRows;
+    dc->nby = (long long)d.D * nby < nb_flat ? nby : 0;
+    dc->nb = dc->nby ? (long long)d.D * nby : nb_flat;
+    const long long nb = dc->nb;
     std::vector<int> pair_group;
     for (size_t gi = 0; gi < dc->groups.size(); gi++) {
         DirGroup &g = dc->groups[gi];
@@ -776,6 +789,7 @@ cudaError_t direct_convolve(DirectConv *dc, float *U, int *err, cudaStream_t st)
     p.x3 = dc->mode == LENIA_CONV_DIRECT_BF16X3;
     p.ns = dc->ns;
     p.seg_every = dc->seg_every;
+    p.nby = dc->nby;
     p.N = dc->d.N;
     p.data_bytes = dc->data_bytes;
     p.data_tx = dc->data_tx;
@@ -787,7 +801,7 @@ cudaError_t direct_convolve(DirectConv *dc, float *U, int *err, cudaStream_t st)
     p.strips_lo = (const unsigned char *)(dc->strips + dc->strip_count * dc->S * 64);
     p.U = U;
     p.err = err;
-    const long long nb = ((long long)dc->d.D * dc->Hp + kTileRows - 1) / kTileRows;
+    const long long nb = dc->nb;
     dim3 grid((unsigned)nb, (unsigned)((dc->d.W + kTileX - 1) / kTileX), (unsigned)dc->groups.size());
     k_direct<<<grid, kThreads, dc->smem, st>>>(p, dc->tm);
     return cudaGetLastError();

@@ -34,6 +34,10 @@ def _case(name):
                            asymptotic=(False,) * 4)
         ks = P.sample_kernels(rng, 3, radius=10)
         return P.Workload(desc, ks, P.seed_cube(rng, desc, 40))
+    if name == "plane_128":
+        # 128 rows of one plane per tile (fewer tiles than rows run on
+        # across planes with their y padding)
+        return P.config2(seed=4, width=128, radius=10)
     if name == "four_ch_64":
         # four kernels per source channel: four accumulators of 128 columns
         return P.config1(seed=2, width=64, radius=13)
@@ -69,7 +73,7 @@ def _worlds(wl, mode):
     return wf, wd
 
 
-@pytest.mark.parametrize("case", ["cfg0_32", "wide_144x40", "four_ch_64"])
+@pytest.mark.parametrize("case", ["cfg0_32", "wide_144x40", "four_ch_64", "plane_128"])
 @pytest.mark.parametrize("mode", ["DIRECT_BF16X3", "DIRECT_BF16"])
 def test_u_against_float64(cuda_lib, oracle_built, case, mode):
     wl = _case(case)
