@@ -15,8 +15,9 @@ sum over ranks divided by the slowest rank's time.  `--impl reference` times
 the CPU restatement of the reference's step (oracle, complex-to-complex
 spectral structure like the reference's FFTW path) on the host cores.
 
-Beside the headline (N = 1 only): `batched` (config 3 mix as one batch) and
-`conv_modes`: the growth stage of the 256^3, radius-20 precision workload in
+Beside the headline: `config1_schedule` (500 steps with every channel
+meshed every 10 steps, each mesh with its host synchronisation); and, with
+N = 1 only, `batched` (config 3 mix as one batch) and `conv_modes`: the growth stage of the 256^3, radius-20 precision workload in
 each convolution mode (FP32 FFT, direct BF16 and BF16x3 on the tensor cores,
 with the direct kernel's tensor roofline) and the autotuner's choice.
 """
@@ -474,6 +475,30 @@ def run_ours(args):
             "vertices": mesher.n_vertices, "triangles": mesher.n_triangles, "gpu_launches_per_mesh": 5}
     mesher.close()
 
+    # config 1's schedule: 500 steps with mesh snapshots, the grid of every
+    # channel meshed at the reference's iso value every 10 steps (view
+    # NORMAL, as the reference meshes its snapshot)
+    sched_steps, sched_every = (500, 10) if args.steps >= 500 else (50, 10)
+    ws = World(wl.desc, wl.kernels)
+    ws.set_stream(stream.cuda_stream)
+    ws.set_snapshots(True)
+    ws.set_state(wl.A0.ravel())
+    smesh = Mesher.for_view("NORMAL", wl.desc.width, wl.desc.height, C, iso_value=wl.desc.iso_value)
+    barrier()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    tri = 0
+    for i in range(sched_steps // sched_every):
+        ws.step(sched_every)
+        tri += smesh.run_world(ws, "NORMAL")[1]
+    s1.record(stream)
+    barrier()
+    sched_ms = max_over_ranks(s0.elapsed_time(s1))
+    schedule = {"steps": sched_steps, "mesh_every": sched_every, "ms": sched_ms,
+                "ms_per_step_with_meshing": sched_ms / sched_steps, "triangles_total": int(tri)}
+    smesh.close()
+    ws.close()
+
     batched = batch_measure(args, rank, n, stream, barrier, max_over_ranks) if args.batch_worlds > 0 else None
     conv = conv_measure(args) if (args.conv_width > 0 and n == 1) else None
 
@@ -497,6 +522,7 @@ def run_ours(args):
                               "frac": step_bytes_per_cell(wl) * N * args.steps / (ms / 1000.0) / 1e9 / peak},
             "kernels": kernels_table,
             "mesh": mesh,
+            "config1_schedule": schedule,
         }
         if batched is not None:
             line["batched"] = batched
