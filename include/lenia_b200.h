@@ -85,6 +85,9 @@ typedef struct LeniaWorldDesc {
     int soft_clip[LENIA_MAX_CHANNELS];
     int rt_all_channels; /* 0 = reference: SRT/RT transport channels 0-2 only */
     int alpha_index_fix; /* 0 = reference: PREALPHA/GA read at the padded offset */
+    int exact_bell;      /* 0 = reference: growth from the 256^3 table at the truncated
+                          * indices of u, m and s (Q1, lenia.h:79-84); 1 = bell(u, m, s)
+                          * evaluated for each cell (no quantisation of u) */
 } LeniaWorldDesc;
 
 /* One kernel: the parameter part of `Kernel` (render.h:347-361). */

@@ -181,9 +181,12 @@ lenia_status lenia_load(const char *path, lenia_world **out, unsigned long long 
         fprintf(stderr, "lenia_load: %s has version %u, this library reads %u\n", path, version, kVersion);
         return LENIA_ERR_UNSUPPORTED;
     }
-    if (rd.u32() != kDescWords) return LENIA_ERR_UNSUPPORTED;
-    uint32_t words[kDescWords];
-    for (uint32_t i = 0; i < kDescWords; i++) words[i] = rd.u32();
+    // a descriptor written before trailing fields were added is read with
+    // those fields 0 (their reference behaviour)
+    const uint32_t nwords = rd.u32();
+    if (nwords > kDescWords || nwords < 2) return LENIA_ERR_UNSUPPORTED;
+    uint32_t words[kDescWords] = {};
+    for (uint32_t i = 0; i < nwords; i++) words[i] = rd.u32();
     LeniaWorldDesc desc;
     memcpy(&desc, words, sizeof(desc));
     const uint32_t nk = rd.u32();

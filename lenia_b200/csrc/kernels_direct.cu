@@ -532,7 +532,10 @@ __global__ void k_growth_from_u(Dims d, GrowthJobs jobs, const float *__restrict
         const int c = jobs.c1[k];
         const int ui = (int)(u * 255);
         float l;
-        if (ui >= 0 && ui < 256) l = lut_rows[k * 256 + ui];
+        if (jobs.exact_bell) {
+            if (!(u == u)) bad = 1;
+            l = bell_dev(u, jobs.m[k], jobs.s[k]);
+        } else if (ui >= 0 && ui < 256) l = lut_rows[k * 256 + ui];
         else {
             if (!(u == u)) bad = 1;
             l = lut_flat_dev((long long)jobs.lut_base[k] + ui);

@@ -228,7 +228,10 @@ __global__ void __launch_bounds__(kRowThreads) k_growth_rows(Dims d, FftPlan px,
                 uacc[c * T + e] = uacc[c * T + e] + u;
                 const int ui = (int)(u * 255);
                 float l;
-                if (ui >= 0 && ui < 256) l = lut[k * 256 + ui];
+                if (jobs.exact_bell) {
+                    if (!(u == u)) bad = 1;
+                    l = bell_dev(u, jobs.m[k], jobs.s[k]);
+                } else if (ui >= 0 && ui < 256) l = lut[k * 256 + ui];
                 else {
                     if (!(u == u)) bad = 1;
                     l = lut_flat_dev((long long)jobs.lut_base[k] + ui);

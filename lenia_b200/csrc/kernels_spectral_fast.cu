@@ -237,7 +237,10 @@ __global__ void __launch_bounds__(kGrowthThreads) k_growth_rows_s(GrowthJobs job
                 u[i] = kPow2 ? re * kInvN : re / nf;
                 const int ui = (int)(u[i] * 255);
                 float l;
-                if (ui >= 0 && ui < 256) l = lut[k * 256 + ui];
+                if (jobs.exact_bell) {
+                    if (!(u[i] == u[i])) bad = 1;
+                    l = bell_dev(u[i], jobs.m[k], jobs.s[k]);
+                } else if (ui >= 0 && ui < 256) l = lut[k * 256 + ui];
                 else {
                     if (!(u[i] == u[i])) bad = 1;
                     l = lut_flat_dev((long long)jobs.lut_base[k] + ui);
@@ -387,7 +390,10 @@ __global__ void __launch_bounds__(kGwWarps * 32) k_growth_warp(GrowthJobs jobs, 
                 const float u = kPow2 ? re * kInvN : re / nf;
                 const int ui = (int)(u * 255);
                 float l;
-                if (ui >= 0 && ui < 256) l = lut[k * 256 + ui];
+                if (jobs.exact_bell) {
+                    if (!(u == u)) bad = 1;
+                    l = bell_dev(u, jobs.m[k], jobs.s[k]);
+                } else if (ui >= 0 && ui < 256) l = lut[k * 256 + ui];
                 else {
                     if (!(u == u)) bad = 1;
                     l = lut_flat_dev((long long)jobs.lut_base[k] + ui);

@@ -472,6 +472,11 @@ lenia_status stage_growth(lenia_world *w)
     }
     gj.growth_rt = w->desc.growth_type == LENIA_GROWTH_RT;
     gj.timestep = w->desc.timestep;
+    gj.exact_bell = w->desc.exact_bell;
+    for (int k = 0; k < w->K; k++) {
+        gj.m[k] = w->kernels[k].m;
+        gj.s[k] = w->kernels[k].s;
+    }
     if (w->conv_mode != LENIA_CONV_FFT) {
         // direct convolution on the tensor cores, then the growth from u_k
         if (!w->dconv && w->K > 0) return fail(w, LENIA_ERR_INVALID_ARG, "direct convolution has no plan");
@@ -993,7 +998,10 @@ lenia_status lenia_sync(lenia_world *w)
     if (e != cudaSuccess) return cuda_fail(w, e, "sync");
     if (flag) {
         cudaMemset(w->err_flag, 0, sizeof(int));
-        if (flag & 2) return fail(w, LENIA_ERR_TIMEOUT, "a tile copy of the flow or transport stage did not complete in time");
+        if (flag & 2)
+            return fail(w, LENIA_ERR_TIMEOUT,
+                        "a bounded wait ran out (a tile copy of the flow or transport stage, or the direct "
+                        "convolution's copy/MMA/drain pipeline)");
         return fail(w, LENIA_ERR_NONFINITE, "non-finite u met in the growth table lookup");
     }
     return LENIA_OK;

@@ -59,6 +59,9 @@ struct GrowthJobs {
     int soft_clip[kMaxChannels];
     int growth_rt;  // write BACK
     float timestep;
+    int exact_bell;            // growth = bell(u, m, s) instead of the table entry
+    float m[kMaxKernels];      // growth centre and width per kernel (exact_bell)
+    float s[kMaxKernels];
 };
 
 // Inverse row pass storing field/N (the blur).

@@ -66,6 +66,7 @@ class WorldDesc:
     soft_clip: Sequence[bool] = (False, False, False, False)
     rt_all_channels: bool = False  # False: SRT/RT move channels 0-2 only (Q7)
     alpha_index_fix: bool = False  # False: PREALPHA/GA channel offsets as the reference (Q20)
+    exact_bell: bool = False       # False: growth from the reference's 256^3 table (Q1); True: bell(u, m, s)
 
     @property
     def depth(self) -> int:

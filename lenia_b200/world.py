@@ -231,6 +231,8 @@ def read_checkpoint_header(path: str) -> dict:
     off = 20
     raw = data[off:off + 4 * nwords]
     off += 4 * nwords
+    # an older, shorter descriptor: trailing fields read as 0
+    raw = raw + bytes(max(0, ctypes.sizeof(_lib.LeniaWorldDesc) - len(raw)))
     cdesc = _lib.LeniaWorldDesc.from_buffer_copy(raw)
     d = {}
     for name, ctype in _lib.LeniaWorldDesc._fields_:

@@ -151,11 +151,12 @@ class Fp64Step:
 
     exact_bell=False keeps the reference's growth table (truncating index of
     u into bell values on a 1/255 grid); True evaluates the growth as the
-    continuous bell(u, m, s) in double, the function the table samples."""
+    continuous bell(u, m, s) in double, the function the table samples;
+    None follows the description's exact_bell flag."""
 
-    def __init__(self, desc, kernels, xp: Xp = None, exact_bell: bool = False):
+    def __init__(self, desc, kernels, xp: Xp = None, exact_bell: bool = None):
         self.xp = xp or Xp()
-        self.exact_bell = exact_bell
+        self.exact_bell = bool(getattr(desc, "exact_bell", False)) if exact_bell is None else exact_bell
         self.desc = desc
         self.kernels = list(kernels)
         d = desc

@@ -52,7 +52,7 @@ class OraParams(ctypes.Structure):
         ("osc_la_amt", ctypes.c_float), ("osc_flow_amt", ctypes.c_float),
         ("osc_div_flow_amt", ctypes.c_float),
         ("asymptotic", ctypes.c_int * 4), ("soft_clip", ctypes.c_int * 4),
-        ("rt_all_channels", ctypes.c_int), ("alpha_index_fix", ctypes.c_int),
+        ("rt_all_channels", ctypes.c_int), ("alpha_index_fix", ctypes.c_int), ("exact_bell", ctypes.c_int),
     ]
 
 
@@ -67,7 +67,7 @@ class OraKernel(ctypes.Structure):
 def make_params(d: dict) -> OraParams:
     p = OraParams()
     for name, ctype in OraParams._fields_:
-        v = d[name]
+        v = d.get(name, 0)
         if name in ("asymptotic", "soft_clip"):
             arr = (ctypes.c_int * 4)(*[int(bool(x)) for x in (list(v) + [0] * 4)[:4]])
             setattr(p, name, arr)

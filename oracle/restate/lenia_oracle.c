@@ -113,9 +113,12 @@ static float lut_flat(long f)
 
 float ora_bell_lut(int m, int s, int u) { return lut_flat((long)m * 65536 + s * 256 + u); }
 
-/* bell_lookup (lenia.h:79-84): truncating index into the 256^3 table. */
+/* bell_lookup (lenia.h:79-84): truncating index into the 256^3 table; with
+ * exact_bell (no counterpart in the reference) the bell itself. */
 static inline float growth_lookup(const ora_world *w, int k, float u)
 {
+    /* exact_bell: the function the table samples, at u itself */
+    if (w->p.exact_bell) return bell(u, w->kern[k].m, w->kern[k].s);
     int ui = (int)(u * 255);
     if (ui >= 0 && ui < 256) return w->lut[k * 256 + ui];
     return lut_flat((long)w->lut_base[k] + ui);

@@ -56,6 +56,7 @@ typedef struct {
     int soft_clip[ORA_MAX_CHANNELS];
     int rt_all_channels; /* 0: reference (SRT/RT move channels 0-2 only, Q7) */
     int alpha_index_fix; /* 0: reference (PREALPHA/GA channel offsets, Q20) */
+    int exact_bell;      /* 0: reference growth table (Q1); 1: bell(u, m, s) per cell */
 } ora_params;
 
 typedef struct {

@@ -34,9 +34,18 @@ VARIANTS = {
 }
 
 
+# name -> overrides of this library's clean-mode options (no counterpart in
+# the reference: pinned GPU against the C restatement only)
+CLEAN_VARIANTS = {
+    "exact_bell": dict(exact_bell=True),
+    "exact_bell_asym_softclip": dict(exact_bell=True, soft_clip=(True, False, True, False),
+                                     asymptotic=(False, True, True, False)),
+}
+
+
 def variant(name: str, seed: int = 3, width: int = 32) -> P.Workload:
     wl = P.config0(seed=seed, width=width)
-    for k, v in VARIANTS[name].items():
+    for k, v in {**VARIANTS, **CLEAN_VARIANTS}[name].items():
         setattr(wl.desc, k, v)
     return wl
 

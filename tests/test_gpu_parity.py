@@ -9,7 +9,7 @@ group of every step, every field, in every mode.
 import numpy as np
 import pytest
 
-from lenia_cases import VARIANTS, as_oracle, diff_report, four_channels, two_channel_div_flow, variant
+from lenia_cases import CLEAN_VARIANTS, VARIANTS, as_oracle, diff_report, four_channels, two_channel_div_flow, variant
 from lenia_b200 import params as P
 from oracle.oracle import RestateOracle
 
@@ -76,6 +76,15 @@ def run_staged(wl, steps=2):
 @pytest.mark.parametrize("name", sorted(VARIANTS))
 def test_stages_bit_exact(cuda_lib, oracle_built, name):
     problems = run_staged(variant(name))
+    assert not problems, "\n".join(problems[:12])
+
+
+@pytest.mark.parametrize("name", sorted(CLEAN_VARIANTS))
+def test_stages_bit_exact_clean_modes(cuda_lib, oracle_built, name):
+    """The library's exact-bell growth (no growth table) against the C
+    restatement with the same option."""
+    wl = variant(name, seed=21)
+    problems = run_staged(wl, steps=2)
     assert not problems, "\n".join(problems[:12])
 
 

@@ -73,3 +73,24 @@ def test_exact_bell_differs_only_by_table_quantisation(oracle_built):
     hsum = sum(float(np.float32(k.h)) for k in wl.kernels)
     for ha, hb in zip(a.H, b.H):
         assert 0 < np.abs(ha - hb).max() <= hsum * 0.2
+
+
+def test_exact_bell_option_of_the_restatement(oracle_built):
+    """exact_bell in the C restatement (float32) against the float64 oracle's
+    exact bell: the growth agrees to float32 rounding, with no table steps."""
+    from oracle import fp64
+    wl = P.config0(seed=5)
+    wl.desc.exact_bell = True
+    d = wl.desc
+    C = d.channels
+    ora = oracle_built.RestateOracle(d.as_dict(), [k.as_dict() for k in wl.kernels])
+    ora.set_state(A=wl.A0.ravel())
+    ora.run_event("FFT")
+    ora.run_event("FFT_MT")
+    f = fp64.Fp64Step(d, wl.kernels)
+    assert f.exact_bell
+    f.set_state(wl.A0)
+    f.step()
+    H32 = ora.get("H").reshape(C, -1).astype(np.float64)
+    H64 = np.stack([h.ravel() for h in f.H])
+    assert np.abs(H32 - H64).max() < 1e-3  # u differs by ~1e-6, the bell slope is up to ~1/s
