@@ -19,7 +19,10 @@ the exact bell in place of the growth table: the table's quantisation then
 counts as error).
 
   python tests/precision_study.py --width 256 --radius 20 --steps 100 \
-      --json out.json --md summary.md
+      --json out.json --md summary.md [--exact-bell]
+
+--exact-bell runs worlds and oracle with the exact-bell growth option (no
+growth table), so that no growth-table bin flips mask the arithmetic.
 """
 from __future__ import annotations
 
@@ -38,9 +41,10 @@ if ROOT not in sys.path:
 MODES = ("FFT", "DIRECT_BF16", "DIRECT_BF16X3")
 
 
-def workload(width: int, radius: int, seed: int):
+def workload(width: int, radius: int, seed: int, exact_bell: bool = False):
     from lenia_b200 import params as P
     wl = P.config2(seed=seed, width=width, radius=radius)
+    wl.desc.exact_bell = exact_bell
     return wl.desc, wl.kernels, wl.A0
 
 
@@ -50,14 +54,14 @@ def _err(x, ref):
     return float(d.max()), float(torch.linalg.vector_norm(x.double() - ref) / torch.linalg.vector_norm(ref))
 
 
-def run(width=256, radius=20, steps=100, seed=2, regime="trajectory", modes=MODES, log=None):
+def run(width=256, radius=20, steps=100, seed=2, regime="trajectory", modes=MODES, log=None, exact_bell=False):
     import torch
     from lenia_b200.world import World
     from oracle import fp64
     dev = torch.device("cuda")
-    desc, ks, A0 = workload(width, radius, seed)
+    desc, ks, A0 = workload(width, radius, seed, exact_bell)
     C, K, N = desc.channels, len(ks), desc.cells
-    ref = fp64.Fp64Step(desc, ks, fp64.Xp(dev), exact_bell=regime == "one-step-exact")
+    ref = fp64.Fp64Step(desc, ks, fp64.Xp(dev), exact_bell=exact_bell or regime == "one-step-exact")
     ref.set_state(A0)
     worlds = {}
     for m in modes:
@@ -132,14 +136,18 @@ def main():
     ap.add_argument("--regimes", default="one-step,trajectory")
     ap.add_argument("--json", default=None)
     ap.add_argument("--md", default=None)
+    ap.add_argument("--exact-bell", action="store_true",
+                    help="worlds and oracle with the exact-bell growth option (no growth table)")
     a = ap.parse_args()
     results = {}
     for regime in a.regimes.split(","):
-        results[regime] = run(a.width, a.radius, a.steps, a.seed, regime, log=sys.stdout)
+        results[regime] = run(a.width, a.radius, a.steps, a.seed, regime, log=sys.stdout, exact_bell=a.exact_bell)
     if a.json:
         with open(a.json, "w") as f:
             json.dump(results, f)
     md = summary_md(results, a.width, a.radius, a.steps)
+    if a.exact_bell:
+        md = md.replace("float64 oracle,", "float64 oracle (exact-bell growth in worlds and oracle),", 1)
     if a.md:
         with open(a.md, "w") as f:
             f.write(md)
