@@ -147,6 +147,40 @@ def test_batch_autotune_then_matches_worlds_with_the_same_choice():
 
 
 @pytest.mark.gpu
+def test_batch_runs_the_direct_convolution_in_its_graphs():
+    """With the autotuner restricted to BF16X3 every world of the batch
+    convolves on the tensor cores inside the captured step graphs, bit for
+    bit as worlds stepped alone in that mode."""
+    from lenia_b200.batch import Batch
+    from lenia_b200.world import World
+    wls = P.config3(4, seed=14, sizes=(24, 32))
+    b = Batch([wl.desc for wl in wls], [wl.kernels for wl in wls], lanes=2)
+    for i, wl in enumerate(wls):
+        b.set_state(i, wl.A0)
+    res = b.autotune(modes=("DIRECT_BF16X3",))
+    assert all(r["conv_mode"] == "DIRECT_BF16X3" for r in res)
+    alone = []
+    for wl in wls:
+        w = World(wl.desc, wl.kernels)
+        w.set_conv_mode("DIRECT_BF16X3")
+        w.set_state(wl.A0.ravel())
+        alone.append(w)
+    b.step(3)
+    for w in alone:
+        w.step(3)
+    b.sync()
+    for i, w in enumerate(alone):
+        w.sync()
+        for name in ("A", "V", "GA", "SUM"):
+            got, want = b.get(i, name), w.get(name)
+            assert np.isfinite(got).all()
+            assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (i, name)
+    for w in alone:
+        w.close()
+    b.close()
+
+
+@pytest.mark.gpu
 def test_batch_rejects_scratch_fields():
     from lenia_b200.batch import Batch
     from lenia_b200._lib import LeniaError
