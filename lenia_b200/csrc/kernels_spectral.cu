@@ -462,7 +462,7 @@ static cudaError_t set_smem(const void *fn, size_t bytes)
 cudaError_t launch_fwd_rows(const Dims &d, const FftPlan &px, const float2 *tw_x, const FwdRowJobs &jobs,
                             cudaStream_t st)
 {
-    if (fast_supported(d)) return launch_fwd_rows_fast(d, tw_x, jobs, st);
+    if (fast_rows_supported(d)) return launch_fwd_rows_fast(d, tw_x, jobs, st);
     const int TY = row_tile(d, px);
     if (TY == 0) return cudaErrorInvalidValue;
     const size_t smem = (size_t)(d.W + TY * d.W) * sizeof(float2);
@@ -500,7 +500,7 @@ cudaError_t launch_growth_rows(const Dims &d, const FftPlan &px, const float2 *t
                                const float *lut_rows, const float *A, float *H, float *U_SUM, float *BACK,
                                float *U_dbg, int *err_flag, cudaStream_t st)
 {
-    if (fast_supported(d))
+    if (fast_rows_supported(d))
         return launch_growth_rows_fast(d, tw_x_inv, jobs, lut_rows, A, H, U_SUM, BACK, U_dbg, err_flag, st);
     int TY = row_tile(d, px);
     if (TY == 0) return cudaErrorInvalidValue;
@@ -521,7 +521,7 @@ cudaError_t launch_growth_rows(const Dims &d, const FftPlan &px, const float2 *t
 cudaError_t launch_blur_rows(const Dims &d, const FftPlan &px, const float2 *tw_x_inv, const BlurJobs &jobs,
                              cudaStream_t st)
 {
-    if (fast_supported(d)) return launch_blur_rows_fast(d, tw_x_inv, jobs, st);
+    if (fast_rows_supported(d)) return launch_blur_rows_fast(d, tw_x_inv, jobs, st);
     const int TY = row_tile(d, px);
     if (TY == 0) return cudaErrorInvalidValue;
     const size_t smem = (size_t)(d.W + TY * d.W) * sizeof(float2);

@@ -26,11 +26,12 @@ constexpr int kFastRowThreads = 256;
 constexpr int kFastPlaneThreads = LENIA_PLANE_THREADS;    // block of the plane transform
 constexpr int kGrowthThreads = LENIA_GROWTH_THREADS;      // block of the growth pass
 
-// Rows per tile of the growth pass.
+// Rows per tile of the growth pass: at most 2048 cells, so that a thread's
+// cells (prefetched spectra and growth sums in registers) stay at 8.
 constexpr int growth_tile_for(int n)
 {
     for (int t = LENIA_GROWTH_ROWS; t > 1; t--)
-        if (n % t == 0) return t;
+        if (n % t == 0 && t * n <= 2048) return t;
     return 1;
 }
 
@@ -527,6 +528,9 @@ cudaError_t blur_rows_w(const float2 *tw, const BlurJobs &jobs, cudaStream_t st)
 }  // namespace
 
 #define LENIA_FAST_SIZES(X) X(24) X(32) X(36) X(44) X(48) X(64) X(96) X(128)
+// Row transforms also for 256: a 256 x 256 plane does not fit shared memory,
+// so the plane transforms of that size run as the runtime-sized split passes.
+#define LENIA_FAST_ROW_SIZES(X) LENIA_FAST_SIZES(X) X(256)
 
 bool fast_supported(const Dims &d)
 {
@@ -540,11 +544,23 @@ bool fast_supported(const Dims &d)
     }
 }
 
+bool fast_rows_supported(const Dims &d)
+{
+    if (d.W != d.H) return false;
+    switch (d.W) {
+#define CASE(n) case n:
+        LENIA_FAST_ROW_SIZES(CASE)
+#undef CASE
+        return true;
+    default: return false;
+    }
+}
+
 cudaError_t launch_fwd_rows_fast(const Dims &d, const float2 *tw_x, const FwdRowJobs &jobs, cudaStream_t st)
 {
     switch (d.W) {
 #define CASE(n) case n: return fwd_rows_w<n>(d, tw_x, jobs, st);
-        LENIA_FAST_SIZES(CASE)
+        LENIA_FAST_ROW_SIZES(CASE)
 #undef CASE
     default: return cudaErrorInvalidValue;
     }
@@ -568,7 +584,7 @@ cudaError_t launch_growth_rows_fast(const Dims &d, const float2 *tw_x_inv, const
     switch (d.W) {
 #define CASE(n) \
     case n: return growth_rows_w<n>(tw_x_inv, jobs, lut_rows, A, H, U_SUM, BACK, U_dbg, err_flag, st);
-        LENIA_FAST_SIZES(CASE)
+        LENIA_FAST_ROW_SIZES(CASE)
 #undef CASE
     default: return cudaErrorInvalidValue;
     }
@@ -578,7 +594,7 @@ cudaError_t launch_blur_rows_fast(const Dims &d, const float2 *tw_x_inv, const B
 {
     switch (d.W) {
 #define CASE(n) case n: return blur_rows_w<n>(tw_x_inv, jobs, st);
-        LENIA_FAST_SIZES(CASE)
+        LENIA_FAST_ROW_SIZES(CASE)
 #undef CASE
     default: return cudaErrorInvalidValue;
     }

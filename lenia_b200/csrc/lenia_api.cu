@@ -1060,7 +1060,7 @@ lenia_status lenia_autotune(lenia_world *w, int modes, LeniaTuneResult *out)
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     std::vector<int> tiles = {0};
-    if (!fast_supported(w->d)) {
+    if (!fast_rows_supported(w->d)) {
         tiles.clear();
         for (int ty = 32; ty >= 1; ty /= 2) {
             Dims t = w->d;

@@ -138,6 +138,9 @@ cudaError_t launch_transport(const StepParams &p, const TransportBuffers &b, cud
 // Size-specialised spectral kernels (kernels_spectral_fast.cu) for cubic
 // grids of the sizes they are instantiated for.
 bool fast_supported(const Dims &d);
+// The size-specialised row transforms (forward rows, growth, blur) also
+// serve cubic grids whose planes use the runtime-sized plane passes.
+bool fast_rows_supported(const Dims &d);
 cudaError_t launch_fwd_rows_fast(const Dims &d, const float2 *tw_x, const FwdRowJobs &jobs, cudaStream_t st);
 cudaError_t launch_planes_fast(const Dims &d, const float2 *tw_y, const float2 *tw_z, const PlaneJobs &jobs, int sign,
                                cudaStream_t st);

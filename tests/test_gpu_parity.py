@@ -130,6 +130,25 @@ def test_stages_bit_exact_split_planes(cuda_lib, oracle_built):
     assert not problems, "\n".join(problems[:12])
 
 
+def test_growth_stage_bit_exact_256(cuda_lib, oracle_built):
+    """256^3: the size-specialised row transforms with the split plane passes
+    (a 256 x 256 plane exceeds shared memory) give the growth stage's u_k, H,
+    U_SUM and BACK bit for bit (2 channels, 2 kernels keep the CPU side short)."""
+    wl = P.config2(seed=9, width=256, radius=12)
+    wl.desc.channels = 2
+    wl.kernels = [k for k in wl.kernels if k.c0 < 2 and k.c1 < 2][:2]
+    wl.A0 = wl.A0[:2].copy()
+    ora, gpu = make_pair(wl)
+    for ev in GROWTH_EVENTS:
+        ora.run_event(ev)
+    gpu.stage("GROWTH")
+    gpu.sync()
+    problems = []
+    compare(ora, gpu, ["U", "H", "U_SUM", "BACK"], "256^3 GROWTH", problems)
+    gpu.close()
+    assert not problems, "\n".join(problems[:12])
+
+
 def test_trajectory_bit_exact_cfg0(cuda_lib, oracle_built):
     """Whole steps (the production path, no debug outputs) stay bit-exact over
     100 steps of the 32^3 plain-step configuration."""
