@@ -88,6 +88,10 @@ typedef struct LeniaWorldDesc {
     int exact_bell;      /* 0 = reference: growth from the 256^3 table at the truncated
                           * indices of u, m and s (Q1, lenia.h:79-84); 1 = bell(u, m, s)
                           * evaluated for each cell (no quantisation of u) */
+    int conserve_mass;   /* 0 = reference; 1 = after every step each channel is rescaled
+                          * so that its total (summed in double on the GPU, fixed order)
+                          * equals the total it had when the grid was last written
+                          * (lenia_set_field of A, lenia_create, lenia_set_params) */
 } LeniaWorldDesc;
 
 /* One kernel: the parameter part of `Kernel` (render.h:347-361). */

@@ -50,6 +50,7 @@ class LeniaWorldDesc(ctypes.Structure):
         ("osc_div_flow_amt", ctypes.c_float),
         ("asymptotic", ctypes.c_int * MAX_CHANNELS), ("soft_clip", ctypes.c_int * MAX_CHANNELS),
         ("rt_all_channels", ctypes.c_int), ("alpha_index_fix", ctypes.c_int), ("exact_bell", ctypes.c_int),
+        ("conserve_mass", ctypes.c_int),
     ]
 
 

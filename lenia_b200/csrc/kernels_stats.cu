@@ -76,7 +76,64 @@ __global__ void k_stats_final(const double *__restrict__ partial, int nblk, doub
     out[c * kStats + j] = r;
 }
 
+// Channel totals for mass conservation: the same fixed-order two-pass sum.
+__global__ void __launch_bounds__(kStatThreads) k_mass_partial(const float *__restrict__ A, long long N,
+                                                               double *__restrict__ partial, int nblk)
+{
+    __shared__ double s[kStatThreads];
+    const int c = blockIdx.y, t = threadIdx.x;
+    const long long per = (N + nblk - 1) / nblk;
+    const long long beg = blockIdx.x * per, end = beg + per < N ? beg + per : N;
+    const float *a = A + (long long)c * N;
+    double v = 0.0;
+    for (long long i = beg + t; i < end; i += kStatThreads) v += (double)__ldg(a + i);
+    s[t] = v;
+    __syncthreads();
+    for (int o = kStatThreads / 2; o > 0; o >>= 1) {
+        if (t < o) s[t] = s[t] + s[t + o];
+        __syncthreads();
+    }
+    if (t == 0) partial[(long long)c * nblk + blockIdx.x] = s[0];
+}
+
+__global__ void k_mass_final(const double *__restrict__ partial, int nblk, int C, double *__restrict__ out)
+{
+    const int c = threadIdx.x;
+    if (c >= C) return;
+    double r = 0.0;
+    for (int b = 0; b < nblk; b++) r = r + partial[(long long)c * nblk + b];
+    out[c] = r;
+}
+
+// A_c *= float(target_c / total_c) (no change for an empty channel).
+__global__ void k_mass_scale(float *__restrict__ A, long long N, int C, const double *__restrict__ target,
+                             const double *__restrict__ total)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)C * N) return;
+    const int c = (int)(i / N);
+    const double m = total[c];
+    if (!(m > 0.0)) return;
+    A[i] = A[i] * (float)(target[c] / m);
+}
+
 }  // namespace
+
+cudaError_t launch_mass_totals(const float *A, const Dims &d, int C, double *partial, int nblk, double *out,
+                               cudaStream_t st)
+{
+    k_mass_partial<<<dim3(nblk, C), kStatThreads, 0, st>>>(A, d.N, partial, nblk);
+    k_mass_final<<<1, 32, 0, st>>>(partial, nblk, C, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mass_scale(float *A, const Dims &d, int C, const double *target, const double *total,
+                              cudaStream_t st)
+{
+    const long long n = (long long)C * d.N;
+    k_mass_scale<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(A, d.N, C, target, total);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_stats(const float *A, const Dims &d, int C, const double *trig, float fill, double *partial,
                          int nblk, double *out, cudaStream_t st)

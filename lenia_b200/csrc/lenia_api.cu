@@ -86,13 +86,14 @@ enum KernelId {
     KID_DIRECT_PAD,
     KID_DIRECT_CONV,
     KID_GROWTH_U,
+    KID_MASS,
     KID_MAX
 };
 const char *const kKernelNames[KID_MAX] = {"fwd_rows",          "planes_fwd",          "planes_inv",
                                            "growth_rows",       "blur_fwd_rows",       "blur_planes_fwd",
                                            "blur_planes_inv",   "blur_rows",           "flow",
                                            "transport",         "direct_pad",          "direct_conv",
-                                           "growth_u"};
+                                           "growth_u",          "mass"};
 
 struct ProfRec {
     int kid;
@@ -132,6 +133,8 @@ struct lenia_world {
     bool blur_valid = false;  // U_S / SUM_S hold a blur result
     int conv_mode = LENIA_CONV_FFT;
     DirectConv *dconv = nullptr;  // plan of the direct convolution modes
+    // conserve_mass: the channel totals to restore, this step's totals, partials
+    double *mass_target = nullptr, *mass_total = nullptr, *mass_partial = nullptr;
     // profiling
     bool profile = false;
     std::vector<ProfRec> prof_pending;
@@ -398,7 +401,7 @@ void free_world(lenia_world *w)
     for (float *p : fs)
         if (p) cudaFree(p);
     void *vs[] = {w->lut_base, w->kp_dev, w->tw_x_fwd, w->tw_x_inv, w->tw_y_fwd, w->tw_y_inv, w->err_flag,
-                  w->stats_trig, w->stats_partial};
+                  w->stats_trig, w->stats_partial, w->mass_target, w->mass_total, w->mass_partial};
     for (void *p : vs)
         if (p) cudaFree(p);
     direct_destroy(w->dconv);
@@ -435,6 +438,24 @@ lenia_status world_stats_async(lenia_world *w, float fill, double *dst)
     }
     e = launch_stats(w->A, w->d, w->C, w->stats_trig, fill, w->stats_partial, kStatBlocks, dst, w->stream);
     if (e != cudaSuccess) return cuda_fail(w, e, "statistics");
+    return LENIA_OK;
+}
+
+constexpr int kMassBlocks = 64;
+
+// conserve_mass: records the current channel totals of A as the totals every
+// later step restores (allocates its buffers on first use; stream-ordered).
+lenia_status mass_record_target(lenia_world *w)
+{
+    cudaError_t e = cudaSuccess;
+    if (!w->mass_target) {
+        w->mass_target = dalloc<double>(kMaxChannels, e);
+        w->mass_total = dalloc<double>(kMaxChannels, e);
+        w->mass_partial = dalloc<double>((size_t)kMaxChannels * kMassBlocks, e);
+        if (e != cudaSuccess) return cuda_fail(w, e, "mass conservation buffers");
+    }
+    e = launch_mass_totals(w->A, w->d, w->C, w->mass_partial, kMassBlocks, w->mass_target, w->stream);
+    if (e != cudaSuccess) return cuda_fail(w, e, "mass totals");
     return LENIA_OK;
 }
 
@@ -680,6 +701,17 @@ lenia_status stage_transport(lenia_world *w)
     if (e != cudaSuccess) return cuda_fail(w, e, "transport");
     std::swap(w->A, w->A_next);
     w->launches++;
+    if (w->desc.conserve_mass) {
+        // the new grid's channel totals (double, fixed order), then the
+        // rescaling that restores the recorded totals
+        if (!w->mass_target) return fail(w, LENIA_ERR_INVALID_ARG, "conserve_mass has no recorded totals");
+        ProfScope ps(w, KID_MASS);
+        if ((e = launch_mass_totals(w->A, w->d, w->C, w->mass_partial, kMassBlocks, w->mass_total, w->stream)) !=
+                cudaSuccess ||
+            (e = launch_mass_scale(w->A, w->d, w->C, w->mass_target, w->mass_total, w->stream)) != cudaSuccess)
+            return cuda_fail(w, e, "mass conservation");
+        w->launches += 3;
+    }
     return LENIA_OK;
 }
 
@@ -827,6 +859,7 @@ lenia_status create_world(const LeniaWorldDesc *desc, const LeniaKernelParams *k
         return s;
     }
     s = build_kernels(w);
+    if (s == LENIA_OK && w->desc.conserve_mass) s = mass_record_target(w);
     if (s != LENIA_OK) {
         fprintf(stderr, "lenia_create: %s\n", w->err.c_str());
         free_world(w);
@@ -872,6 +905,7 @@ lenia_status lenia_set_params(lenia_world *w, const LeniaWorldDesc *desc)
     if (desc->width != w->desc.width || desc->height != w->desc.height || desc->channels != w->desc.channels)
         return fail(w, LENIA_ERR_INVALID_ARG, "set_params cannot change the grid shape or channel count");
     w->desc = *desc;
+    if (desc->conserve_mass) return mass_record_target(w);
     return LENIA_OK;
 }
 
@@ -933,6 +967,7 @@ lenia_status lenia_set_field(lenia_world *w, int field, const float *src, size_t
                                     on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, w->stream);
     if (e == cudaSuccess && !on_device) e = cudaStreamSynchronize(w->stream);
     if (e != cudaSuccess) return cuda_fail(w, e, "set_field");
+    if (field == LENIA_FIELD_A && w->desc.conserve_mass) return mass_record_target(w);
     return LENIA_OK;
 }
 

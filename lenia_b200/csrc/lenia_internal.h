@@ -155,6 +155,12 @@ constexpr int kStats = 9;
 constexpr int kStatBlocks = 64;
 cudaError_t launch_stats(const float *A, const Dims &d, int C, const double *trig, float fill, double *partial,
                          int nblk, double *out, cudaStream_t st);
+// Per-channel totals of A in double (fixed summation order) into out[C], and
+// the rescaling A_c *= float(target_c / total_c) that restores them.
+cudaError_t launch_mass_totals(const float *A, const Dims &d, int C, double *partial, int nblk, double *out,
+                               cudaStream_t st);
+cudaError_t launch_mass_scale(float *A, const Dims &d, int C, const double *target, const double *total,
+                              cudaStream_t st);
 
 // Host FFT plans and twiddle tables (lenia_api.cu).
 int fft_factor(int n, int *radix);

@@ -67,6 +67,7 @@ class WorldDesc:
     rt_all_channels: bool = False  # False: SRT/RT move channels 0-2 only (Q7)
     alpha_index_fix: bool = False  # False: PREALPHA/GA channel offsets as the reference (Q20)
     exact_bell: bool = False       # False: growth from the reference's 256^3 table (Q1); True: bell(u, m, s)
+    conserve_mass: bool = False    # True: each channel's total restored after every step (FP64 sums on the GPU)
 
     @property
     def depth(self) -> int:
