@@ -175,6 +175,8 @@ __global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p
         mbar_init_fence();
     }
     __syncthreads();
+    pdl_trigger();
+    pdl_wait();
     // field 0 is SUM, field 1 + c is H channel c
     auto issue = [&](int f) {
         if (!leader) return;
@@ -402,8 +404,7 @@ cudaError_t launch_flow(const StepParams &p, const FlowBuffers &b, cudaStream_t 
     dim3 grid(tiles_x * tiles_y, (d.D + kFlowZ - 1) / kFlowZ);
     dim3 block(kFX, kFY);
     const size_t smem = 2 * kTile * sizeof(float);
-    k_flow<<<grid, block, smem, st>>>(p, b, tm_sum, tm_h);
-    return cudaGetLastError();
+    return launch_pdl(k_flow, grid, block, smem, st, p, b, tm_sum, tm_h);
 }
 
 }  // namespace lenia

@@ -60,6 +60,8 @@ __global__ void __launch_bounds__(kFastRowThreads) k_fwd_rows_s(FwdRowJobs jobs,
     float2 *oa = jobs.out[2 * pair];
     float2 *ob = jobs.out[2 * pair + 1];
     for (int i = threadIdx.x; i < W; i += kFastRowThreads) tw[i] = tw_x[i];
+    pdl_trigger();
+    pdl_wait();
     const long long base = ((long long)z * H + y0) * W;
     for (int e = threadIdx.x; e < TY * W; e += kFastRowThreads) {
         const int ty = e / W, x = e % W;
@@ -96,6 +98,8 @@ __global__ void __launch_bounds__(kFastPlaneThreads) k_planes_s(PlaneJobs jobs, 
     const float *kc = jobs.kc[job];
     for (int i = threadIdx.x; i < H; i += kFastPlaneThreads) twy[i] = tw_y[i];
     for (int i = threadIdx.x; i < D; i += kFastPlaneThreads) twz[i] = tw_z[i];
+    pdl_trigger();
+    pdl_wait();
     constexpr int KZ = D / 2 + 1, KY = H / 2 + 1;
     if (kc) {
         const float *kp = kc + (long long)kx * KZ * KY;
@@ -148,7 +152,8 @@ __device__ __forceinline__ void load_packed_rows_s(float2 *buf, const float2 *s0
     }
 }
 
-template <int W>
+// EXACT: the exact-bell growth (a separate instance keeps the table path as it was)
+template <int W, bool EXACT>
 __global__ void __launch_bounds__(kGrowthThreads) k_growth_rows_s(GrowthJobs jobs, const float2 *__restrict__ tw_x,
                                                                    const float *__restrict__ lut_rows,
                                                                    const float *__restrict__ A,
@@ -170,6 +175,8 @@ __global__ void __launch_bounds__(kGrowthThreads) k_growth_rows_s(GrowthJobs job
     const float nf = (float)N;
     for (int i = threadIdx.x; i < W; i += kGrowthThreads) tw[i] = tw_x[i];
     for (int i = threadIdx.x; i < 256 * K; i += kGrowthThreads) lut[i] = lut_rows[i];
+    pdl_trigger();
+    pdl_wait();
 
     // The packed row spectrum of a kernel pair: element e of the tile is
     // (ty = e % TY, kx = e / TY); its half-spectrum values are prefetched into
@@ -238,7 +245,7 @@ __global__ void __launch_bounds__(kGrowthThreads) k_growth_rows_s(GrowthJobs job
                 u[i] = kPow2 ? re * kInvN : re / nf;
                 const int ui = (int)(u[i] * 255);
                 float l;
-                if (jobs.exact_bell) {
+                if (EXACT) {
                     if (!(u[i] == u[i])) bad = 1;
                     l = bell_dev(u[i], jobs.m[k], jobs.s[k]);
                 } else if (ui >= 0 && ui < 256) l = lut[k * 256 + ui];
@@ -469,8 +476,7 @@ cudaError_t fwd_rows_w(const Dims &d, const float2 *tw, const FwdRowJobs &jobs, 
     const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2);
     cudaError_t e = smem_attr((const void *)k_fwd_rows_s<W>, smem);
     if (e != cudaSuccess) return e;
-    k_fwd_rows_s<W><<<dim3(W * (W / S::TY), jobs.npairs), kFastRowThreads, smem, st>>>(jobs, tw);
-    return cudaGetLastError();
+    return launch_pdl(k_fwd_rows_s<W>, dim3(W * (W / S::TY), jobs.npairs), dim3(kFastRowThreads), smem, st, jobs, tw);
 }
 
 template <int W>
@@ -480,8 +486,8 @@ cudaError_t planes_w(const Dims &d, const float2 *twy, const float2 *twz, const 
     const size_t smem = (size_t)(2 * W + PadMat<W>::size(W)) * sizeof(float2);
     cudaError_t e = smem_attr((const void *)k_planes_s<W>, smem);
     if (e != cudaSuccess) return e;
-    k_planes_s<W><<<dim3(W / 2 + 1, jobs.njobs), kFastPlaneThreads, smem, st>>>(jobs, twy, twz, sign);
-    return cudaGetLastError();
+    return launch_pdl(k_planes_s<W>, dim3(W / 2 + 1, jobs.njobs), dim3(kFastPlaneThreads), smem, st, jobs, twy, twz,
+                      sign);
 }
 
 template <int W>
@@ -507,10 +513,11 @@ cudaError_t growth_rows_w(const float2 *tw, const GrowthJobs &jobs, const float 
         using S = RowShape<W, true>;
         const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2) + (size_t)256 * jobs.K * sizeof(float) +
                             (size_t)jobs.C * S::T * sizeof(float);
-        cudaError_t e = smem_attr((const void *)k_growth_rows_s<W>, smem);
+        auto kern = jobs.exact_bell ? k_growth_rows_s<W, true> : k_growth_rows_s<W, false>;
+        cudaError_t e = smem_attr((const void *)kern, smem);
         if (e != cudaSuccess) return e;
-        k_growth_rows_s<W><<<W * (W / S::TY), kGrowthThreads, smem, st>>>(jobs, tw, lut, A, H, U, BACK, Udbg, err);
-        return cudaGetLastError();
+        return launch_pdl(kern, dim3(W * (W / S::TY)), dim3(kGrowthThreads), smem, st, jobs, tw, lut, A, H, U, BACK,
+                          Udbg, err);
     }
 }
 

@@ -350,6 +350,8 @@ __global__ void __launch_bounds__(kTX *kTY, LENIA_TRANSPORT_MINB) k_transport_ti
         mbar_init_fence();
     }
     __syncthreads();
+    pdl_trigger();
+    pdl_wait();
     // queues channel c's MU and ARR tiles (cells plus a DD halo) into buffer c % kTBufs
     auto issue = [&](int c) {
         if (!leader) return;
@@ -506,8 +508,7 @@ cudaError_t launch_transport(const StepParams &p, const TransportBuffers &b, cud
             const size_t smem = kTBufs * 4 * (size_t)sv * sizeof(float);
             e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
-            kern<<<grid, block, smem, st>>>(p, b, tm_mu, tm_arr);
-            return cudaGetLastError();
+            return launch_pdl(kern, grid, block, smem, st, p, b, tm_mu, tm_arr);
         };
         const bool c1 = p.clip == 1.0f;
         if (p.dd == 1) {

@@ -116,6 +116,31 @@ struct TransportBuffers {
     int *err;            // bit 2 set when a tile copy did not complete in time
 };
 
+// Programmatic dependent launch between the kernels of a step (forward rows,
+// planes, growth, flow, transport): a kernel lets the next one launch once
+// all its blocks run (pdl_trigger), and waits for the previous kernel's
+// completion and memory (pdl_wait) after its constant set-up and before it
+// reads or writes any field.  Without the launch attribute both are no-ops.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // Launch wrappers (kernels_*.cu); all are asynchronous on `st`.
 cudaError_t launch_fwd_rows(const Dims &d, const FftPlan &px, const float2 *tw_x, const FwdRowJobs &jobs,
                             cudaStream_t st);
