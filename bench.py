@@ -146,8 +146,9 @@ def gpu_uuid(dev: int) -> str:
 
 # ----------------------------------------------------- algorithmic bytes
 def kernel_bytes(wl) -> dict:
-    """Algorithmic HBM bytes per launch of each kernel (each input read once,
-    each output written once; derivation in DESIGN.md)."""
+    """Algorithmic HBM bytes per launch of each kernel: each input read once,
+    each output written once (half spectra of KX x D x H complex values,
+    octant kernel spectra of KX x (D/2+1) x (H/2+1) floats, 4-byte fields)."""
     d = wl.desc
     W, H, C = d.width, d.height, d.channels
     D = W

@@ -6,7 +6,7 @@
  *   - defines the globals that main.cpp / render.cpp normally define
  *     (main.cpp:9-98, render.cpp:85), with the same defaults;
  *   - replays the 12-event step of render.cpp:357-604 serially, thread slab 0
- *     then slab 1 for every event, with the fix-ups documented in DESIGN.md:
+ *     then slab 1 for every event, with these fix-ups:
  *       * the step always starts at SIM_EVENT_FFT with T = FFT(GRID)
  *         (main.cpp:198/321 would start the first step at FFT_MT);
  *       * with BLUR_CENTRAL_DIFF off, the H -> U_S and SUM -> SUM_S copy is

@@ -9,7 +9,7 @@
  * bit, the reference's own sources compiled here (oracle/_ref/libleniaref.so,
  * 32x32x32) on every stage and mode (tests/test_oracle_pin.py), the two builds
  * sharing the LFFT engine in place of FFTW.  With ORA_FFT_HALF it follows the
- * CUDA library's half-spectrum convolution (documented in DESIGN.md) so that
+ * CUDA library's half-spectrum convolution (described below) so that
  * GPU and CPU trajectories can be compared bit for bit; every other stage is
  * the same code in both modes.
  *
@@ -215,7 +215,7 @@ static void build_blur_grid(const ora_world *w, float *grid)
 
 /* --------------------------------------------------- half-spectrum path */
 /*
- * The CUDA library's convolution ("Spectral convolution"):
+ * The CUDA library's convolution:
  *   forward  two real fields a, b packed as a + i b; x-FFT per row; split into
  *            the two half spectra kx in [0, W/2]; then per kx plane the
  *            y-FFT and z-FFT.  Layout [kx][z][y], y fastest.
