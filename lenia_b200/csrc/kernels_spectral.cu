@@ -477,6 +477,7 @@ cudaError_t launch_planes(const Dims &d, const FftPlan &py, const FftPlan &pz, c
                           const float2 *tw_z, const PlaneJobs &jobs, int sign, cudaStream_t st)
 {
     if (fast_supported(d)) return launch_planes_fast(d, tw_y, tw_z, jobs, sign, st);
+    if (fast_split_planes_supported(d)) return launch_planes_split_fast(d, tw_y, tw_z, jobs, sign, st);
     if (!plane_fits(d, py, pz)) {
         const int TZ = split_tile(d.D, d.H, py, d.H), TY = split_tile(d.H, d.D, pz, d.D);
         if (TZ == 0 || TY == 0) return cudaErrorInvalidValue;

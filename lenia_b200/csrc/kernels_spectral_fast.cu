@@ -132,6 +132,75 @@ __global__ void __launch_bounds__(kFastPlaneThreads) k_planes_s(PlaneJobs jobs, 
     }
 }
 
+// Split plane passes with compile-time plans, for cubic grids whose kx plane
+// exceeds shared memory (256): pass y transforms kSplitLines z-lines of one
+// plane (after the optional kernel product), pass z kSplitLines y-columns.
+// Each line takes the same transform as in k_planes_s, so results are
+// identical.
+constexpr int kSplitLines = 32;
+constexpr int kSplitThreads = 512;
+
+template <int W>
+__global__ void __launch_bounds__(kSplitThreads) k_plane_lines_y_s(PlaneJobs jobs, const float2 *__restrict__ tw_y,
+                                                                   int sign)
+{
+    constexpr int H = W, D = W, TZ = kSplitLines;
+    using PM = PadMat<H>;
+    extern __shared__ float2 smem[];
+    float2 *twy = smem;
+    float2 *buf = smem + H;
+    const int kx = blockIdx.x, z0 = blockIdx.y * TZ, job = blockIdx.z;
+    const long long base = ((long long)kx * D + z0) * H;
+    const float2 *src = jobs.src[job] + base;
+    float2 *dst = jobs.dst[job] + base;
+    const float *kc = jobs.kc[job];
+    for (int i = threadIdx.x; i < H; i += kSplitThreads) twy[i] = tw_y[i];
+    pdl_trigger();
+    pdl_wait();
+    constexpr int KZ = D / 2 + 1, KY = H / 2 + 1;
+    for (int e = threadIdx.x; e < TZ * H; e += kSplitThreads) {
+        const int t = e / H, y = e % H;
+        float2 v = __ldg(src + e);
+        if (kc) {
+            const int z = z0 + t;
+            const int oz = z <= D - z ? z : D - z;
+            const int oy = y <= H - y ? y : H - y;
+            const float k = __ldg(kc + (long long)kx * KZ * KY + oz * KY + oy);
+            v = make_float2(v.x * k, v.y * k);
+        }
+        buf[PM::at(t, y)] = v;
+    }
+    __syncthreads();
+    static_fft<H, TZ, false, H, kSplitThreads>(buf, twy, sign);
+    for (int e = threadIdx.x; e < TZ * H; e += kSplitThreads) dst[e] = buf[PM::at(e / H, e % H)];
+}
+
+template <int W>
+__global__ void __launch_bounds__(kSplitThreads) k_plane_lines_z_s(PlaneJobs jobs, const float2 *__restrict__ tw_z,
+                                                                   int sign)
+{
+    constexpr int H = W, D = W, TY = kSplitLines;
+    using PM = PadMat<TY>;
+    extern __shared__ float2 smem[];
+    float2 *twz = smem;
+    float2 *buf = smem + D;
+    const int kx = blockIdx.x, y0 = blockIdx.y * TY, job = blockIdx.z;
+    float2 *dst = jobs.dst[job] + (long long)kx * D * H + y0;
+    for (int i = threadIdx.x; i < D; i += kSplitThreads) twz[i] = tw_z[i];
+    pdl_trigger();
+    pdl_wait();
+    for (int e = threadIdx.x; e < D * TY; e += kSplitThreads) {
+        const int z = e / TY, t = e % TY;
+        buf[PM::at(z, t)] = dst[(long long)z * H + t];
+    }
+    __syncthreads();
+    static_fft<D, TY, true, TY, kSplitThreads>(buf, twz, sign);
+    for (int e = threadIdx.x; e < D * TY; e += kSplitThreads) {
+        const int z = e / TY, t = e % TY;
+        dst[(long long)z * H + t] = buf[PM::at(z, t)];
+    }
+}
+
 // Packed row spectrum of two kernels (or fields) for one tile: kx < W/2+1
 // from the stored half spectra, the rest by Hermitian symmetry.
 template <int W>
@@ -491,6 +560,21 @@ cudaError_t planes_w(const Dims &d, const float2 *twy, const float2 *twz, const 
 }
 
 template <int W>
+cudaError_t planes_split_w(const float2 *twy, const float2 *twz, const PlaneJobs &jobs, int sign, cudaStream_t st)
+{
+    static_assert(W % kSplitLines == 0, "split plane passes take whole line groups");
+    const size_t sy = (size_t)(W + PadMat<W>::size(kSplitLines)) * sizeof(float2);
+    const size_t sz = (size_t)(W + PadMat<kSplitLines>::size(W)) * sizeof(float2);
+    cudaError_t e = smem_attr((const void *)k_plane_lines_y_s<W>, sy);
+    if (e == cudaSuccess) e = smem_attr((const void *)k_plane_lines_z_s<W>, sz);
+    if (e != cudaSuccess) return e;
+    const dim3 grid(W / 2 + 1, W / kSplitLines, jobs.njobs);
+    e = launch_pdl(k_plane_lines_y_s<W>, grid, dim3(kSplitThreads), sy, st, jobs, twy, sign);
+    if (e != cudaSuccess) return e;
+    return launch_pdl(k_plane_lines_z_s<W>, grid, dim3(kSplitThreads), sz, st, jobs, twz, sign);
+}
+
+template <int W>
 cudaError_t growth_rows_w(const float2 *tw, const GrowthJobs &jobs, const float *lut, const float *A, float *H,
                           float *U, float *BACK, float *Udbg, int *err, cudaStream_t st)
 {
@@ -582,6 +666,15 @@ cudaError_t launch_planes_fast(const Dims &d, const float2 *tw_y, const float2 *
 #undef CASE
     default: return cudaErrorInvalidValue;
     }
+}
+
+bool fast_split_planes_supported(const Dims &d) { return d.W == d.H && d.W == 256; }
+
+cudaError_t launch_planes_split_fast(const Dims &d, const float2 *tw_y, const float2 *tw_z, const PlaneJobs &jobs,
+                                     int sign, cudaStream_t st)
+{
+    if (d.W == 256 && d.H == 256) return planes_split_w<256>(tw_y, tw_z, jobs, sign, st);
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_growth_rows_fast(const Dims &d, const float2 *tw_x_inv, const GrowthJobs &jobs,

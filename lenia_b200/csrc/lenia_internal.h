@@ -166,6 +166,10 @@ bool fast_supported(const Dims &d);
 // The size-specialised row transforms (forward rows, growth, blur) also
 // serve cubic grids whose planes use the runtime-sized plane passes.
 bool fast_rows_supported(const Dims &d);
+// Plane transforms of such grids as two line passes with compile-time plans.
+bool fast_split_planes_supported(const Dims &d);
+cudaError_t launch_planes_split_fast(const Dims &d, const float2 *tw_y, const float2 *tw_z, const PlaneJobs &jobs,
+                                     int sign, cudaStream_t st);
 cudaError_t launch_fwd_rows_fast(const Dims &d, const float2 *tw_x, const FwdRowJobs &jobs, cudaStream_t st);
 cudaError_t launch_planes_fast(const Dims &d, const float2 *tw_y, const float2 *tw_z, const PlaneJobs &jobs, int sign,
                                cudaStream_t st);
