@@ -312,7 +312,9 @@ def batch_measure(args, rank, n, stream, barrier, max_over_ranks):
     sides 24-96, 3 channels, 9 kernels, RT or advection per world), sharded
     across the ranks by cost with no exchange while stepping; beside it the
     plain loop (each world its own World, stepped one after another) over a
-    subset of this rank's worlds."""
+    subset of this rank's worlds.  The batch is tuned first
+    (lenia_batch_autotune: per grid shape the convolution mode, row tile and
+    fused or split growth that time fastest), outside the timed region."""
     import torch
     from lenia_b200 import params as P
     from lenia_b200.batch import Batch, shard_worlds, world_cost
@@ -323,6 +325,11 @@ def batch_measure(args, rank, n, stream, barrier, max_over_ranks):
     b = Batch([wl.desc for wl in sub], [wl.kernels for wl in sub], lanes=64)
     for i, wl in enumerate(sub):
         b.set_state(i, wl.A0)
+    tune = b.autotune()
+    choices = {}
+    for wl, r in zip(sub, tune):
+        choices.setdefault(str(wl.desc.width), {"conv_mode": r["conv_mode"], "growth_split": r["growth_split"],
+                                                "row_tile": r["row_tile"]})
     b.set_stream(stream.cuda_stream)
     b.step(3)
     steps = 10
@@ -361,7 +368,7 @@ def batch_measure(args, rank, n, stream, barrier, max_over_ranks):
             "cell_updates_per_s": cells / (ms / 1000.0), "graph_launches_per_step": 1,
             "gpu_launches_per_step": launches,
             "plain_world_steps_per_s_per_gpu": len(ws) / (plain_ms / 1000.0),
-            "plain_sample_worlds": len(ws)}
+            "plain_sample_worlds": len(ws), "autotune_by_side": choices}
 
 
 # ------------------------------------------------------------ GPU arm

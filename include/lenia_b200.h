@@ -217,14 +217,23 @@ lenia_status lenia_conv_macs(lenia_world *w, double *issued, double *useful);
  * stream for every convolution mode whose bit is set in `modes` (bit i = mode
  * i; LENIA_CONV_FFT and LENIA_CONV_DIRECT_BF16X3 give FP32-level results,
  * DIRECT_BF16 does not), and for the FFT path every row tile its
- * runtime-sized kernels take (grids without size-specialised kernels), then
- * keeps the fastest.  The grid state is left as it was.  Synchronous. */
+ * runtime-sized kernels take (grids without size-specialised kernels), each
+ * with the fused and the split growth (lenia_set_tuning), then keeps the
+ * fastest.  The grid state is left as it was.  Synchronous. */
 typedef struct LeniaTuneResult {
-    int conv_mode;  /* the mode kept */
-    int row_tile;   /* rows per block of the FFT row transforms (0: built-in choice) */
-    float ms[3];    /* growth-stage milliseconds per mode, best tile; -1: not measured */
+    int conv_mode;    /* the mode kept */
+    int row_tile;     /* rows per block of the FFT row transforms (0: built-in choice) */
+    float ms[3];      /* growth-stage milliseconds per mode, best variant; -1: not measured */
+    int growth_split; /* FFT growth as two passes (see lenia_set_tuning) */
 } LeniaTuneResult;
 lenia_status lenia_autotune(lenia_world *w, int modes, LeniaTuneResult *out);
+/* No counterpart in the reference.  The FFT path's tuning, as lenia_autotune
+ * sets it: row_tile = rows per block of the runtime-sized row transforms (0:
+ * the largest that fits; size-specialised grids ignore it); growth_split = 1
+ * runs the growth stage as two passes, the inverse row transforms storing u_k
+ * of every kernel (K x N floats, allocated here) and then the growth from
+ * u_k, instead of one fused pass.  Results are identical either way. */
+lenia_status lenia_set_tuning(lenia_world *w, int row_tile, int growth_split);
 
 /* No counterpart in the reference.  u_out = Re(IFFT(FFT(field) * K^))/N for
  * one field and one kernel, computed exactly as a world's growth stage computes

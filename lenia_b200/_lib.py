@@ -31,7 +31,8 @@ CONV = {"FFT": 0, "DIRECT_BF16": 1, "DIRECT_BF16X3": 2}
 
 
 class LeniaTuneResult(ctypes.Structure):
-    _fields_ = [("conv_mode", ctypes.c_int), ("row_tile", ctypes.c_int), ("ms", ctypes.c_float * 3)]
+    _fields_ = [("conv_mode", ctypes.c_int), ("row_tile", ctypes.c_int), ("ms", ctypes.c_float * 3),
+                ("growth_split", ctypes.c_int)]
 
 
 class LeniaWorldDesc(ctypes.Structure):
@@ -133,6 +134,7 @@ def load() -> ctypes.CDLL:
         "lenia_get_conv_mode": ([P], ctypes.c_int),
         "lenia_conv_macs": ([P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
         "lenia_autotune": ([P, ctypes.c_int, ctypes.POINTER(LeniaTuneResult)], ctypes.c_int),
+        "lenia_set_tuning": ([P, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "lenia_set_snapshots": ([P, ctypes.c_int], ctypes.c_int),
         "lenia_launches_per_step": ([P], ctypes.c_int),
         "lenia_set_profiling": ([P, ctypes.c_int], ctypes.c_int),

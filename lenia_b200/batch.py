@@ -114,7 +114,7 @@ class Batch:
         res = (_lib.LeniaTuneResult * n)()
         self._check(self._lib.lenia_batch_autotune(self._h, mask, res))
         names = {v: k for k, v in _lib.CONV.items()}
-        return [{"conv_mode": names[r.conv_mode], "row_tile": r.row_tile,
+        return [{"conv_mode": names[r.conv_mode], "row_tile": r.row_tile, "growth_split": bool(r.growth_split),
                  "ms": {names[i]: (float(r.ms[i]) if r.ms[i] >= 0 else None) for i in range(3)}} for r in res]
 
     def stats(self, fill_threshold: float = 0.1) -> List[np.ndarray]:

@@ -517,46 +517,80 @@ __global__ void k_count_taps(const float *__restrict__ grids, long long n, unsig
 // The growth accumulation of mt_fft_step (lenia.cpp:501-538) and the early
 // growth into BACK (lenia.cpp:542-592) from stored u_k, per cell, in kernel
 // order (the same arithmetic as the spectral path's inverse-row epilogue).
+// Four consecutive cells per thread (N is a multiple of 4), 16-byte loads
+// and stores; each cell's sums still run over the kernels in order.
+__device__ __forceinline__ float growth_value(const GrowthJobs &jobs, const float *__restrict__ lut_rows, int k,
+                                              float u, int &bad)
+{
+    const int ui = (int)(u * 255);
+    float l;
+    if (jobs.exact_bell) {
+        if (!(u == u)) bad = 1;
+        l = bell_dev(u, jobs.m[k], jobs.s[k]);
+    } else if (ui >= 0 && ui < 256) l = __ldg(lut_rows + k * 256 + ui);
+    else {
+        if (!(u == u)) bad = 1;
+        l = lut_flat_dev((long long)jobs.lut_base[k] + ui);
+    }
+    return l;
+}
+
 __global__ void k_growth_from_u(Dims d, GrowthJobs jobs, const float *__restrict__ lut_rows,
                                 const float *__restrict__ U, const float *__restrict__ A, float *__restrict__ Hout,
                                 float *__restrict__ Uout, float *__restrict__ BACK, int *err_flag)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 4;
     if (i >= d.N) return;
-    float hacc[kMaxChannels], uacc[kMaxChannels];
+    float hacc[kMaxChannels][4], uacc[kMaxChannels][4];
 #pragma unroll
-    for (int c = 0; c < kMaxChannels; c++) hacc[c] = uacc[c] = 0.0f;
+    for (int c = 0; c < kMaxChannels; c++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) hacc[c][j] = uacc[c][j] = 0.0f;
     int bad = 0;
+#pragma unroll 2
     for (int k = 0; k < jobs.K; k++) {
-        const float u = U[(long long)k * d.N + i];
+        const float4 u4 = __ldg(reinterpret_cast<const float4 *>(U + (long long)k * d.N + i));
+        const float u[4] = {u4.x, u4.y, u4.z, u4.w};
         const int c = jobs.c1[k];
-        const int ui = (int)(u * 255);
-        float l;
-        if (jobs.exact_bell) {
-            if (!(u == u)) bad = 1;
-            l = bell_dev(u, jobs.m[k], jobs.s[k]);
-        } else if (ui >= 0 && ui < 256) l = lut_rows[k * 256 + ui];
-        else {
-            if (!(u == u)) bad = 1;
-            l = lut_flat_dev((long long)jobs.lut_base[k] + ui);
-        }
+        const float h = jobs.h[k];
+        float l[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) l[j] = growth_value(jobs, lut_rows, k, u[j], bad);
 #pragma unroll
         for (int cc = 0; cc < kMaxChannels; cc++) {
             if (cc != c) continue;
-            uacc[cc] = uacc[cc] + u;
-            float g;
-            if (jobs.asymptotic[cc]) g = (l - A[(long long)cc * d.N + i]) * jobs.h[k];
-            else g = l * jobs.h[k];
-            hacc[cc] = hacc[cc] + g;
+            float a[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            if (jobs.asymptotic[cc]) {
+                const float4 a4 = __ldg(reinterpret_cast<const float4 *>(A + (long long)cc * d.N + i));
+                a[0] = a4.x;
+                a[1] = a4.y;
+                a[2] = a4.z;
+                a[3] = a4.w;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                uacc[cc][j] = uacc[cc][j] + u[j];
+                float g;
+                if (jobs.asymptotic[cc]) g = (l[j] - a[j]) * h;
+                else g = l[j] * h;
+                hacc[cc][j] = hacc[cc][j] + g;
+            }
         }
     }
 #pragma unroll
     for (int c = 0; c < kMaxChannels; c++) {
         if (c >= jobs.C) break;
         const long long o = (long long)c * d.N + i;
-        Hout[o] = hacc[c];
-        Uout[o] = uacc[c];
-        if (jobs.growth_rt) BACK[o] = early_growth(A[o], hacc[c], jobs.timestep, jobs.soft_clip[c]);
+        *reinterpret_cast<float4 *>(Hout + o) = make_float4(hacc[c][0], hacc[c][1], hacc[c][2], hacc[c][3]);
+        *reinterpret_cast<float4 *>(Uout + o) = make_float4(uacc[c][0], uacc[c][1], uacc[c][2], uacc[c][3]);
+        if (jobs.growth_rt) {
+            const float4 a4 = __ldg(reinterpret_cast<const float4 *>(A + o));
+            const float4 b = make_float4(early_growth(a4.x, hacc[c][0], jobs.timestep, jobs.soft_clip[c]),
+                                         early_growth(a4.y, hacc[c][1], jobs.timestep, jobs.soft_clip[c]),
+                                         early_growth(a4.z, hacc[c][2], jobs.timestep, jobs.soft_clip[c]),
+                                         early_growth(a4.w, hacc[c][3], jobs.timestep, jobs.soft_clip[c]));
+            *reinterpret_cast<float4 *>(BACK + o) = b;
+        }
     }
     if (bad && err_flag) atomicOr(err_flag, 1);
 }
@@ -824,7 +858,9 @@ int direct_radius(const DirectConv *dc) { return dc->R; }
 cudaError_t launch_growth_from_u(const Dims &d, const GrowthJobs &jobs, const float *lut_rows, const float *U,
                                  const float *A, float *H, float *U_SUM, float *BACK, int *err_flag, cudaStream_t st)
 {
-    k_growth_from_u<<<(unsigned)((d.N + 255) / 256), 256, 0, st>>>(d, jobs, lut_rows, U, A, H, U_SUM, BACK, err_flag);
+    const long long threads = d.N / 4;  // N is a multiple of 4 (the width is)
+    k_growth_from_u<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(d, jobs, lut_rows, U, A, H, U_SUM, BACK,
+                                                                      err_flag);
     return cudaGetLastError();
 }
 

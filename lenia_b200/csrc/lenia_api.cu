@@ -87,13 +87,14 @@ enum KernelId {
     KID_DIRECT_CONV,
     KID_GROWTH_U,
     KID_MASS,
+    KID_INV_ROWS,
     KID_MAX
 };
 const char *const kKernelNames[KID_MAX] = {"fwd_rows",          "planes_fwd",          "planes_inv",
                                            "growth_rows",       "blur_fwd_rows",       "blur_planes_fwd",
                                            "blur_planes_inv",   "blur_rows",           "flow",
                                            "transport",         "direct_pad",          "direct_conv",
-                                           "growth_u",          "mass"};
+                                           "growth_u",          "mass",                "inverse_rows"};
 
 struct ProfRec {
     int kid;
@@ -132,6 +133,7 @@ struct lenia_world {
     int lut_base_host[kMaxKernels];
     bool blur_valid = false;  // U_S / SUM_S hold a blur result
     int conv_mode = LENIA_CONV_FFT;
+    int growth_split = 0;         // FFT growth as inverse rows storing u_k, then the growth from u_k
     DirectConv *dconv = nullptr;  // plan of the direct convolution modes
     // conserve_mass: the channel totals to restore, this step's totals, partials
     double *mass_target = nullptr, *mass_total = nullptr, *mass_partial = nullptr;
@@ -563,6 +565,31 @@ lenia_status stage_growth(lenia_world *w)
         if ((e = launch_planes(d, w->py, w->px, w->tw_y_inv, w->tw_x_inv, pj, +1, st)) != cudaSuccess)
             return cuda_fail(w, e, "planes (inverse)");
         w->launches++;
+    }
+    if (w->growth_split && w->K > 0) {
+        // two passes: the inverse row transforms store u_k of every kernel
+        // (kernel pairs as in the fused pass, ten fields per launch), then
+        // the growth from u_k in kernel order
+        if (!w->U) return fail(w, LENIA_ERR_INVALID_ARG, "the split growth has no u_k buffer");
+        for (int k0 = 0; k0 < w->K; k0 += 2 * kMaxChannels + 2) {
+            BlurJobs bj;
+            memset(&bj, 0, sizeof(bj));
+            bj.nfields = std::min(w->K - k0, 2 * kMaxChannels + 2);
+            for (int i = 0; i < bj.nfields; i++) {
+                bj.spec[i] = w->S + (size_t)(k0 + i) * d.HS;
+                bj.out[i] = w->U + (size_t)(k0 + i) * d.N;
+            }
+            ProfScope ps(w, KID_INV_ROWS);
+            if ((e = launch_blur_rows(d, w->px, w->tw_x_inv, bj, st)) != cudaSuccess)
+                return cuda_fail(w, e, "inverse rows");
+            w->launches++;
+        }
+        ProfScope ps(w, KID_GROWTH_U);
+        if ((e = launch_growth_from_u(d, gj, w->lut_rows, w->U, w->A, w->H, w->U_SUM, w->BACK, w->err_flag, st)) !=
+            cudaSuccess)
+            return cuda_fail(w, e, "growth_u");
+        w->launches++;
+        return LENIA_OK;
     }
     {
         ProfScope ps(w, KID_GROWTH_ROWS);
@@ -1074,6 +1101,22 @@ lenia_status lenia_set_conv_mode(lenia_world *w, int mode)
 
 int lenia_get_conv_mode(lenia_world *w) { return w ? w->conv_mode : -1; }
 
+lenia_status lenia_set_tuning(lenia_world *w, int row_tile, int growth_split)
+{
+    if (!w) return LENIA_ERR_INVALID_ARG;
+    if (row_tile < 0 || row_tile > 32 || (row_tile & (row_tile - 1)))
+        return fail(w, LENIA_ERR_INVALID_ARG, "row tile %d is not 0 or a power of two up to 32", row_tile);
+    cudaError_t e = cudaStreamSynchronize(w->stream);
+    if (e != cudaSuccess) return cuda_fail(w, e, "set_tuning");
+    if (growth_split && !w->U && w->K > 0) {
+        w->U = dalloc<float>((size_t)w->K * w->d.N, e);
+        if (e != cudaSuccess) return cuda_fail(w, e, "u_k buffer");
+    }
+    w->d.ty = row_tile;
+    w->growth_split = growth_split != 0;
+    return LENIA_OK;
+}
+
 // Times the growth stage (the convolution and the growth table) for every
 // allowed convolution mode and, on the FFT path's runtime-sized kernels, every
 // row tile that fits; keeps the fastest.  The grid state is untouched: the
@@ -1089,7 +1132,7 @@ lenia_status lenia_autotune(lenia_world *w, int modes, LeniaTuneResult *out)
     for (int i = 0; i < 3; i++) out->ms[i] = -1.0f;
     const bool snaps = w->snapshots;
     const int launches = w->launches;
-    const int mode0 = w->conv_mode, ty0 = w->d.ty;
+    const int mode0 = w->conv_mode, ty0 = w->d.ty, split0 = w->growth_split;
     w->snapshots = false;
     cudaEvent_t a = nullptr, b = nullptr;
     cudaEventCreate(&a);
@@ -1103,7 +1146,7 @@ lenia_status lenia_autotune(lenia_world *w, int modes, LeniaTuneResult *out)
             if (row_tile(t, w->px) == ty) tiles.push_back(ty);
         }
     }
-    int best_mode = -1, best_ty = 0;
+    int best_mode = -1, best_ty = 0, best_split = 0;
     float best = 1e30f;
     lenia_status s = LENIA_OK;
     for (int mode = 0; mode < 3 && s == LENIA_OK; mode++) {
@@ -1112,9 +1155,25 @@ lenia_status lenia_autotune(lenia_world *w, int modes, LeniaTuneResult *out)
             w->conv_mode = mode;
             if (build_kernels(w) != LENIA_OK) continue;  // e.g. a radius the direct modes do not take
         }
-        const std::vector<int> cand = mode == LENIA_CONV_FFT ? tiles : std::vector<int>{ty0};
-        for (int ty : cand) {
+        // FFT: every row tile, with the fused growth and with the split one
+        std::vector<std::pair<int, int>> cand;
+        if (mode == LENIA_CONV_FFT) {
+            for (int ty : tiles)
+                for (int split = 0; split < 2; split++) cand.push_back({ty, split});
+        } else {
+            cand.push_back({ty0, 0});
+        }
+        for (const auto &c : cand) {
+            const int ty = c.first;
+            if (c.second && !w->U && w->K > 0) {
+                w->U = dalloc<float>((size_t)w->K * w->d.N, e);
+                if (e != cudaSuccess) {
+                    s = cuda_fail(w, e, "u_k buffer");
+                    break;
+                }
+            }
             w->d.ty = ty;
+            w->growth_split = c.second;
             if ((s = stage_growth(w)) != LENIA_OK) break;  // warm-up
             cudaEventRecord(a, w->stream);
             for (int r = 0; r < 3 && s == LENIA_OK; r++) s = stage_growth(w);
@@ -1132,6 +1191,7 @@ lenia_status lenia_autotune(lenia_world *w, int modes, LeniaTuneResult *out)
                 best = ms;
                 best_mode = mode;
                 best_ty = ty;
+                best_split = c.second;
             }
         }
     }
@@ -1142,6 +1202,7 @@ lenia_status lenia_autotune(lenia_world *w, int modes, LeniaTuneResult *out)
     if (s == LENIA_OK && best_mode < 0) s = fail(w, LENIA_ERR_UNSUPPORTED, "autotune: no allowed mode runs");
     const int keep_mode = s == LENIA_OK ? best_mode : mode0;
     w->d.ty = s == LENIA_OK ? best_ty : ty0;
+    w->growth_split = s == LENIA_OK ? best_split : split0;
     if (w->conv_mode != keep_mode) {
         w->conv_mode = keep_mode;
         const lenia_status s2 = build_kernels(w);
@@ -1149,6 +1210,7 @@ lenia_status lenia_autotune(lenia_world *w, int modes, LeniaTuneResult *out)
     }
     out->conv_mode = w->conv_mode;
     out->row_tile = w->d.ty;
+    out->growth_split = w->growth_split;
     return s;
 }
 
@@ -1539,6 +1601,12 @@ lenia_status lenia_batch_autotune(lenia_batch *b, int modes, LeniaTuneResult *pe
             if (done[j] || w->d.W != rep->d.W || w->d.H != rep->d.H) continue;
             done[j] = 1;
             w->d.ty = r.row_tile;
+            if (r.growth_split && !w->U && w->K > 0) {
+                cudaError_t ea = cudaSuccess;
+                w->U = dalloc<float>((size_t)w->K * w->d.N, ea);
+                if (ea != cudaSuccess) return bfail(b, LENIA_ERR_OOM, "world %zu: u_k buffer", j);
+            }
+            w->growth_split = r.growth_split;
             if (w->conv_mode != r.conv_mode) {
                 w->conv_mode = r.conv_mode;
                 if ((s = build_kernels(w)) != LENIA_OK) return bfail(b, s, "world %zu: %s", j, w->err.c_str());

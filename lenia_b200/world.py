@@ -150,8 +150,13 @@ class World:
         r = _lib.LeniaTuneResult()
         self._check(self._lib.lenia_autotune(self._h, mask, ctypes.byref(r)))
         names = {v: k for k, v in _lib.CONV.items()}
-        return {"conv_mode": names[r.conv_mode], "row_tile": r.row_tile,
+        return {"conv_mode": names[r.conv_mode], "row_tile": r.row_tile, "growth_split": bool(r.growth_split),
                 "ms": {names[i]: (float(r.ms[i]) if r.ms[i] >= 0 else None) for i in range(3)}}
+
+    def set_tuning(self, row_tile: int = 0, growth_split: bool = False) -> None:
+        """The FFT path's tuning (lenia_set_tuning): row tile of the
+        runtime-sized row transforms and the split (two-pass) growth."""
+        self._check(self._lib.lenia_set_tuning(self._h, int(row_tile), int(bool(growth_split))))
 
     def set_stream(self, stream_ptr: int) -> None:
         self._check(self._lib.lenia_set_stream(self._h, ctypes.c_void_p(stream_ptr)))

@@ -208,3 +208,23 @@ def test_autotune_keeps_state_and_picks_fastest(cuda_lib, shape):
             assert np.array_equal(a.get(n).view(np.uint32), b.get(n).view(np.uint32)), n
     with pytest.raises(Exception):
         a.autotune(modes=())
+
+
+@pytest.mark.parametrize("shape", [(32, 32), (40, 24), (96, 96)])
+def test_split_growth_is_bit_identical(cuda_lib, shape):
+    """The growth stage as two passes (inverse rows storing u_k, then the
+    growth from u_k) gives the fused pass's fields bit for bit."""
+    from lenia_b200.world import World
+    w_, h_ = shape
+    wl = P.config0(seed=16, width=w_)
+    wl.desc.height = h_
+    wl.A0 = P.seed_cube(np.random.default_rng(16), wl.desc, min(w_, h_) // 2)
+    a, b = World(wl.desc, wl.kernels), World(wl.desc, wl.kernels)
+    b.set_tuning(0, True)
+    for w in (a, b):
+        w.set_debug(True)
+        w.set_state(wl.A0.ravel())
+        w.step(3)
+        w.sync()
+    for n in ("A", "V", "GA", "SUM", "H", "U_SUM", "BACK", "U"):
+        assert np.array_equal(a.get(n).view(np.uint32), b.get(n).view(np.uint32)), n
