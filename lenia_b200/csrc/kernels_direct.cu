@@ -547,9 +547,16 @@ __global__ void k_growth_from_u(Dims d, GrowthJobs jobs, const float *__restrict
 #pragma unroll
         for (int j = 0; j < 4; j++) hacc[c][j] = uacc[c][j] = 0.0f;
     int bad = 0;
-#pragma unroll 2
+    // u of the next two kernels is loaded ahead of the current one's growth
+    const float4 *U4 = reinterpret_cast<const float4 *>(U + i);
+    const long long kstride = d.N / 4;
+    const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float4 n1 = jobs.K > 0 ? __ldg(U4) : zero4;
+    float4 n2 = jobs.K > 1 ? __ldg(U4 + kstride) : zero4;
     for (int k = 0; k < jobs.K; k++) {
-        const float4 u4 = __ldg(reinterpret_cast<const float4 *>(U + (long long)k * d.N + i));
+        const float4 u4 = n1;
+        n1 = n2;
+        if (k + 2 < jobs.K) n2 = __ldg(U4 + (long long)(k + 2) * kstride);
         const float u[4] = {u4.x, u4.y, u4.z, u4.w};
         const int c = jobs.c1[k];
         const float h = jobs.h[k];
