@@ -81,6 +81,96 @@ __global__ void __launch_bounds__(kFastRowThreads) k_fwd_rows_s(FwdRowJobs jobs,
     }
 }
 
+// A plane of work: (kx, job) in the order of the former 2D grid (kx fastest),
+// so that jobs reading one source spectrum run close together and share its
+// planes through L2.
+template <int W>
+__device__ __forceinline__ void plane_unit_prefetch(const PlaneJobs &jobs, int u)
+{
+    constexpr int KX = W / 2 + 1, KZ = W / 2 + 1, KY = W / 2 + 1;
+    const int kx = u % KX, job = u / KX;
+    prefetch_l2(jobs.src[job] + (long long)kx * W * W, (size_t)W * W * sizeof(float2));
+    if (jobs.kc[job]) prefetch_l2(jobs.kc[job] + (long long)kx * KZ * KY, (size_t)KZ * KY * sizeof(float));
+}
+
+// Stage 0 of the y transforms of a plane (rows z, length H along y) with its
+// inputs read from global memory, times the octant kernel spectrum when kp is
+// given: the butterflies of static_stage<H, 0, D, false> on the values the
+// plane load would have put in buf, without that load's shared-memory pass.
+template <int W>
+__device__ __forceinline__ void plane_first_stage(float2 *buf, const float2 *__restrict__ src,
+                                                  const float *__restrict__ kp, const float2 *tw, int sign, int tid)
+{
+    constexpr int H = W, D = W, R = plan_radix(H, 0), M = H / R, TOTAL = D * M, KY = H / 2 + 1;
+    constexpr int NB = (TOTAL + kFastPlaneThreads - 1) / kFastPlaneThreads;
+    static_assert(plan_ns(H, 0) == 1, "stage 0 takes no twiddles");
+    using PM = PadMat<H>;
+#pragma unroll
+    for (int i = 0; i < NB; i++) {
+        const int b = tid + i * kFastPlaneThreads;
+        if (TOTAL % kFastPlaneThreads == 0 || b < TOTAL) {
+            const int j = b % M, z = b / M;
+            const int oz = z <= D - z ? z : D - z;
+            float2 v[R];
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int y = j + r * M;
+                const float2 t = __ldg(src + z * H + y);
+                if (kp) {
+                    const int oy = y <= H - y ? y : H - y;
+                    const float k = __ldg(kp + oz * KY + oy);
+                    v[r] = make_float2(t.x * k, t.y * k);
+                } else {
+                    v[r] = t;
+                }
+            }
+            dft_small<R>(v, sign, tw, H);
+#pragma unroll
+            for (int r = 0; r < R; r++) buf[PM::at(z, j * R + r)] = v[r];
+        }
+    }
+    __syncthreads();
+}
+
+// Last stage of the z transforms (columns y, length D along z) with its
+// outputs written to global memory: the butterflies of
+// static_stage<D, last, H, true> without the store's shared-memory pass.
+template <int W>
+__device__ __forceinline__ void plane_last_stage(const float2 *buf, float2 *__restrict__ dst, const float2 *tw,
+                                                 int sign, int tid)
+{
+    constexpr int H = W, D = W, S = plan_count(D) - 1, R = plan_radix(D, S), NS = plan_ns(D, S), M = D / R;
+    constexpr int TOTAL = H * M, TSTEP = D / (NS * R);
+    constexpr int NB = (TOTAL + kFastPlaneThreads - 1) / kFastPlaneThreads;
+    using PM = PadMat<H>;
+    float2 v[NB][R];
+#pragma unroll
+    for (int i = 0; i < NB; i++) {
+        const int b = tid + i * kFastPlaneThreads;
+        if (TOTAL % kFastPlaneThreads == 0 || b < TOTAL) {
+            const int l = b % H, j = b / H;
+#pragma unroll
+            for (int r = 0; r < R; r++) v[i][r] = buf[PM::at(j + r * M, l)];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NB; i++) {
+        const int b = tid + i * kFastPlaneThreads;
+        if (TOTAL % kFastPlaneThreads == 0 || b < TOTAL) {
+            const int l = b % H, j = b / H;
+            const int jm = j % NS;
+            if (NS > 1 && jm != 0) {
+#pragma unroll
+                for (int r = 1; r < R; r++) v[i][r] = cmul(v[i][r], tw[r * jm * TSTEP]);
+            }
+            dft_small<R>(v[i], sign, tw, D);
+            const int base = (j / NS) * NS * R + jm;
+#pragma unroll
+            for (int r = 0; r < R; r++) dst[(base + r * NS) * H + l] = v[i][r];
+        }
+    }
+}
+
 template <int W>
 __global__ void __launch_bounds__(kFastPlaneThreads) k_planes_s(PlaneJobs jobs, const float2 *__restrict__ tw_y,
                                                                 const float2 *__restrict__ tw_z, int sign)
@@ -129,6 +219,59 @@ __global__ void __launch_bounds__(kFastPlaneThreads) k_planes_s(PlaneJobs jobs, 
         const int z = (2 * e) / H, y = (2 * e) % H;
         const float2 a = buf[PM::at(z, y)], b = buf[PM::at(z, y + 1)];
         dst[e] = make_float4(a.x, a.y, b.x, b.y);
+    }
+}
+
+
+// At 128 the plane pass runs persistent with its first and last stages on
+// global memory (k_planes_stream_s: one 1024-thread block per SM walks about
+// seven planes; 136 -> 114 us for 16 inverse planes of 128^2 x 65).  Below it
+// k_planes_s keeps one plane per block: a loop over planes costs registers
+// there (64 instead of 32 at 64 and 48, so one block per SM instead of two;
+// spills at 96 and 44), and the persistent form measured 1-4 % slower in
+// batches of worlds of 24-96 cells per side.
+template <int W>
+constexpr bool planes_persistent() { return W >= 128; }
+
+// Persistent: gridDim.x blocks walk the KX * njobs planes with stride
+// gridDim.x; once a block has read its plane it asks L2 for its next one, so
+// that load comes from L2 while this plane's transforms run.  The y
+// transforms' first stage reads global memory and the z transforms' last
+// stage writes it, so the plane crosses shared memory only between stages.
+template <int W>
+__global__ void __launch_bounds__(kFastPlaneThreads) k_planes_stream_s(PlaneJobs jobs, const float2 *__restrict__ tw_y,
+                                                                const float2 *__restrict__ tw_z, int sign)
+{
+    constexpr int H = W, D = W, KX = W / 2 + 1, KZ = D / 2 + 1, KY = H / 2 + 1;
+    static_assert(plan_count(H) >= 2, "first and last stages are separate passes");
+    extern __shared__ float2 smem[];
+    float2 *twy = smem;
+    float2 *twz = smem + H;
+    float2 *buf = smem + H + D;
+    for (int i = threadIdx.x; i < H; i += kFastPlaneThreads) twy[i] = tw_y[i];
+    for (int i = threadIdx.x; i < D; i += kFastPlaneThreads) twz[i] = tw_z[i];
+    pdl_trigger();
+    pdl_wait();
+    __syncthreads();
+    const int units = KX * jobs.njobs;
+    const int stride = gridDim.x;
+    for (int u = blockIdx.x; u < units; u += stride) {
+        const int kx = u % KX;
+        const int job = u / KX;
+        const float2 *src = jobs.src[job] + (long long)kx * D * H;
+        float2 *dst = jobs.dst[job] + (long long)kx * D * H;
+        const float *kp = jobs.kc[job] ? jobs.kc[job] + (long long)kx * KZ * KY : nullptr;
+        // the thread index read afresh per plane, so that the stages' index
+        // arithmetic is not hoisted out of the loop into registers held
+        // across it
+        int tid;
+        asm volatile("mov.u32 %0, %%tid.x;" : "=r"(tid));
+        plane_first_stage<W>(buf, src, kp, twy, sign, tid);
+        if (tid == 0 && u + stride < units) plane_unit_prefetch<W>(jobs, u + stride);
+        static_stages<H, 1, D, false, H, kFastPlaneThreads, false>(buf, twy, sign, tid);
+        static_stages<D, 0, H, true, H, kFastPlaneThreads, false, plan_count(D) - 1>(buf, twz, sign, tid);
+        plane_last_stage<W>(buf, dst, twz, sign, tid);
+        __syncthreads();  // the next plane's first stage overwrites buf
     }
 }
 
@@ -553,10 +696,30 @@ cudaError_t planes_w(const Dims &d, const float2 *twy, const float2 *twz, const 
                      cudaStream_t st)
 {
     const size_t smem = (size_t)(2 * W + PadMat<W>::size(W)) * sizeof(float2);
-    cudaError_t e = smem_attr((const void *)k_planes_s<W>, smem);
-    if (e != cudaSuccess) return e;
-    return launch_pdl(k_planes_s<W>, dim3(W / 2 + 1, jobs.njobs), dim3(kFastPlaneThreads), smem, st, jobs, twy, twz,
-                      sign);
+    if constexpr (planes_persistent<W>()) {
+        cudaError_t e = smem_attr((const void *)k_planes_stream_s<W>, smem);
+        if (e != cudaSuccess) return e;
+        // one resident wave of blocks; each walks its planes with stride grid
+        static int resident = 0;
+        if (resident == 0) {
+            int dev = 0, nsm = 0, per_sm = 0;
+            e = cudaGetDevice(&dev);
+            if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            if (e == cudaSuccess)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_planes_stream_s<W>, kFastPlaneThreads,
+                                                                  smem);
+            if (e != cudaSuccess) return e;
+            resident = nsm * (per_sm > 0 ? per_sm : 1);
+        }
+        const int units = (W / 2 + 1) * jobs.njobs;
+        return launch_pdl(k_planes_stream_s<W>, dim3(units < resident ? units : resident), dim3(kFastPlaneThreads),
+                          smem, st, jobs, twy, twz, sign);
+    } else {
+        cudaError_t e = smem_attr((const void *)k_planes_s<W>, smem);
+        if (e != cudaSuccess) return e;
+        return launch_pdl(k_planes_s<W>, dim3(W / 2 + 1, jobs.njobs), dim3(kFastPlaneThreads), smem, st, jobs, twy,
+                          twz, sign);
+    }
 }
 
 template <int W>

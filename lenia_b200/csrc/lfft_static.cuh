@@ -105,12 +105,13 @@ __device__ __forceinline__ void static_stage(float2 *buf, const float2 *tw, int 
     else __syncthreads();
 }
 
-template <int N, int S, int NLINES, bool COLS, int NC, int THREADS, bool WARP>
+// Stages S .. END-1 of the plan (END defaults to the whole plan).
+template <int N, int S, int NLINES, bool COLS, int NC, int THREADS, bool WARP, int END = plan_count(N)>
 __device__ __forceinline__ void static_stages(float2 *buf, const float2 *tw, int sign, int tid)
 {
-    if constexpr (S < plan_count(N)) {
+    if constexpr (S < END) {
         static_stage<N, S, NLINES, COLS, NC, THREADS, WARP>(buf, tw, sign, tid);
-        static_stages<N, S + 1, NLINES, COLS, NC, THREADS, WARP>(buf, tw, sign, tid);
+        static_stages<N, S + 1, NLINES, COLS, NC, THREADS, WARP, END>(buf, tw, sign, tid);
     }
 }
 
