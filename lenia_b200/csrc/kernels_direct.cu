@@ -535,67 +535,61 @@ __device__ __forceinline__ float growth_value(const GrowthJobs &jobs, const floa
     return l;
 }
 
-__global__ void k_growth_from_u(Dims d, GrowthJobs jobs, const float *__restrict__ lut_rows,
-                                const float *__restrict__ U, const float *__restrict__ A, float *__restrict__ Hout,
-                                float *__restrict__ Uout, float *__restrict__ BACK, int *err_flag)
+// The kernels grouped by target channel c1, in kernel order within a group.
+struct ChannelOrder {
+    int k[kMaxKernels];
+};
+
+// One channel at a time: its kernels' growth and u summed in kernel order
+// (the additions of the all-channel form, so the fields are identical), then
+// its H, U_SUM and BACK written; only one channel's sums are live.
+// Five blocks of 256 per SM (48 registers, no spills).
+__global__ void __launch_bounds__(256, 5)
+    k_growth_from_u(Dims d, GrowthJobs jobs, ChannelOrder ord, const float *__restrict__ lut_rows,
+                    const float *__restrict__ U, const float *__restrict__ A, float *__restrict__ Hout,
+                    float *__restrict__ Uout, float *__restrict__ BACK, int *err_flag)
 {
     const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 4;
     if (i >= d.N) return;
-    float hacc[kMaxChannels][4], uacc[kMaxChannels][4];
-#pragma unroll
-    for (int c = 0; c < kMaxChannels; c++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) hacc[c][j] = uacc[c][j] = 0.0f;
     int bad = 0;
-    // u of the next two kernels is loaded ahead of the current one's growth
+    // u of the next two kernels (in channel order) is loaded ahead of the
+    // current one's growth
     const float4 *U4 = reinterpret_cast<const float4 *>(U + i);
     const long long kstride = d.N / 4;
     const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    float4 n1 = jobs.K > 0 ? __ldg(U4) : zero4;
-    float4 n2 = jobs.K > 1 ? __ldg(U4 + kstride) : zero4;
-    for (int k = 0; k < jobs.K; k++) {
-        const float4 u4 = n1;
-        n1 = n2;
-        if (k + 2 < jobs.K) n2 = __ldg(U4 + (long long)(k + 2) * kstride);
-        const float u[4] = {u4.x, u4.y, u4.z, u4.w};
-        const int c = jobs.c1[k];
-        const float h = jobs.h[k];
-        float l[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) l[j] = growth_value(jobs, lut_rows, k, u[j], bad);
-#pragma unroll
-        for (int cc = 0; cc < kMaxChannels; cc++) {
-            if (cc != c) continue;
-            float a[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            if (jobs.asymptotic[cc]) {
-                const float4 a4 = __ldg(reinterpret_cast<const float4 *>(A + (long long)cc * d.N + i));
-                a[0] = a4.x;
-                a[1] = a4.y;
-                a[2] = a4.z;
-                a[3] = a4.w;
-            }
+    float4 n1 = jobs.K > 0 ? __ldg(U4 + (long long)ord.k[0] * kstride) : zero4;
+    float4 n2 = jobs.K > 1 ? __ldg(U4 + (long long)ord.k[1] * kstride) : zero4;
+    int pos = 0;
+    for (int c = 0; c < jobs.C; c++) {
+        const long long o = (long long)c * d.N + i;
+        const bool need_a = jobs.asymptotic[c] || jobs.growth_rt;
+        const float4 a4 = need_a ? __ldg(reinterpret_cast<const float4 *>(A + o)) : zero4;
+        float hacc[4] = {0.0f, 0.0f, 0.0f, 0.0f}, uacc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        for (; pos < jobs.K && jobs.c1[ord.k[pos]] == c; pos++) {
+            const int k = ord.k[pos];
+            const float4 u4 = n1;
+            n1 = n2;
+            if (pos + 2 < jobs.K) n2 = __ldg(U4 + (long long)ord.k[pos + 2] * kstride);
+            const float u[4] = {u4.x, u4.y, u4.z, u4.w};
+            const float a[4] = {a4.x, a4.y, a4.z, a4.w};
+            const float h = jobs.h[k];
 #pragma unroll
             for (int j = 0; j < 4; j++) {
-                uacc[cc][j] = uacc[cc][j] + u[j];
+                const float l = growth_value(jobs, lut_rows, k, u[j], bad);
+                uacc[j] = uacc[j] + u[j];
                 float g;
-                if (jobs.asymptotic[cc]) g = (l[j] - a[j]) * h;
-                else g = l[j] * h;
-                hacc[cc][j] = hacc[cc][j] + g;
+                if (jobs.asymptotic[c]) g = (l - a[j]) * h;
+                else g = l * h;
+                hacc[j] = hacc[j] + g;
             }
         }
-    }
-#pragma unroll
-    for (int c = 0; c < kMaxChannels; c++) {
-        if (c >= jobs.C) break;
-        const long long o = (long long)c * d.N + i;
-        *reinterpret_cast<float4 *>(Hout + o) = make_float4(hacc[c][0], hacc[c][1], hacc[c][2], hacc[c][3]);
-        *reinterpret_cast<float4 *>(Uout + o) = make_float4(uacc[c][0], uacc[c][1], uacc[c][2], uacc[c][3]);
+        *reinterpret_cast<float4 *>(Hout + o) = make_float4(hacc[0], hacc[1], hacc[2], hacc[3]);
+        *reinterpret_cast<float4 *>(Uout + o) = make_float4(uacc[0], uacc[1], uacc[2], uacc[3]);
         if (jobs.growth_rt) {
-            const float4 a4 = __ldg(reinterpret_cast<const float4 *>(A + o));
-            const float4 b = make_float4(early_growth(a4.x, hacc[c][0], jobs.timestep, jobs.soft_clip[c]),
-                                         early_growth(a4.y, hacc[c][1], jobs.timestep, jobs.soft_clip[c]),
-                                         early_growth(a4.z, hacc[c][2], jobs.timestep, jobs.soft_clip[c]),
-                                         early_growth(a4.w, hacc[c][3], jobs.timestep, jobs.soft_clip[c]));
+            const float4 b = make_float4(early_growth(a4.x, hacc[0], jobs.timestep, jobs.soft_clip[c]),
+                                         early_growth(a4.y, hacc[1], jobs.timestep, jobs.soft_clip[c]),
+                                         early_growth(a4.z, hacc[2], jobs.timestep, jobs.soft_clip[c]),
+                                         early_growth(a4.w, hacc[3], jobs.timestep, jobs.soft_clip[c]));
             *reinterpret_cast<float4 *>(BACK + o) = b;
         }
     }
@@ -866,7 +860,16 @@ cudaError_t launch_growth_from_u(const Dims &d, const GrowthJobs &jobs, const fl
                                  const float *A, float *H, float *U_SUM, float *BACK, int *err_flag, cudaStream_t st)
 {
     const long long threads = d.N / 4;  // N is a multiple of 4 (the width is)
-    k_growth_from_u<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(d, jobs, lut_rows, U, A, H, U_SUM, BACK,
+    // stable grouping by target channel; kernels aimed past the last channel
+    // go last and, as in the all-channel form, reach no output
+    ChannelOrder ord{};
+    int n = 0;
+    for (int c = 0; c <= kMaxChannels; c++)
+        for (int k = 0; k < jobs.K; k++) {
+            const int t = jobs.c1[k] >= 0 && jobs.c1[k] < kMaxChannels ? jobs.c1[k] : kMaxChannels;
+            if (t == c) ord.k[n++] = k;
+        }
+    k_growth_from_u<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(d, jobs, ord, lut_rows, U, A, H, U_SUM, BACK,
                                                                       err_flag);
     return cudaGetLastError();
 }
