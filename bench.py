@@ -149,7 +149,7 @@ def gpu_uuid(dev: int) -> str:
 # ----------------------------------------------------- algorithmic bytes
 def kernel_bytes(wl) -> dict:
     """Algorithmic HBM bytes per step of each kernel (one launch per step;
-    the inverse rows of the split growth run as ceil(K / 10) launches that
+    the inverse rows of the split growth run as ceil(K / 16) launches that
     together move these bytes): each input read once,
     each output written once (half spectra of KX x D x H complex values,
     octant kernel spectra of KX x (D/2+1) x (H/2+1) floats, 4-byte fields)."""

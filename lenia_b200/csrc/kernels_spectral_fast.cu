@@ -351,16 +351,14 @@ __device__ __forceinline__ void load_packed_rows_s(float2 *buf, const float2 *s0
 {
     using S = RowShape<W>;
     constexpr int H = W, D = W, TY = S::TY, KX = W / 2 + 1;
-    for (int e = threadIdx.x; e < TY * W; e += kFastRowThreads) {
-        const int ty = e % TY, kx = e / TY;
-        const int m = kx < KX ? kx : W - kx;
+    // each half-spectrum value read once, for column m and its mirror W - m
+    for (int e = threadIdx.x; e < TY * KX; e += kFastRowThreads) {
+        const int ty = e % TY, m = e / TY;
         const long long o = ((long long)m * D + z) * H + y0 + ty;
         const float2 a = __ldg(s0 + o);
         const float2 b = s1 ? __ldg(s1 + o) : make_float2(0.0f, 0.0f);
-        float2 r;
-        if (kx < KX) r = make_float2(a.x - b.y, a.y + b.x);
-        else r = make_float2(a.x + b.y, b.x - a.y);
-        buf[S::PM::at(ty, kx)] = r;
+        buf[S::PM::at(ty, m)] = make_float2(a.x - b.y, a.y + b.x);
+        if (m > 0 && W - m >= KX) buf[S::PM::at(ty, W - m)] = make_float2(a.x + b.y, b.x - a.y);
     }
 }
 
@@ -664,6 +662,8 @@ __global__ void __launch_bounds__(kFastRowThreads) k_blur_rows_s(BlurJobs jobs, 
     const long long base = ((long long)z * H + y0) * W;
     const float nf = (float)N;
     for (int i = threadIdx.x; i < W; i += kFastRowThreads) tw[i] = tw_x[i];
+    pdl_trigger();
+    pdl_wait();
     const int f0 = 2 * pair, f1 = 2 * pair + 1 < jobs.nfields ? 2 * pair + 1 : -1;
     load_packed_rows_s<W>(buf, jobs.spec[f0], f1 >= 0 ? jobs.spec[f1] : nullptr, z, y0);
     __syncthreads();
@@ -775,8 +775,8 @@ cudaError_t blur_rows_w(const float2 *tw, const BlurJobs &jobs, cudaStream_t st)
     const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2);
     cudaError_t e = smem_attr((const void *)k_blur_rows_s<W>, smem);
     if (e != cudaSuccess) return e;
-    k_blur_rows_s<W><<<dim3(W * (W / S::TY), (jobs.nfields + 1) / 2), kFastRowThreads, smem, st>>>(jobs, tw);
-    return cudaGetLastError();
+    return launch_pdl(k_blur_rows_s<W>, dim3(W * (W / S::TY), (jobs.nfields + 1) / 2), dim3(kFastRowThreads), smem,
+                      st, jobs, tw);
 }
 
 }  // namespace

@@ -568,13 +568,13 @@ lenia_status stage_growth(lenia_world *w)
     }
     if (w->growth_split && w->K > 0) {
         // two passes: the inverse row transforms store u_k of every kernel
-        // (kernel pairs as in the fused pass, ten fields per launch), then
-        // the growth from u_k in kernel order
+        // (kernel pairs as in the fused pass, sixteen fields per launch),
+        // then the growth from u_k
         if (!w->U) return fail(w, LENIA_ERR_INVALID_ARG, "the split growth has no u_k buffer");
-        for (int k0 = 0; k0 < w->K; k0 += 2 * kMaxChannels + 2) {
+        for (int k0 = 0; k0 < w->K; k0 += kBlurFields) {
             BlurJobs bj;
             memset(&bj, 0, sizeof(bj));
-            bj.nfields = std::min(w->K - k0, 2 * kMaxChannels + 2);
+            bj.nfields = std::min(w->K - k0, kBlurFields);
             for (int i = 0; i < bj.nfields; i++) {
                 bj.spec[i] = w->S + (size_t)(k0 + i) * d.HS;
                 bj.out[i] = w->U + (size_t)(k0 + i) * d.N;

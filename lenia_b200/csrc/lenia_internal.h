@@ -64,10 +64,11 @@ struct GrowthJobs {
     float s[kMaxKernels];
 };
 
-// Inverse row pass storing field/N (the blur).
+// Inverse row pass storing field/N (the blur, and u_k of the split growth).
+constexpr int kBlurFields = 16;  // >= 2 * kMaxChannels + 2, the blur's fields
 struct BlurJobs {
-    const float2 *spec[2 * kMaxChannels + 2];
-    float *out[2 * kMaxChannels + 2];
+    const float2 *spec[kBlurFields];
+    float *out[kBlurFields];
     int nfields;
 };
 
