@@ -55,6 +55,10 @@ def parse():
                     help="worlds of the batched measurement (config 3 mix; 0 = skip)")
     ap.add_argument("--conv-width", type=int, default=256,
                     help="side of the convolution-mode measurement (config 2 workload; 0 = skip)")
+    ap.add_argument("--growth", default="auto", choices=["auto", "split", "fused"],
+                    help="growth form of the headline world: chosen by the autotuner (default), or fixed "
+                         "(FFT convolution, the size's default row tile), e.g. for a profiler run in which "
+                         "the autotuner's timings would not be the real ones")
     return ap.parse_args()
 
 
@@ -401,7 +405,11 @@ def run_ours(args):
     C, N = wl.desc.channels, wl.desc.cells
     # the world as its user runs it: tuned by the library's autotuner
     # (convolution mode, row tile, fused or split growth), outside the timing
-    tuning = w.autotune()
+    if args.growth == "auto":
+        tuning = w.autotune()
+    else:
+        w.set_tuning(0, args.growth == "split")
+        tuning = {"conv_mode": "FFT", "row_tile": 0, "growth_split": args.growth == "split", "ms": None}
 
     def barrier():
         torch.cuda.synchronize()

@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p
                 if (!((gvalid >> lz) & 1u)) {
                     alpha = 0.0f;
                 } else {
-                    float pg = gv / ta;
+                    float pg = p.inv_theta_a != 0.0f ? gv * p.inv_theta_a : gv / ta;
                     pg = pg * pg;
                     alpha = smin(smax(pg, 0.0f), 1.0f);
                 }

@@ -351,14 +351,28 @@ __device__ __forceinline__ void load_packed_rows_s(float2 *buf, const float2 *s0
 {
     using S = RowShape<W>;
     constexpr int H = W, D = W, TY = S::TY, KX = W / 2 + 1;
-    // each half-spectrum value read once, for column m and its mirror W - m
-    for (int e = threadIdx.x; e < TY * KX; e += kFastRowThreads) {
-        const int ty = e % TY, m = e / TY;
-        const long long o = ((long long)m * D + z) * H + y0 + ty;
-        const float2 a = __ldg(s0 + o);
-        const float2 b = s1 ? __ldg(s1 + o) : make_float2(0.0f, 0.0f);
-        buf[S::PM::at(ty, m)] = make_float2(a.x - b.y, a.y + b.x);
-        if (m > 0 && W - m >= KX) buf[S::PM::at(ty, W - m)] = make_float2(a.x + b.y, b.x - a.y);
+    constexpr int NE = TY * KX, NI = (NE + kFastRowThreads - 1) / kFastRowThreads;
+    // each half-spectrum value read once, for column m and its mirror W - m;
+    // all of a thread's loads are issued before its shared-memory stores
+    float2 a[NI], b[NI];
+#pragma unroll
+    for (int i = 0; i < NI; i++) {
+        const int e = threadIdx.x + i * kFastRowThreads;
+        if (NE % kFastRowThreads == 0 || e < NE) {
+            const int ty = e % TY, m = e / TY;
+            const long long o = ((long long)m * D + z) * H + y0 + ty;
+            a[i] = __ldg(s0 + o);
+            b[i] = s1 ? __ldg(s1 + o) : make_float2(0.0f, 0.0f);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NI; i++) {
+        const int e = threadIdx.x + i * kFastRowThreads;
+        if (NE % kFastRowThreads == 0 || e < NE) {
+            const int ty = e % TY, m = e / TY;
+            buf[S::PM::at(ty, m)] = make_float2(a[i].x - b[i].y, a[i].y + b[i].x);
+            if (m > 0 && W - m >= KX) buf[S::PM::at(ty, W - m)] = make_float2(a[i].x + b[i].y, b[i].x - a[i].y);
+        }
     }
 }
 

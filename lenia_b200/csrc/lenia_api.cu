@@ -246,6 +246,11 @@ StepParams step_params(const lenia_world *w)
     p.C = w->C;
     p.timestep = s.timestep;
     p.theta_a = s.theta_a;
+    {
+        int ex = 0;
+        const float m = frexpf(s.theta_a, &ex);  // theta_a = m * 2^ex, m in [0.5, 1)
+        p.inv_theta_a = (m == 0.5f && ex - 1 >= -126 && ex - 1 <= 126) ? ldexpf(1.0f, 1 - ex) : 0.0f;
+    }
     p.s_norm = s.s_norm;
     p.gta = s.gta;
     p.sta = s.sta;

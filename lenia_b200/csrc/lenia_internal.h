@@ -86,6 +86,10 @@ struct StepParams {
     int rt_all_channels, alpha_index_fix;
     // derived (computed on the host in the reference's float expressions)
     float ma, sn, clip, si, gws, ghs;
+    // 1 / theta_a when theta_a is a power of two whose reciprocal is a
+    // normal float (then a / theta_a == a * inv_theta_a for every a: both are
+    // the correctly rounded value of the same real number), else 0
+    float inv_theta_a;
 };
 
 struct FlowBuffers {
