@@ -63,11 +63,21 @@ __global__ void __launch_bounds__(kFastRowThreads) k_fwd_rows_s(FwdRowJobs jobs,
     pdl_trigger();
     pdl_wait();
     const long long base = ((long long)z * H + y0) * W;
-    for (int e = threadIdx.x; e < TY * W; e += kFastRowThreads) {
-        const int ty = e / W, x = e % W;
-        const float a = __ldg(fa + base + e);
-        const float b = fb ? __ldg(fb + base + e) : 0.0f;
-        buf[S::PM::at(ty, x)] = make_float2(a, b);
+    // all of a thread's loads are issued before its shared-memory stores
+    constexpr int NE = TY * W, NI = (NE + kFastRowThreads - 1) / kFastRowThreads;
+    float va[NI], vb[NI];
+#pragma unroll
+    for (int i = 0; i < NI; i++) {
+        const int e = threadIdx.x + i * kFastRowThreads;
+        if (NE % kFastRowThreads == 0 || e < NE) {
+            va[i] = __ldg(fa + base + e);
+            vb[i] = fb ? __ldg(fb + base + e) : 0.0f;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NI; i++) {
+        const int e = threadIdx.x + i * kFastRowThreads;
+        if (NE % kFastRowThreads == 0 || e < NE) buf[S::PM::at(e / W, e % W)] = make_float2(va[i], vb[i]);
     }
     __syncthreads();
     static_fft<W, TY, false, W, kFastRowThreads>(buf, tw, -1);
