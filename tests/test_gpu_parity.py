@@ -168,14 +168,18 @@ def test_trajectory_bit_exact_cfg0(cuda_lib, oracle_built):
     gpu.sync()
 
 
-def test_config1_step_bit_exact(cuda_lib, oracle_built):
-    """One full step of the 128^3 x 4 channel, 16-kernel configuration."""
+@pytest.mark.parametrize("growth_split", [False, True], ids=["fused_growth", "split_growth"])
+def test_config1_step_bit_exact(cuda_lib, oracle_built, growth_split):
+    """One full step of the 128^3 x 4 channel, 16-kernel configuration, with
+    the growth stage as one fused pass or as inverse rows storing u_k followed
+    by the growth from u_k (the form the autotuner picks for this world)."""
     from lenia_b200.world import World
     wl = P.config1(seed=1)
     p, ks = as_oracle(wl)
     ora = RestateOracle(p, ks, fft_mode="half")
     ora.set_state(A=wl.A0.ravel())
     gpu = World(wl.desc, wl.kernels)
+    gpu.set_tuning(0, growth_split)
     gpu.set_state(wl.A0.ravel())
     ora.step(1)
     gpu.step(1)
