@@ -557,8 +557,10 @@ __global__ void __launch_bounds__(256, 5)
     const float4 *U4 = reinterpret_cast<const float4 *>(U + i);
     const long long kstride = d.N / 4;
     const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    float4 n1 = jobs.K > 0 ? __ldg(U4 + (long long)ord.k[0] * kstride) : zero4;
-    float4 n2 = jobs.K > 1 ? __ldg(U4 + (long long)ord.k[1] * kstride) : zero4;
+    // u_k is read once (evict-first loads), U_SUM is not read in the step
+    // (evict-first store): L2 keeps H and BACK for the flow and transport
+    float4 n1 = jobs.K > 0 ? __ldcs(U4 + (long long)ord.k[0] * kstride) : zero4;
+    float4 n2 = jobs.K > 1 ? __ldcs(U4 + (long long)ord.k[1] * kstride) : zero4;
     int pos = 0;
     for (int c = 0; c < jobs.C; c++) {
         const long long o = (long long)c * d.N + i;
@@ -569,7 +571,7 @@ __global__ void __launch_bounds__(256, 5)
             const int k = ord.k[pos];
             const float4 u4 = n1;
             n1 = n2;
-            if (pos + 2 < jobs.K) n2 = __ldg(U4 + (long long)ord.k[pos + 2] * kstride);
+            if (pos + 2 < jobs.K) n2 = __ldcs(U4 + (long long)ord.k[pos + 2] * kstride);
             const float u[4] = {u4.x, u4.y, u4.z, u4.w};
             const float a[4] = {a4.x, a4.y, a4.z, a4.w};
             const float h = jobs.h[k];
@@ -584,7 +586,7 @@ __global__ void __launch_bounds__(256, 5)
             }
         }
         *reinterpret_cast<float4 *>(Hout + o) = make_float4(hacc[0], hacc[1], hacc[2], hacc[3]);
-        *reinterpret_cast<float4 *>(Uout + o) = make_float4(uacc[0], uacc[1], uacc[2], uacc[3]);
+        __stcs(reinterpret_cast<float4 *>(Uout + o), make_float4(uacc[0], uacc[1], uacc[2], uacc[3]));
         if (jobs.growth_rt) {
             const float4 b = make_float4(early_growth(a4.x, hacc[0], jobs.timestep, jobs.soft_clip[c]),
                                          early_growth(a4.y, hacc[1], jobs.timestep, jobs.soft_clip[c]),
