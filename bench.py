@@ -11,11 +11,14 @@ world is tuned by the library's autotuner before the timed region
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-With N > 1 (torchrun, one process per GPU) every rank advances its own world
-(the single-world step does not shard: replicas, weak scaling); `value` is the
-sum over ranks divided by the slowest rank's time.  `--impl reference` times
-the CPU restatement of the reference's step (oracle, complex-to-complex
-spectral structure like the reference's FFTW path) on the host cores.
+With N > 1 every rank (one process per GPU) advances its own world (the
+single-world step does not shard: replicas, weak scaling); `value` is the sum
+over ranks divided by the slowest rank's time.  Started as one process with
+`--gpus N`, the script launches its N ranks itself under torch.distributed.run
+(lenia_b200/launch.py); started by torchrun, it is one of them.
+`--impl reference` times the reference's CPU step (rank 0 only) on the host
+cores: every asked step if the run fits its time budget, else the steps that
+fit, and the line reports the steps it timed.
 
 Beside the headline: `config1_schedule` (500 steps with every channel
 meshed every 10 steps, each mesh with its host synchronisation); and, with
@@ -291,26 +294,57 @@ def cpu_threads() -> int:
         return os.cpu_count() or 1
 
 
+# The reference arm's whole run (warm-up and timed steps) is kept to about
+# this many seconds of host time: a step that would take it past the budget
+# is not started, and the line reports the steps actually timed.
+REF_BUDGET_S = 180.0
+
+
 def run_reference(args):
+    """The reference's CPU step on the host cores, on this arm's workload:
+    rank 0 alone runs (the other ranks of a multi-rank launch exit at once).
+    Warm-up steps (at most `--warmup`, within a quarter of the budget), then
+    up to `--steps` timed steps, each one full step of the world; the steps
+    actually timed are the line's `steps`."""
     rank = int(os.environ.get("RANK", "0"))
-    n = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    n = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
+    from oracle.oracle import RestateOracle
     wl = workload(args)
-    steps = max(1, min(args.steps, 8))
-    warm = 1 if args.warmup > 0 else 0
-    rate, dt = cpu_port_rate(wl, steps, warm)
-    ms = dt * 1000.0 / steps
+    p, ks = wl.desc.as_dict(), [k.as_dict() for k in wl.kernels]
+    o = RestateOracle(p, ks, fft_mode="c2c")
+    o.set_state(A=wl.A0.ravel())
+    t_start = time.perf_counter()
+    warm = 0
+    for _ in range(args.warmup):
+        t0 = time.perf_counter()
+        o.step(1)
+        warm += 1
+        if (time.perf_counter() - t_start) + (time.perf_counter() - t0) > REF_BUDGET_S / 4:
+            break
+    timed, dt = 0, 0.0
+    while timed < args.steps:
+        t0 = time.perf_counter()
+        o.step(1)
+        dt += time.perf_counter() - t0
+        timed += 1
+        if timed < args.steps and (time.perf_counter() - t_start) + dt / timed > REF_BUDGET_S:
+            break
+    cells = wl.desc.cells * wl.desc.channels
+    rate = cells * timed / dt
     cores = cpu_threads()
+    sample = (f"{timed} timed steps (+{warm} warm-up) of the whole world on the host"
+              + ("" if timed == args.steps else f" (of {args.steps} asked: the run is kept within "
+                 f"{REF_BUDGET_S:.0f} s)")
+              + f"; C restatement of the reference step with its complex-to-complex FFT structure, "
+                f"OpenMP over {cores} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": n,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "steps": timed, "warmup": warm, "ms_per_step": dt * 1000.0 / timed, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
         "config": config_dict(args, wl, 1),
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{steps} timed steps (+{warm} warm-up) of the same world on the host, "
-                                   f"C restatement of the reference step with its complex-to-complex FFT "
-                                   f"structure, OpenMP over {cores} threads"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -390,6 +424,8 @@ def run_ours(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     n = int(os.environ.get("WORLD_SIZE", "1"))
+    if local >= torch.cuda.device_count():
+        raise SystemExit(f"rank {rank}: local rank {local} but {torch.cuda.device_count()} visible GPU(s)")
     torch.cuda.set_device(local)
     dist = None
     if n > 1:
@@ -576,6 +612,12 @@ def run_ours(args):
 
 def main():
     args = parse()
+    # `--gpus N` started as one process: launch N ranks (one per GPU) of this
+    # script under torch.distributed.run and return their exit code
+    from lenia_b200.launch import maybe_spawn
+    rc = maybe_spawn(os.path.abspath(__file__), sys.argv[1:], args.gpus)
+    if rc is not None:
+        return rc
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -185,6 +185,15 @@ lenia_status lenia_set_stream(lenia_world *w, void *stream);
 lenia_status lenia_sync(lenia_world *w);
 /* 1: keep the intermediate fields marked (debug) in LeniaField. */
 lenia_status lenia_set_debug(lenia_world *w, int on);
+/* No counterpart in the reference (it has no error handling, lenia.h:73).
+ * Poll limit of the first wait of each block of the flow and transport
+ * kernels for a tile copy into shared memory.  When a block's wait runs out,
+ * the block records LENIA_ERR_TIMEOUT (reported by the next lenia_sync),
+ * waits with the library's fixed long limit for the copies it still has in
+ * flight, and returns without writing its tile's outputs; the world stays
+ * usable.  polls < 0 restores the default (2^24 polls); 0 makes every such
+ * wait give up at once (for tests of the timeout path). */
+lenia_status lenia_set_wait_limit(lenia_world *w, long long polls);
 /* 1: keep the mesh snapshots H_RB / U_SUM_RB / RBB every step. */
 lenia_status lenia_set_snapshots(lenia_world *w, int on);
 
@@ -238,12 +247,14 @@ lenia_status lenia_set_tuning(lenia_world *w, int row_tile, int growth_split);
 /* No counterpart in the reference.  u_out = Re(IFFT(FFT(field) * K^))/N for
  * one field and one kernel, computed exactly as a world's growth stage computes
  * u for that kernel, for callers that cannot allocate device memory: every
- * intermediate buffer lives in one fixed __device__ array (about 3.4 MB per
- * GPU, held until exit), so this call allocates nothing.  field and u_out are
+ * intermediate buffer lives in one fixed __device__ array (4,439,040 bytes,
+ * about 4.4 MB per GPU, held until exit), so this call allocates nothing.  field and u_out are
  * device pointers of width*height*width floats; grids up to 64^3 are accepted
  * (larger ones return LENIA_ERR_INVALID_ARG).  Calls share that array, so
  * calls that overlap on the GPU race; the first call on a device looks up the
- * array's address (cudaGetSymbolAddress) with that device current. */
+ * array's address (cudaGetSymbolAddress) with that device current and keeps
+ * it, so after a cudaDeviceReset of that device the kept address is stale and
+ * this call must not be used on it again in the same process. */
 lenia_status lenia_convolve_noalloc(int width, int height, const float *field, const LeniaKernelParams *kernel,
                                     float *u_out, void *stream);
 

@@ -18,6 +18,13 @@ MAX_CHANNELS = 4
 MAX_BETA = 12
 
 LENIA_OK = 0
+LENIA_ERR_INVALID_ARG = 1
+LENIA_ERR_OOM = 2
+LENIA_ERR_CUDA = 3
+LENIA_ERR_TIMEOUT = 4
+LENIA_ERR_NONFINITE = 5
+LENIA_ERR_NO_DEVICE = 6
+LENIA_ERR_UNSUPPORTED = 7
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA", 4: "TIMEOUT", 5: "NONFINITE",
                 6: "NO_DEVICE", 7: "UNSUPPORTED"}
 
@@ -130,6 +137,7 @@ def load() -> ctypes.CDLL:
         "lenia_set_stream": ([P, ctypes.c_void_p], ctypes.c_int),
         "lenia_sync": ([P], ctypes.c_int),
         "lenia_set_debug": ([P, ctypes.c_int], ctypes.c_int),
+        "lenia_set_wait_limit": ([P, ctypes.c_longlong], ctypes.c_int),
         "lenia_set_conv_mode": ([P, ctypes.c_int], ctypes.c_int),
         "lenia_get_conv_mode": ([P], ctypes.c_int),
         "lenia_conv_macs": ([P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], ctypes.c_int),

@@ -2,9 +2,13 @@
 
 Every float operation of the step is kept separate (-fmad=false): the kernels
 reproduce the reference's rounding order and the project's FFT contract.
+Each translation unit compiles to its own object (in parallel; an object is
+rebuilt when its source or any header is newer), then one link makes the
+shared library.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import glob
 import os
 import shutil
@@ -15,6 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liblenia_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+OBJ_DIR = os.path.join(HERE, "_build")
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",
@@ -22,7 +27,6 @@ NVCC_FLAGS = [
     "-fmad=false", "-prec-div=true", "-prec-sqrt=true",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
     "--expt-relaxed-constexpr",
-    "-shared",
 ]
 
 
@@ -37,20 +41,48 @@ def sources() -> list[str]:
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
 
-def _stale() -> bool:
-    if not os.path.exists(LIB):
-        return True
-    t = os.path.getmtime(LIB)
-    deps = sources() + glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
+def headers() -> list[str]:
+    return glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
         glob.glob(os.path.join(INCLUDE, "*.h"))
+
+
+def _obj(src: str) -> str:
+    return os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + ".o")
+
+
+def _newer(path: str, deps: list[str]) -> bool:
+    if not os.path.exists(path):
+        return True
+    t = os.path.getmtime(path)
     return any(os.path.getmtime(p) > t for p in deps)
+
+
+def _stale() -> bool:
+    return _newer(LIB, sources() + headers())
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    hdrs = headers()
+    todo = [s for s in sources() if force or _newer(_obj(s), [s] + hdrs)]
+
+    def compile_one(src: str) -> None:
+        tmp = _obj(src) + ".tmp"
+        cmd = [nvcc(), *NVCC_FLAGS, "-I", INCLUDE, "-c", src, "-o", tmp]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, _obj(src))
+
+    workers = max(1, min(len(todo), os.cpu_count() or 1))
+    with concurrent.futures.ThreadPoolExecutor(workers) as ex:
+        for f in [ex.submit(compile_one, s) for s in todo]:
+            f.result()
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *NVCC_FLAGS, "-I", INCLUDE, "-o", tmp, *sources()]
+    cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp,
+           *[_obj(s) for s in sources()]]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

@@ -4,7 +4,8 @@
 //
 // Layout (little-endian):
 //   "LENIACKP"                      8-byte magic
-//   u32 version (1), u32 flags (0)
+//   u32 version (1), u32 flags (bit 0: a mass-target record follows the
+//     fields)
 //   u32 n_desc_words, then the LeniaWorldDesc fields in declaration order as
 //     32-bit words (ints as i32, floats as IEEE-754 binary32)
 //   u32 n_kernels, then per kernel radius, beta_size, b[12], r_a, m, s, h,
@@ -12,6 +13,10 @@
 //   u64 step (caller's counter)
 //   u32 n_fields, then per field: u32 LeniaField id, u64 float count, the
 //     floats (A, V, GA, SUM: everything that carries over between steps)
+//   flags bit 0: u32 n_channels, then per channel the conserve_mass target
+//     total as an IEEE-754 binary64 (the totals every later step restores;
+//     without them a resumed world would take its restored grid's rounded
+//     totals as the target and drift from the run that never stopped)
 //   u32 CRC-32 (IEEE 802.3 polynomial, reflected) of every byte before it
 #include <stdint.h>
 #include <stdio.h>
@@ -25,6 +30,7 @@ namespace {
 
 constexpr char kMagic[8] = {'L', 'E', 'N', 'I', 'A', 'C', 'K', 'P'};
 constexpr uint32_t kVersion = 1;
+constexpr uint32_t kFlagMassTarget = 1;
 
 uint32_t crc32_update(uint32_t crc, const unsigned char *p, size_t n)
 {
@@ -57,6 +63,12 @@ struct Writer {
         uint32_t v;
         memcpy(&v, &f, 4);
         u32(v);
+    }
+    void f64(double f)
+    {
+        uint64_t v;
+        memcpy(&v, &f, 8);
+        u64(v);
     }
 };
 
@@ -93,6 +105,13 @@ struct Reader {
         memcpy(&f, &v, 4);
         return f;
     }
+    double f64()
+    {
+        const uint64_t v = u64();
+        double f;
+        memcpy(&f, &v, 8);
+        return f;
+    }
 };
 
 // LeniaWorldDesc as 32-bit words in declaration order (every member is a
@@ -110,10 +129,12 @@ lenia_status lenia_save(lenia_world *w, const LeniaWorldDesc *desc, const LeniaK
                         unsigned long long step, const char *path)
 {
     if (!w || !desc || (n_kernels > 0 && !kernels) || n_kernels < 0 || !path) return LENIA_ERR_INVALID_ARG;
+    double target[LENIA_MAX_CHANNELS];
+    const int n_target = desc->conserve_mass ? lenia::mass_target_get(w, target, LENIA_MAX_CHANNELS) : 0;
     Writer wr;
     wr.bytes(kMagic, 8);
     wr.u32(kVersion);
-    wr.u32(0);
+    wr.u32(n_target > 0 ? kFlagMassTarget : 0);
     wr.u32(kDescWords);
     uint32_t words[kDescWords];
     memcpy(words, desc, sizeof(LeniaWorldDesc));
@@ -142,6 +163,10 @@ lenia_status lenia_save(lenia_world *w, const LeniaWorldDesc *desc, const LeniaK
         wr.u32((uint32_t)field);
         wr.u64(n);
         for (size_t i = 0; i < n; i++) wr.f32(tmp[i]);
+    }
+    if (n_target > 0) {
+        wr.u32((uint32_t)n_target);
+        for (int c = 0; c < n_target; c++) wr.f64(target[c]);
     }
     wr.u32(crc32_update(0, wr.buf.data(), wr.buf.size()));
     FILE *f = fopen(path, "wb");
@@ -176,7 +201,7 @@ lenia_status lenia_load(const char *path, lenia_world **out, unsigned long long 
     Reader rd(buf);
     rd.pos = 8;
     const uint32_t version = rd.u32();
-    rd.u32();  // flags
+    const uint32_t flags = rd.u32();
     if (version != kVersion) {
         fprintf(stderr, "lenia_load: %s has version %u, this library reads %u\n", path, version, kVersion);
         return LENIA_ERR_UNSUPPORTED;
@@ -221,6 +246,16 @@ lenia_status lenia_load(const char *path, lenia_world **out, unsigned long long 
         tmp.resize(n);
         for (uint64_t j = 0; j < n; j++) tmp[j] = rd.f32();
         s = lenia_set_field(w, field, tmp.data(), n, 0);
+    }
+    // the saved conserve_mass totals replace the ones lenia_set_field just
+    // recorded from the restored grid
+    if (s == LENIA_OK && (flags & kFlagMassTarget)) {
+        const uint32_t nc = rd.u32();
+        double target[LENIA_MAX_CHANNELS];
+        if (!rd.ok || nc > LENIA_MAX_CHANNELS || nc != (uint32_t)desc.channels) s = LENIA_ERR_INVALID_ARG;
+        for (uint32_t c = 0; c < nc && s == LENIA_OK; c++) target[c] = rd.f64();
+        if (s == LENIA_OK && !rd.ok) s = LENIA_ERR_INVALID_ARG;
+        if (s == LENIA_OK && desc.conserve_mass) s = lenia::mass_target_set(w, target, (int)nc);
     }
     if (s != LENIA_OK) {
         lenia_destroy(w);

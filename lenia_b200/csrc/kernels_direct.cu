@@ -587,6 +587,8 @@ __global__ void __launch_bounds__(256, 5)
         }
         *reinterpret_cast<float4 *>(Hout + o) = make_float4(hacc[0], hacc[1], hacc[2], hacc[3]);
         __stcs(reinterpret_cast<float4 *>(Uout + o), make_float4(uacc[0], uacc[1], uacc[2], uacc[3]));
+        // a NaN u indexes the table at 0 ((int)NaN is 0 here): test the sums
+        if (!(isfinite(uacc[0]) && isfinite(uacc[1]) && isfinite(uacc[2]) && isfinite(uacc[3]))) bad = 1;
         if (jobs.growth_rt) {
             const float4 b = make_float4(early_growth(a4.x, hacc[0], jobs.timestep, jobs.soft_clip[c]),
                                          early_growth(a4.y, hacc[1], jobs.timestep, jobs.soft_clip[c]),

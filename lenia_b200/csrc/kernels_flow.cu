@@ -39,7 +39,6 @@ constexpr int kFlowZ = LENIA_FLOW_Z;      // output cells per thread along z
 constexpr int kTX = 40, kTY = kFY + 2;    // staged tile: x from x0 - 4 (TMA x must be 16-byte aligned), y halo
 constexpr int kTZ = kFlowZ + 2;
 constexpr int kTile = kTX * kTY * kTZ;    // floats per staged field
-constexpr unsigned kTmaWaitLimit = 1u << 24;
 
 __device__ __forceinline__ float smax(float a, float b) { return a > b ? a : b; }
 __device__ __forceinline__ float smin(float a, float b) { return a < b ? a : b; }
@@ -187,17 +186,23 @@ __global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p
         else tma_load_4d(tiles[buf], &tm_h, x0 - 4, y0 - 1, z0 - 1, f - 1, &bars[buf]);
     };
 
-    // Waits for field f's tile, patches its faces and decides the path; returns
-    // whether the literal (non-finite) path is needed.
-    auto land = [&](int f) -> bool {
+    // Waits for field f's tile, patches its faces and decides the path:
+    // 1 when the literal (non-finite) path is needed, 0 otherwise, -1 when the
+    // wait ran out (block-wide): the timeout is recorded and the copies in
+    // flight (fields f and f + 1) are drained; the block then returns.
+    auto land = [&](int f) -> int {
         float *tile = tiles[f & 1];
-        if (!mbar_wait(&bars[f & 1], (unsigned)(f >> 1) & 1u, kTmaWaitLimit) && b.err) atomicOr(b.err, 2);
-        __syncthreads();
+        if (!block_wait(&bars[f & 1], (unsigned)(f >> 1) & 1u, p.wait_polls)) {
+            mbar_wait(&bars[f & 1], (unsigned)(f >> 1) & 1u, kDrainPolls);
+            if (f + 1 <= C) mbar_wait(&bars[(f + 1) & 1], (unsigned)((f + 1) >> 1) & 1u, kDrainPolls);
+            if (leader && b.err) atomicOr(b.err, 2);
+            return -1;
+        }
         if (patch) {
             patch_faces(tile, f == 0 ? b.SUM : b.H + (f - 1) * N, d, p.sobel_border, x0, y0, z0);
             __syncthreads();
         }
-        return sobel && tile_unsafe(tile);
+        return (sobel && tile_unsafe(tile)) ? 1 : 0;
     };
     // the column: tile index of (x, y, z0 + lz) is col + (lz + 1) * plane
     const int col = (tx + 4) + (ty + 1) * kTX;
@@ -231,7 +236,9 @@ __global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p
     issue(0);
     issue(1);
     {
-        const bool literal = land(0);
+        const int landed = land(0);
+        if (landed < 0) return;
+        const bool literal = landed != 0;
         float win[3][9];
 #pragma unroll
         for (int lz = 0; lz < kFlowZ; lz++) {
@@ -278,7 +285,9 @@ __global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p
                 gvalid |= (valid ? 1u : 0u) << lz;
             }
         }
-        const bool literal = land(f);
+        const int landed = land(f);
+        if (landed < 0) return;
+        const bool literal = landed != 0;
         float win[3][9];
 #pragma unroll
         for (int lz = 0; lz < kFlowZ; lz++) {

@@ -250,7 +250,9 @@ __global__ void __launch_bounds__(kRowThreads) k_growth_rows(Dims d, FftPlan px,
             const long long o = (long long)c * d.N + base + e;
             const float hv = hacc[c * T + e];
             Hout[o] = hv;
-            Uout[o] = uacc[c * T + e];
+            const float us = uacc[c * T + e];
+            Uout[o] = us;
+            if (!isfinite(us)) bad = 1;  // a NaN u indexes the table at 0: test the sum
             if (jobs.growth_rt) BACK[o] = early_growth(A[o], hv, jobs.timestep, jobs.soft_clip[c]);
         }
     }

@@ -513,7 +513,9 @@ __global__ void __launch_bounds__(kGrowthThreads) k_growth_rows_s(GrowthJobs job
             const long long o = (long long)c * N + base + e;
             const float hv = hacc[i][c];
             Hout[o] = hv;
-            Uout[o] = uacc[c * T + e];
+            const float us = uacc[c * T + e];
+            Uout[o] = us;
+            if (!isfinite(us)) bad = 1;  // a NaN u indexes the table at 0: test the sum
             if (jobs.growth_rt) BACK[o] = early_growth(__ldg(A + o), hv, jobs.timestep, jobs.soft_clip[c]);
         }
     }
@@ -664,7 +666,9 @@ __global__ void __launch_bounds__(kGwWarps * 32) k_growth_warp(GrowthJobs jobs, 
             const long long o = (long long)c * N + base + e;
             const float hv = hacc[i][c];
             Hout[o] = hv;
-            Uout[o] = uacc[c * T + e];
+            const float us = uacc[c * T + e];
+            Uout[o] = us;
+            if (!isfinite(us)) bad = 1;  // a NaN u indexes the table at 0: test the sum
             if (jobs.growth_rt) BACK[o] = early_growth(__ldg(A + o), hv, jobs.timestep, jobs.soft_clip[c]);
         }
     }

@@ -276,7 +276,6 @@ __global__ void __launch_bounds__(256) k_transport(StepParams p, TransportBuffer
 // float operations, so the result is bit-identical.
 constexpr int kTX = 32, kTY = 8, kTZ = 4;
 constexpr int kTBoxX = 40;  // staged x range x0 - 4 .. x0 + 35 (TMA x must be 16-byte aligned)
-constexpr unsigned kTmaWaitLimitT = 1u << 24;
 
 // min(max(si - |d|, 0), clip).  With clip == 1 the clamp is a saturating
 // add: identical for every input (NaN and negative values give +0 either
@@ -409,8 +408,14 @@ __global__ void __launch_bounds__(kTX *kTY, LENIA_TRANSPORT_MINB) k_transport_ti
     for (int c = 0; c < crt; c++) {
         if (kTBufs == 2 && c + 1 < crt) issue(c + 1);
         float *buf = tiles + (c % kTBufs) * 4 * SV;
-        if (!mbar_wait(&bars[c % kTBufs], (unsigned)(c / kTBufs) & 1u, kTmaWaitLimitT) && b.err) atomicOr(b.err, 2);
-        __syncthreads();
+        if (!block_wait(&bars[c % kTBufs], (unsigned)(c / kTBufs) & 1u, p.wait_polls)) {
+            // the wait ran out: record it, drain the copies in flight, return
+            mbar_wait(&bars[c % kTBufs], (unsigned)(c / kTBufs) & 1u, kDrainPolls);
+            if (kTBufs == 2 && c + 1 < crt)
+                mbar_wait(&bars[(c + 1) % kTBufs], (unsigned)((c + 1) / kTBufs) & 1u, kDrainPolls);
+            if (leader && b.err) atomicOr(b.err, 2);
+            return;
+        }
         if (patch) {
             patch_faces(c, buf);
             __syncthreads();

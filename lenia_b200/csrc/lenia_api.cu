@@ -129,6 +129,7 @@ struct lenia_world {
     LeniaKernelParams *kp_dev = nullptr;
     float2 *tw_x_fwd = nullptr, *tw_x_inv = nullptr, *tw_y_fwd = nullptr, *tw_y_inv = nullptr;
     int *err_flag = nullptr;
+    unsigned wait_polls = kDefaultTileWaitPolls;  // first wait for a tile copy (lenia_set_wait_limit)
     double *stats_trig = nullptr, *stats_partial = nullptr;  // lenia_world_stats buffers (allocated on first use)
     int lut_base_host[kMaxKernels];
     bool blur_valid = false;  // U_S / SUM_S hold a blur result
@@ -290,6 +291,7 @@ StepParams step_params(const lenia_world *w)
     p.si = 0.5f + sigma;
     p.gws = (float)w->d.W - sigma;
     p.ghs = (float)w->d.H - sigma;
+    p.wait_polls = w->wait_polls;
     return p;
 }
 
@@ -465,6 +467,34 @@ lenia_status mass_record_target(lenia_world *w)
     if (e != cudaSuccess) return cuda_fail(w, e, "mass totals");
     return LENIA_OK;
 }
+
+}  // namespace
+
+// The conserve_mass target totals (one double per channel) of a world that
+// has recorded them: copied out (synchronises the world's stream; returns the
+// channel count, 0 when none are recorded) or replaced (stream-ordered).
+int lenia::mass_target_get(lenia_world *w, double *host, int n)
+{
+    if (!w || !w->mass_target || n < w->C) return 0;
+    if (cudaStreamSynchronize(w->stream) != cudaSuccess) return 0;
+    if (cudaMemcpy(host, w->mass_target, sizeof(double) * w->C, cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+    return w->C;
+}
+
+lenia_status lenia::mass_target_set(lenia_world *w, const double *host, int n)
+{
+    if (!w || n != w->C) return LENIA_ERR_INVALID_ARG;
+    if (!w->mass_target) {
+        const lenia_status s = mass_record_target(w);
+        if (s != LENIA_OK) return s;
+    }
+    const cudaError_t e =
+        cudaMemcpyAsync(w->mass_target, host, sizeof(double) * n, cudaMemcpyHostToDevice, w->stream);
+    if (e == cudaSuccess) return cudaStreamSynchronize(w->stream) == cudaSuccess ? LENIA_OK : LENIA_ERR_CUDA;
+    return cuda_fail(w, e, "mass target");
+}
+
+namespace {
 
 // Per-step buffers a batch lane lends to its worlds (they run one after
 // another on the lane's stream).
@@ -1069,8 +1099,16 @@ lenia_status lenia_sync(lenia_world *w)
             return fail(w, LENIA_ERR_TIMEOUT,
                         "a bounded wait ran out (a tile copy of the flow or transport stage, or the direct "
                         "convolution's copy/MMA/drain pipeline)");
-        return fail(w, LENIA_ERR_NONFINITE, "non-finite u met in the growth table lookup");
+        return fail(w, LENIA_ERR_NONFINITE, "non-finite u (NaN or infinite) met in the growth stage");
     }
+    return LENIA_OK;
+}
+
+lenia_status lenia_set_wait_limit(lenia_world *w, long long polls)
+{
+    if (!w) return LENIA_ERR_INVALID_ARG;
+    if (polls > 0xffffffffLL) return fail(w, LENIA_ERR_INVALID_ARG, "wait limit %lld above 2^32 - 1", polls);
+    w->wait_polls = polls < 0 ? kDefaultTileWaitPolls : (unsigned)polls;
     return LENIA_OK;
 }
 

@@ -17,6 +17,8 @@ constexpr int kPlaneThreads = 512;  // block size of the plane transform
 constexpr int kPlaneCap = 32;       // values per thread in the plane transform
 constexpr int kRowThreads = 256;    // block size of the row transforms
 constexpr int kRowCap = 32;
+// default poll limit of the first wait for a tile copy (StepParams::wait_polls)
+constexpr unsigned kDefaultTileWaitPolls = 1u << 24;
 
 enum { kBorderTorus = 0, kBorderWall = 1, kBorderNone = 2 };
 enum { kGrowthNone = 0, kGrowthRT = 1, kGrowthTransposition = 2 };
@@ -90,6 +92,10 @@ struct StepParams {
     // normal float (then a / theta_a == a * inv_theta_a for every a: both are
     // the correctly rounded value of the same real number), else 0
     float inv_theta_a;
+    // poll limit of the first wait for each tile copy in the flow and
+    // transport kernels (lenia_set_wait_limit); a block whose wait runs out
+    // records the timeout, drains its copies in flight and returns
+    unsigned wait_polls;
 };
 
 struct FlowBuffers {
@@ -195,6 +201,12 @@ cudaError_t launch_mass_totals(const float *A, const Dims &d, int C, double *par
                                cudaStream_t st);
 cudaError_t launch_mass_scale(float *A, const Dims &d, int C, const double *target, const double *total,
                               cudaStream_t st);
+
+// The conserve_mass target totals of a world (lenia_api.cu): copied out to
+// `host` (n >= channels; returns the channel count, 0 when none are
+// recorded) or replaced from it (n == channels).
+int mass_target_get(lenia_world *w, double *host, int n);
+lenia_status mass_target_set(lenia_world *w, const double *host, int n);
 
 // Host FFT plans and twiddle tables (lenia_api.cu).
 int fft_factor(int n, int *radix);

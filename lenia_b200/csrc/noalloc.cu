@@ -6,8 +6,8 @@
 // is allowed to use, or a host loop that must not take the implicit
 // device-wide synchronisation an allocation can cause.  For them this entry
 // point keeps every intermediate buffer in one file-scope __device__ array of
-// fixed size (kNoAllocBytes below, about 3.4 MB), which each GPU that loads
-// the library holds until the process exits.  The caller passes the input
+// fixed size (kNoAllocBytes below: 4,439,040 bytes, about 4.4 MB), which each
+// GPU that loads the library holds until the process exits.  The caller passes the input
 // field and the output buffer, both in device memory.
 //
 // The array is shared by every call and keeps the last call's contents; every
@@ -17,10 +17,15 @@
 //
 // The first call on a device looks up the array's device address with
 // cudaGetSymbolAddress while that device is current (the host-side name of a
-// __device__ array is not a device address).
+// __device__ array is not a device address) and keeps it for later calls on
+// that device.  cudaDeviceReset unloads the library's device code, so the
+// kept address is stale afterwards: do not call this entry point on a device
+// after resetting it in the same process.
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
+
+#include <atomic>
 
 #include "lenia_internal.h"
 
@@ -44,12 +49,15 @@ constexpr size_t kOffTw = kOffKc + align256(kNoAllocMaxKH * 4);                 
 constexpr size_t kOffParams = kOffTw + align256(4 * kNoAllocMaxDim * 8);          // kernel parameters
 constexpr size_t kOffSum = kOffParams + align256(sizeof(LeniaKernelParams));     // normalisation sum
 constexpr size_t kNoAllocBytes = kOffSum + 256;
+static_assert(kNoAllocBytes == 4439040, "the documented size of the scratch array (about 4.4 MB)");
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 // Device address of g_noalloc_scratch per device, filled on first use.
+// Atomic: host threads may make their first calls on a device at the same
+// time (each stores the same address).
 constexpr int kMaxDevices = 64;
-unsigned char *g_scratch_ptr[kMaxDevices] = {};
+std::atomic<unsigned char *> g_scratch_ptr[kMaxDevices] = {};
 
 struct TwiddleArgs {
     float2 xf[kNoAllocMaxDim], xi[kNoAllocMaxDim], yf[kNoAllocMaxDim], yi[kNoAllocMaxDim];
@@ -110,16 +118,17 @@ extern "C" lenia_status lenia_convolve_noalloc(int width, int height, const floa
         return LENIA_ERR_INVALID_ARG;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return LENIA_ERR_NO_DEVICE;
-    if (!g_scratch_ptr[dev]) {
+    unsigned char *scratch = g_scratch_ptr[dev].load(std::memory_order_acquire);
+    if (!scratch) {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) {
             fprintf(stderr, "lenia_convolve_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
             return LENIA_ERR_CUDA;
         }
-        g_scratch_ptr[dev] = (unsigned char *)p;
+        scratch = (unsigned char *)p;
+        g_scratch_ptr[dev].store(scratch, std::memory_order_release);
     }
-    unsigned char *scratch = g_scratch_ptr[dev];
     cudaStream_t st = (cudaStream_t)stream;
 
     Dims d;

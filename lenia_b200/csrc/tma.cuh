@@ -52,6 +52,20 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsign
     return false;
 }
 
+// Poll limit of the wait for a copy still in flight after a block gave up on
+// it (the block must not exit while the copy can still write its shared
+// memory).
+constexpr unsigned kDrainPolls = 1u << 24;
+
+// Block-wide wait for a tile copy: each thread polls at most `polls` times;
+// true when every thread saw the phase complete.  Called by every thread of
+// the block; the result is the same in all of them.
+__device__ __forceinline__ bool block_wait(uint64_t *bar, unsigned parity, unsigned polls)
+{
+    const bool ok = mbar_wait(bar, parity, polls);
+    return __syncthreads_or(!ok) == 0;
+}
+
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar)
 {
     asm volatile(

@@ -122,6 +122,12 @@ class World:
     def set_debug(self, on: bool = True) -> None:
         self._check(self._lib.lenia_set_debug(self._h, int(on)))
 
+    def set_wait_limit(self, polls: int = -1) -> None:
+        """Poll limit of the first wait for each tile copy in the flow and
+        transport kernels (-1: the default; 0: every wait gives up at once, so
+        the next sync raises a timeout error)."""
+        self._check(self._lib.lenia_set_wait_limit(self._h, int(polls)))
+
     def set_snapshots(self, on: bool = True) -> None:
         self._check(self._lib.lenia_set_snapshots(self._h, int(on)))
 
@@ -258,4 +264,17 @@ def read_checkpoint_header(path: str) -> dict:
         off += 8
         kernels.append(KernelParams(radius=radius, beta_size=beta, b=b[:beta], r_a=r_a, m=m, s=s, h=h, c0=c0, c1=c1))
     (step,) = struct.unpack_from("<Q", data, off)
-    return {"version": version, "desc": desc, "kernels": kernels, "step": step}
+    off += 8
+    (nf,) = struct.unpack_from("<I", data, off)
+    off += 4
+    fields = []
+    for _ in range(nf):
+        fid, n = struct.unpack_from("<IQ", data, off)
+        off += 12 + 4 * n
+        fields.append(fid)
+    mass_target = None
+    if _flags & 1:
+        (nc,) = struct.unpack_from("<I", data, off)
+        mass_target = list(struct.unpack_from(f"<{nc}d", data, off + 4))
+    return {"version": version, "flags": _flags, "desc": desc, "kernels": kernels, "step": step,
+            "fields": fields, "mass_target": mass_target}

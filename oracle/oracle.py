@@ -95,14 +95,23 @@ def make_kernels(ks) -> ctypes.Array:
 
 _build_lock = threading.Lock()
 
+# Directory of the reference's sources (the project's checkout); tests read
+# marching_cubes.h and lenia.cpp there, and oracle/Makefile builds from it.
+REF_DIR = os.environ.get("LENIA_REFERENCE", "/root/reference")
+
+
+def ref_path(name: str) -> str:
+    """Path of a file of the reference's sources."""
+    return os.path.join(REF_DIR, name)
+
 
 def build(force: bool = False) -> None:
     """Builds both oracles with oracle/Makefile (the reference build only when
     the reference sources are present on this machine)."""
     with _build_lock:
         if force or not os.path.exists(ORACLE_LIB) or (
-                os.path.isdir("/root/reference") and not os.path.exists(REF_LIB)):
-            subprocess.run(["make", "-s", "-C", HERE], check=True)
+                os.path.isdir(REF_DIR) and not os.path.exists(REF_LIB)):
+            subprocess.run(["make", "-s", "-C", HERE, f"REF={REF_DIR}"], check=True)
 
 
 def _fp(a: np.ndarray):

@@ -63,3 +63,28 @@ def test_corrupt_and_foreign_versions_are_rejected(tmp_path):
     with pytest.raises(LeniaError) as e:
         World.load(str(tmp_path / "v2.ckp"))
     assert e.value.status == 7
+
+
+def test_conserve_mass_resume_matches_continuous_run(tmp_path):
+    """A conserve_mass world saved mid-run and resumed steps bit for bit like
+    the world that never stopped: the checkpoint carries the target totals
+    (recorded at the last write of the grid), not the restored grid's."""
+    from lenia_b200.world import World, read_checkpoint_header
+    wl = P.config0(seed=5)
+    wl.desc.conserve_mass = True
+    w = World(wl.desc, wl.kernels)
+    w.set_state(wl.A0.ravel())
+    target = w.get("A").reshape(wl.desc.channels, -1).astype(np.float64).sum(axis=1)
+    w.step(4)
+    path = str(tmp_path / "m.ckp")
+    w.save(path, step=4)
+    hdr = read_checkpoint_header(path)
+    assert hdr["flags"] & 1 and hdr["mass_target"] is not None
+    assert np.allclose(hdr["mass_target"], target, rtol=1e-12, atol=0)
+    w2, _ = World.load(path)
+    w.step(6)
+    w2.step(6)
+    for name in ("A", "V", "GA", "SUM"):
+        assert np.array_equal(w.get(name).view(np.uint32), w2.get(name).view(np.uint32)), name
+    w.close()
+    w2.close()

@@ -17,7 +17,7 @@ from lenia_b200 import params as P
 
 import lenia_cases as LC
 
-REF_MC = "/root/reference/marching_cubes.h"
+REF_MC = O.ref_path("marching_cubes.h")
 needs_ref = pytest.mark.skipif(not os.path.exists(REF_MC), reason="reference sources absent")
 
 

@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 from lenia_cases import VARIANTS, as_oracle, diff_report, four_channels, two_channel_div_flow, variant
-from oracle.oracle import EVENTS, REF_LIB, RefOracle, RestateOracle
+from oracle.oracle import EVENTS, REF_DIR, REF_LIB, RefOracle, RestateOracle
 
 FIELDS = ["A", "V", "GA", "SUM", "H", "U_SUM", "BACK", "NA", "NU", "PREALPHA", "ALPHA", "F", "MU", "TT",
           "U_S", "SUM_S", "U", "H_RB", "U_SUM_RB", "RBB"]
@@ -23,7 +23,7 @@ SUM_TRANSIENT = {"SOBEL_TWO", "F", "MU", "TB"}
 SUM_S_LIVE = {"BLUR", "TSB", "SOBEL_ONE"}
 
 pytestmark = pytest.mark.skipif(
-    not (os.path.isdir("/root/reference") or os.path.exists(REF_LIB)),
+    not (os.path.isdir(REF_DIR) or os.path.exists(REF_LIB)),
     reason="reference sources / build unavailable")
 
 

@@ -11,7 +11,7 @@ from lenia_b200.sampling import MsvcRand, generate_random
 
 import lenia_cases as LC
 
-needs_ref = pytest.mark.skipif(not os.path.exists("/root/reference/lenia.cpp"), reason="reference sources absent")
+needs_ref = pytest.mark.skipif(not os.path.exists(O.ref_path("lenia.cpp")), reason="reference sources absent")
 
 
 def test_msvc_rand_known_sequence():

@@ -29,13 +29,13 @@ def world_u(desc, kernel, A):
     return u
 
 
-@pytest.mark.parametrize("width,seed", [(32, 3), (64, 4), (48, 5)])
-def test_noalloc_matches_growth_stage(cuda_lib, width, seed):
+@pytest.mark.parametrize("width,height,seed", [(32, 32, 3), (64, 64, 4), (48, 48, 5), (48, 32, 6), (40, 64, 7)])
+def test_noalloc_matches_growth_stage(cuda_lib, width, height, seed):
     import torch
     rng = np.random.default_rng(seed)
-    desc = P.WorldDesc(width=width, height=width, channels=1, asymptotic=(False,) * 4)
-    kernel = P.sample_kernels(rng, 1, radius=width // 4)[0]
-    A = P.seed_cube(rng, desc, width // 2).ravel()
+    desc = P.WorldDesc(width=width, height=height, channels=1, asymptotic=(False,) * 4)
+    kernel = P.sample_kernels(rng, 1, radius=min(width, height) // 4)[0]
+    A = P.seed_cube(rng, desc, min(width, height) // 2).ravel()
     want = world_u(desc, kernel, A)
     field = torch.from_numpy(A).cuda()
     out = torch.empty_like(field)
@@ -43,7 +43,7 @@ def test_noalloc_matches_growth_stage(cuda_lib, width, seed):
     stream = torch.cuda.current_stream().cuda_stream
     for call in range(2):
         out.fill_(float("nan"))
-        st = cuda_lib.lenia_convolve_noalloc(width, width, ctypes.c_void_p(field.data_ptr()), ck,
+        st = cuda_lib.lenia_convolve_noalloc(width, height, ctypes.c_void_p(field.data_ptr()), ck,
                                              ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(stream))
         torch.cuda.synchronize()
         assert st == 0, f"call {call}: status {st}"
