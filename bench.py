@@ -287,6 +287,42 @@ def cpu_port_rate(wl, steps: int, warmup: int):
     return cells * steps / dt, dt
 
 
+def reference_lib(wl):
+    """The reference build whose compile-time grid fits this workload (its own
+    lenia.cpp / reintegration.cpp / transposition.cpp / mesh.cpp, unmodified),
+    or None."""
+    from oracle import oracle as O
+    w, h, k = wl.desc.width, wl.desc.height, len(wl.kernels)
+    for path, side, kmax in ((O.REF_LIB, 32, 12), (O.REF_LIB_128, 128, 16)):
+        if w == side and h == side and k <= kmax and os.path.exists(path):
+            return path
+    return None
+
+
+def cpu_reference_rate(wl, path: str, steps: int, warmup: int, budget_s: float):
+    """The reference's own step (the build at `path`) on the host, each event's
+    two slabs on two threads at once as its two sim threads run them.  Up to
+    `steps` timed steps, fewer when the next would pass `budget_s` seconds;
+    returns (cell-updates/s, seconds timed, steps timed)."""
+    from oracle.oracle import RefOracle
+    p, ks = wl.desc.as_dict(), [k.as_dict() for k in wl.kernels]
+    o = RefOracle(p, ks, lib=path)
+    o.set_state(A=wl.A0.ravel())
+    if warmup:
+        o.step(warmup, slab_threads=True)
+    t_start = time.perf_counter()
+    timed, dt = 0, 0.0
+    while timed < steps:
+        t0 = time.perf_counter()
+        o.step(1, slab_threads=True)
+        dt += time.perf_counter() - t0
+        timed += 1
+        if timed < steps and (time.perf_counter() - t_start) + dt / timed > budget_s:
+            break
+    cells = wl.desc.cells * wl.desc.channels
+    return cells * timed / dt, dt, timed
+
+
 def cpu_threads() -> int:
     try:
         return len(os.sched_getaffinity(0))
@@ -312,6 +348,9 @@ def run_reference(args):
         return 0
     from oracle.oracle import RestateOracle
     wl = workload(args)
+    path = reference_lib(wl)
+    if path is not None:
+        return run_reference_build(args, wl, path, n)
     p, ks = wl.desc.as_dict(), [k.as_dict() for k in wl.kernels]
     o = RestateOracle(p, ks, fft_mode="c2c")
     o.set_state(A=wl.A0.ravel())
@@ -345,6 +384,32 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
         "config": config_dict(args, wl, 1),
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_build(args, wl, path: str, n: int):
+    """The reference arm on the reference's own code: its lenia.cpp,
+    reintegration.cpp, transposition.cpp and mesh.cpp built at this
+    workload's size (oracle/_ref), stepped with its two sim threads (each
+    event's two slabs at once, as render.cpp:357-604 runs them).  The
+    reference uses two host threads by design (SIM_THREADS, render.h:14); the
+    project's FFT stands in for FFTW, which is absent."""
+    warm = min(args.warmup, 1)
+    rate, dt, timed = cpu_reference_rate(wl, path, args.steps, warm, REF_BUDGET_S)
+    sample = (f"{timed} timed steps (+{warm} warm-up) of the whole world on the host"
+              + ("" if timed == args.steps else f" (of {args.steps} asked: the run is kept within "
+                 f"{REF_BUDGET_S:.0f} s)")
+              + "; the reference's own step code built at this size, two sim threads (slab 0 and "
+                "slab 1 of every event at once); a project FFT stands in for FFTW")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": n,
+        "steps": timed, "warmup": warm, "ms_per_step": dt * 1000.0 / timed, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": config_dict(args, wl, 1),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 2, "kind": "reference", "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -564,6 +629,31 @@ def run_ours(args):
     smesh.close()
     ws.close()
 
+    # config 1's other reintegration: the same world with advection (semi-
+    # Lagrangian pull of every channel, reintegration.cpp:1112-1260), tuned
+    # and timed the same way
+    adv = None
+    if args.mode == "rt":
+        from lenia_b200 import params as P
+        wa = P.config1(seed=1 + rank, width=args.width, mode=P.MODE_ADV)
+        wv = World(wa.desc, wa.kernels)
+        wv.set_stream(stream.cuda_stream)
+        wv.set_state(wa.A0.ravel())
+        atune = wv.autotune() if args.growth == "auto" else None
+        wv.step(args.warmup)
+        adv_steps = max(10, min(args.steps, 200))
+        barrier()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        wv.step(adv_steps)
+        a1.record(stream)
+        barrier()
+        adv_ms = max_over_ranks(a0.elapsed_time(a1))
+        wv.close()
+        adv = {"workload": config_dict(argparse.Namespace(mode="adv"), wa, n)["workload"],
+               "value": n * N * C * adv_steps / (adv_ms / 1000.0), "unit": UNIT, "steps": adv_steps,
+               "ms_per_step": adv_ms / adv_steps, "tuning": atune}
+
     batched = batch_measure(args, rank, n, stream, barrier, max_over_ranks) if args.batch_worlds > 0 else None
     conv = conv_measure(args) if (args.conv_width > 0 and n == 1) else None
 
@@ -591,16 +681,28 @@ def run_ours(args):
             "mesh": mesh,
             "config1_schedule": schedule,
         }
+        if adv is not None:
+            line["advection"] = adv
         if batched is not None:
             line["batched"] = batched
         if conv is not None:
             line["conv_modes"] = conv
         if n == 1 and not args.no_cpu_baseline:
             rate, dt = cpu_port_rate(wl, 2, 1)
-            line["cpu_baseline"] = {
-                "value": rate, "unit": UNIT, "cores": cpu_threads(), "kind": "port",
-                "sample": "2 timed steps (+1 warm-up) of the same world, C restatement of the reference step "
-                          "(complex-to-complex FFT structure), OpenMP over all host threads"}
+            port = {"value": rate, "unit": UNIT, "cores": cpu_threads(), "kind": "port",
+                    "sample": "2 timed steps (+1 warm-up) of the same world, C restatement of the reference "
+                              "step (complex-to-complex FFT structure), OpenMP over all host threads"}
+            path = reference_lib(wl)
+            if path is not None:
+                rrate, rdt, rsteps = cpu_reference_rate(wl, path, 3, 1, 30.0)
+                line["cpu_baseline"] = {
+                    "value": rrate, "unit": UNIT, "cores": 2, "kind": "reference",
+                    "sample": f"{rsteps} timed steps (+1 warm-up) of the same world: the reference's own step "
+                              "code built at this size, its two sim threads (slabs of every event at once); a "
+                              "project FFT stands in for FFTW"}
+                line["cpu_port"] = port
+            else:
+                line["cpu_baseline"] = port
     w.close()
     if dist is not None:
         dist.barrier()

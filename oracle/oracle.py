@@ -6,7 +6,10 @@ ctypes front end for the two CPU oracles built by oracle/Makefile:
 * `RefOracle`     — oracle/_ref/libleniaref.so: the reference's own
   lenia.cpp, reintegration.cpp, transposition.cpp and mesh.cpp compiled
   unmodified against shim headers, stepped by oracle/refshim/driver.cpp.
-  Its grid is render.h's compile-time 32x32x32 with at most 12 kernels.
+  Its grid is render.h's compile-time 32x32x32 with at most 12 kernels;
+  `RefOracle(..., lib=REF_LIB_128)` is the same code built at 128^3 with at
+  most 16 kernels (one instance per library per process: its state is
+  the library's globals).
 * `RestateOracle` — oracle/_build/liblenia_oracle.so: the C restatement
   (oracle/restate/lenia_oracle.c), any size.  fft_mode "c2c" follows the
   reference's complex-to-complex spectral structure; "half" follows the CUDA
@@ -26,6 +29,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libleniaref.so")
+# The same sources built at the headline size (128^3, at most 16 kernels).
+REF_LIB_128 = os.path.join(HERE, "_ref", "w128", "libleniaref.so")
+# The 32^3 build linked with a float64 FFT stand-in (refshim/fftw_shim64.c):
+# a second valid build of the reference, for its sensitivity to FFT rounding.
+REF_LIB_FFT64 = os.path.join(HERE, "_ref", "fft64", "libleniaref.so")
 ORACLE_LIB = os.path.join(HERE, "_build", "liblenia_oracle.so")
 
 FIELDS = {
@@ -137,29 +145,32 @@ class _Base:
 
 
 class RefOracle(_Base):
-    """The reference's own code at its compile-time size (32^3, <=12 kernels)."""
+    """The reference's own code at its compile-time size (32^3, <=12 kernels,
+    or 128^3, <=16 kernels with lib=REF_LIB_128)."""
 
-    _lib = None
+    _libs: dict = {}
 
     @classmethod
-    def lib(cls):
-        if cls._lib is None:
+    def lib(cls, path: str = REF_LIB):
+        if path not in cls._libs:
             build()
-            if not os.path.exists(REF_LIB):
-                raise FileNotFoundError(REF_LIB)
-            lib = ctypes.CDLL(REF_LIB)
+            if not os.path.exists(path):
+                raise FileNotFoundError(path)
+            lib = ctypes.CDLL(path)
             lib.ref_init()
             lib.ref_get_field.restype = ctypes.c_int
             lib.ref_bell_lut.restype = ctypes.c_float
             lib.ref_bell_lut.argtypes = [ctypes.c_int] * 3
-            cls._lib = lib
-        return cls._lib
+            cls._libs[path] = lib
+        return cls._libs[path]
 
-    def __init__(self, params: dict, kernels: list):
-        lib = self.lib()
+    def __init__(self, params: dict, kernels: list, lib: str = REF_LIB):
+        self._path = lib
+        lib = self.lib(lib)
         self.W = lib.ref_grid_width()
         self.Hh = lib.ref_grid_height()
-        assert params["width"] == self.W and params["height"] == self.Hh, "reference build is 32^3"
+        assert params["width"] == self.W and params["height"] == self.Hh, \
+            f"this reference build is {self.W}x{self.Hh}x{self.W}"
         self.C = params["channels"]
         self.K = len(kernels)
         self.N = self.W * self.Hh * self.W
@@ -170,36 +181,41 @@ class RefOracle(_Base):
 
     def set_state(self, A=None, V=None, GA=None, SUM=None):
         A, V, GA, SUM = (_opt(x) for x in (A, V, GA, SUM))
-        self.lib().ref_set_state(*(None if x is None else _fp(x) for x in (A, V, GA, SUM)))
+        self.lib(self._path).ref_set_state(*(None if x is None else _fp(x) for x in (A, V, GA, SUM)))
 
     def run_event(self, ev):
-        self.lib().ref_run_event(EVENTS.index(ev) if isinstance(ev, str) else int(ev))
+        self.lib(self._path).ref_run_event(EVENTS.index(ev) if isinstance(ev, str) else int(ev))
 
-    def step(self, n=1):
-        self.lib().ref_step(int(n))
+    def step(self, n=1, slab_threads: bool = False):
+        """n steps; slab_threads runs each event's two slabs on two threads
+        at once (the reference's two sim threads), else one after the other."""
+        if slab_threads:
+            self.lib(self._path).ref_step_slabs(int(n))
+        else:
+            self.lib(self._path).ref_step(int(n))
 
     def get(self, name: str) -> np.ndarray:
         out = np.zeros(self.field_size(name), dtype=np.float32)
-        self.lib().ref_get_field(FIELDS[name], _fp(out))
+        self.lib(self._path).ref_get_field(FIELDS[name], _fp(out))
         return out
 
     def kernel_grid(self, k):
         out = np.zeros(self.N, dtype=np.float32)
-        self.lib().ref_get_kernel_grid(int(k), _fp(out))
+        self.lib(self._path).ref_get_kernel_grid(int(k), _fp(out))
         return out
 
     def blur_grid(self):
         out = np.zeros(self.N, dtype=np.float32)
-        self.lib().ref_get_blur_grid(_fp(out))
+        self.lib(self._path).ref_get_blur_grid(_fp(out))
         return out
 
     def kernel_spectrum(self, k):
         out = np.zeros(2 * self.N, dtype=np.float32)
-        self.lib().ref_get_kernel_spectrum(int(k), _fp(out))
+        self.lib(self._path).ref_get_kernel_spectrum(int(k), _fp(out))
         return out
 
     def bell_lut(self, m, s, u):
-        return self.lib().ref_bell_lut(m, s, u)
+        return self.lib(self._path).ref_bell_lut(m, s, u)
 
 
 class RestateOracle(_Base):

@@ -15,6 +15,9 @@
  *         exactly U_S and SUM_S (render.cpp:399-403 overruns SUM_S);
  *       * after SIM_EVENT_TRM the spectra T[c] are recomputed from the
  *         complete `val` (lenia.cpp:1039-1044 races the two slabs);
+ *   - optionally runs each event's two slabs on two threads at once
+ *     (ref_step_slabs), as the reference's SIM_THREADS = 2 sim threads do
+ *     between the barriers of render.cpp:357-604;
  *   - exposes a C API for ctypes (ref_*).
  * It copies no reference code; it calls the reference's functions.
  */
@@ -27,6 +30,7 @@
 
 #include <stdint.h>
 
+#include <thread>
 #include <vector>
 
 #include "../restate/oracle_api.h"
@@ -323,8 +327,20 @@ void ref_set_state(const float *A, const float *V, const float *GAin, const floa
     recompute_spectra();
 }
 
+/* Slab threads: 0 runs the slabs one after the other on the calling thread;
+ * 1 runs slab 1 on a second thread while the caller runs slab 0 and joins it
+ * before the next event (the reference's barrier per event). */
+static int g_slab_threads = 0;
+
 static void run_both(void (*fn)(TD *))
 {
+    if (g_slab_threads) {
+        std::thread other(fn, &sim_td[1]);
+        fn(&sim_td[0]);
+        other.join();
+        for (int t = 2; t < SIM_THREADS; t++) fn(&sim_td[t]);
+        return;
+    }
     for (int t = 0; t < SIM_THREADS; t++) fn(&sim_td[t]);
 }
 
@@ -409,6 +425,14 @@ void ref_step(int nsteps)
 {
     for (int s = 0; s < nsteps; s++)
         for (int ev = 0; ev < ORA_EV_MAX; ev++) ref_run_event(ev);
+}
+
+/* ref_step with the two slabs of every event on two threads at once. */
+void ref_step_slabs(int nsteps)
+{
+    g_slab_threads = 1;
+    ref_step(nsteps);
+    g_slab_threads = 0;
 }
 
 static void get_padded(const float *src, int nch, float *out)
