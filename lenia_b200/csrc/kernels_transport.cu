@@ -12,6 +12,7 @@
 #include "lenia_internal.h"
 #include "growth_common.cuh"
 #include "tma.cuh"
+#include "async_copy.cuh"
 
 namespace lenia {
 
@@ -42,9 +43,11 @@ __device__ __forceinline__ float torus_wrap(float m, int ext)
 
 // Oscillators (lenia.cpp:803-911) and transpose_to_row_major
 // (lenia.cpp:924-1037) for one destination cell; tt holds its reintegrated
-// mass per channel.
+// mass per channel.  ga_pre, when not null, holds the cell's GA per channel
+// (stride ga_stride) already copied to shared memory; else GA is read here.
 __device__ __forceinline__ void transport_epilogue(const StepParams &p, const TransportBuffers &b, float *tt, int x,
-                                                   int y, int z, long long i)
+                                                   int y, int z, long long i, const float *ga_pre = nullptr,
+                                                   int ga_stride = 0)
 {
     const Dims &d = p.d;
     const long long N = d.N;
@@ -121,7 +124,8 @@ __device__ __forceinline__ void transport_epilogue(const StepParams &p, const Tr
         if (c >= C) continue;
         const long long ci = (long long)c * N + i;
         ttsum = ttsum + tt[c];
-        b.GA[ci] = gtam * b.GA[ci] + tt[c] * gtas;
+        const float ga = ga_pre ? ga_pre[c * ga_stride] : b.GA[ci];
+        b.GA[ci] = gtam * ga + tt[c] * gtas;
         b.A_out[ci] = tt[c];
     }
     // SUM was cleared at the end of reintegration (lenia.cpp:912-915)
@@ -316,6 +320,10 @@ __device__ __forceinline__ bool tb_source(const Dims &d, int dd, int &x, int &y,
 // 1 buffer and 4 blocks per SM measured faster than 2 buffers and 2 blocks
 // (121 vs 157 us at 128^3 x 4 channels): other blocks cover the copy.
 constexpr int kTBufs = LENIA_TRANSPORT_BUFS;  // 2: channel c + 1 lands while c is used
+#ifndef LENIA_TRANSPORT_PREGA
+#define LENIA_TRANSPORT_PREGA 1
+#endif
+constexpr bool kTransportPrefetchGA = LENIA_TRANSPORT_PREGA;
 
 template <int DD, bool TORUS, bool CLIP1>
 __global__ void __launch_bounds__(kTX *kTY, LENIA_TRANSPORT_MINB) k_transport_tiled(StepParams p, TransportBuffers b,
@@ -324,7 +332,11 @@ __global__ void __launch_bounds__(kTX *kTY, LENIA_TRANSPORT_MINB) k_transport_ti
 {
     constexpr int SX = kTBoxX, SY = kTY + 2 * DD, SZ = kTZ + 2 * DD, SV = SX * SY * SZ;
     constexpr int OX = 4 - DD;  // staged x of source offset -DD from the tile's first column
-    extern __shared__ __align__(128) float tiles[];  // [kTBufs buffers][MU_x, MU_y, MU_z, ARR][SV]
+    // [kTBufs buffers][MU_x, MU_y, MU_z, ARR][SV], then (DD == 1) the block's
+    // GA values [channel][z][thread], copied while the gather runs
+    extern __shared__ __align__(128) float tiles[];
+    constexpr bool kPreGA = kTransportPrefetchGA && DD == 1;
+    float *ga_s = tiles + kTBufs * 4 * SV;
     __shared__ __align__(8) uint64_t bars[2];
     const Dims &d = p.d;
     const long long N = d.N;
@@ -351,6 +363,19 @@ __global__ void __launch_bounds__(kTX *kTY, LENIA_TRANSPORT_MINB) k_transport_ti
     __syncthreads();
     pdl_trigger();
     pdl_wait();
+    // GA of this thread's cells, read by the epilogue: copied now so that the
+    // epilogue does not wait on global loads after the gather
+    if (kPreGA && x < d.W && y < d.H) {
+#pragma unroll
+        for (int c = 0; c < kMaxChannels; c++)
+#pragma unroll
+            for (int j = 0; j < kTZ; j++)
+                if (c < C && z0 + j < d.D)
+                    cp_async_f32(ga_s + (c * kTZ + j) * (kTX * kTY) + tid,
+                                 b.GA + (long long)c * N + x + (long long)y * d.W + (long long)(z0 + j) * d.W * d.H,
+                                 true);
+        cp_async_commit();
+    }
     // queues channel c's MU and ARR tiles (cells plus a DD halo) into buffer c % kTBufs
     auto issue = [&](int c) {
         if (!leader) return;
@@ -413,6 +438,7 @@ __global__ void __launch_bounds__(kTX *kTY, LENIA_TRANSPORT_MINB) k_transport_ti
             mbar_wait(&bars[c % kTBufs], (unsigned)(c / kTBufs) & 1u, kDrainPolls);
             if (kTBufs == 2 && c + 1 < crt)
                 mbar_wait(&bars[(c + 1) % kTBufs], (unsigned)((c + 1) / kTBufs) & 1u, kDrainPolls);
+            if (kPreGA) cp_async_wait<0>();
             if (leader && b.err) atomicOr(b.err, 2);
             return;
         }
@@ -479,6 +505,7 @@ __global__ void __launch_bounds__(kTX *kTY, LENIA_TRANSPORT_MINB) k_transport_ti
     if (x >= d.W || y >= d.H) return;
 
     // oscillators and transpose_to_row_major, per destination cell
+    if (kPreGA) cp_async_wait<0>();
 #pragma unroll
     for (int j = 0; j < kTZ; j++) {
         const int z = z0 + j;
@@ -487,7 +514,10 @@ __global__ void __launch_bounds__(kTX *kTY, LENIA_TRANSPORT_MINB) k_transport_ti
         float t4[kMaxChannels];
 #pragma unroll
         for (int c = 0; c < kMaxChannels; c++) t4[c] = tt[c][j];
-        transport_epilogue(p, b, t4, x, y, z, i);
+        if (kPreGA)
+            transport_epilogue(p, b, t4, x, y, z, i, ga_s + j * (kTX * kTY) + tid, kTZ * kTX * kTY);
+        else
+            transport_epilogue(p, b, t4, x, y, z, i);
     }
 }
 
@@ -510,7 +540,8 @@ cudaError_t launch_transport(const StepParams &p, const TransportBuffers &b, cud
             if (e == cudaSuccess) e = encode_tensor_map(&tm_arr, b.ARR, 4, darr, box);
             if (e != cudaSuccess) return e;
             const int sv = kTBoxX * (kTY + 2 * dd) * (kTZ + 2 * dd);
-            const size_t smem = kTBufs * 4 * (size_t)sv * sizeof(float);
+            const size_t ga = (kTransportPrefetchGA && dd == 1) ? (size_t)kMaxChannels * kTZ * kTX * kTY : 0;
+            const size_t smem = (kTBufs * 4 * (size_t)sv + ga) * sizeof(float);
             e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
             return launch_pdl(kern, grid, block, smem, st, p, b, tm_mu, tm_arr);
