@@ -328,9 +328,11 @@ lenia_status lenia_batch_stats(lenia_batch *b, float fill_threshold, double *out
  *
  * No counterpart in the reference.  A multilayer perceptron n_in -> hidden ->
  * hidden -> hidden -> 1 with GELU, trained and evaluated by this library's
- * own kernels: weights and activations enter each matrix product rounded to
- * bfloat16, products accumulate in float32, the loss is binary cross-entropy
- * on the logit, and Adam updates float32 master weights.  Parameters are laid
+ * own kernels: every matrix product (forward, weight gradient, activation
+ * gradient) runs on the tcgen05 tensor cores with bfloat16 operands (weights,
+ * activations, and dz in the backward products, rounded to nearest even) and
+ * float32 accumulation in tensor memory; the loss is binary cross-entropy on
+ * the logit, and Adam updates float32 master weights.  Parameters are laid
  * out layer by layer, W (out x in, row-major) then b. */
 typedef struct lenia_mlp lenia_mlp;
 lenia_status lenia_mlp_create(int n_in, int hidden, unsigned long long seed, lenia_mlp **out);

@@ -369,6 +369,20 @@ PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 cudaError_t encode_tensor_map_typed(CUtensorMap *map, const void *base, int dtype, int elem_bytes, int rank,
                                     const unsigned long long *dims, const unsigned *box)
 {
+    unsigned long long strides[4];
+    unsigned long long stride = (unsigned long long)elem_bytes;
+    for (int i = 0; i + 1 < rank && i < 4; i++) {
+        stride *= dims[i];
+        strides[i] = stride;
+    }
+    return encode_tensor_map_strided(map, base, dtype, rank, dims, strides, box);
+}
+
+cudaError_t encode_tensor_map_strided(CUtensorMap *map, const void *base, int dtype, int rank,
+                                      const unsigned long long *dims, const unsigned long long *strides,
+                                      const unsigned *box)
+{
+    if (rank < 1 || rank > 5) return cudaErrorInvalidValue;
     if (!g_encode) {
         void *fn = nullptr;
         cudaDriverEntryPointQueryResult q;
@@ -378,13 +392,11 @@ cudaError_t encode_tensor_map_typed(CUtensorMap *map, const void *base, int dtyp
     }
     cuuint64_t gdim[5], gstride[4];
     cuuint32_t bdim[5], estride[5];
-    unsigned long long stride = (unsigned long long)elem_bytes;
     for (int i = 0; i < rank; i++) {
         gdim[i] = dims[i];
         bdim[i] = box[i];
         estride[i] = 1;
-        if (i > 0) gstride[i - 1] = stride;
-        stride *= dims[i];
+        if (i > 0) gstride[i - 1] = strides[i - 1];
     }
     const CUresult r = g_encode(map, (CUtensorMapDataType)dtype, (cuuint32_t)rank, (void *)base, gdim, gstride, bdim,
                                 estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,

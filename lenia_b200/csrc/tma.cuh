@@ -97,4 +97,12 @@ cudaError_t encode_tensor_map(CUtensorMap *map, const float *base, int rank, con
 cudaError_t encode_tensor_map_typed(CUtensorMap *map, const void *base, int dtype, int elem_bytes, int rank,
                                     const unsigned long long *dims, const unsigned *box);
 
+// Host: the same with explicit byte strides of dimensions 1..rank-1
+// (strides[i] is the stride of dimension i + 1; each a multiple of 16), so
+// that dims[0] may be shorter than the row pitch: reads past dims[0] then
+// return zero.
+cudaError_t encode_tensor_map_strided(CUtensorMap *map, const void *base, int dtype, int rank,
+                                      const unsigned long long *dims, const unsigned long long *strides,
+                                      const unsigned *box);
+
 }  // namespace lenia

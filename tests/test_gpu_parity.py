@@ -187,3 +187,27 @@ def test_config1_step_bit_exact(cuda_lib, oracle_built, growth_split):
         r = diff_report(n, ora.get(n), gpu.get(n))
         assert not r, r
     gpu.sync()
+
+
+@pytest.mark.parametrize("mode", ["rt", "advection"])
+def test_config1_ten_steps_bit_exact(cuda_lib, oracle_built, mode):
+    """The 128^3 x 4 channel, 16-kernel configuration with RT and with
+    advection reintegration (adv_vel: the semi-Lagrangian pull of every
+    channel, reintegration.cpp:1112-1260): whole production steps, autotuned
+    as a user runs them, bit-exact after the first step and after ten."""
+    from lenia_b200.world import World
+    wl = P.config1(seed=4, mode=P.MODE_RT if mode == "rt" else P.MODE_ADV)
+    p, ks = as_oracle(wl)
+    ora = RestateOracle(p, ks, fft_mode="half")
+    ora.set_state(A=wl.A0.ravel())
+    gpu = World(wl.desc, wl.kernels)
+    gpu.autotune(modes=("FFT",))
+    gpu.set_state(wl.A0.ravel())
+    for steps in (1, 9):
+        ora.step(steps)
+        gpu.step(steps)
+        for n in ("A", "V", "GA", "SUM"):
+            r = diff_report(n, ora.get(n), gpu.get(n))
+            assert not r, f"{mode}: {r}"
+    gpu.sync()
+    gpu.close()

@@ -1,5 +1,6 @@
 """The proposal network: forward and gradients against a numpy float64
-restatement with the same bfloat16 rounding, and training."""
+restatement with the same bfloat16 rounding of every tensor-core operand
+(activations, weights, and dz in the backward products), and training."""
 import numpy as np
 import pytest
 from scipy.special import erf
@@ -32,11 +33,14 @@ def np_forward_backward(p, x, y):
     grads = []
     for i in range(len(layers) - 1, -1, -1):
         W, _ = layers[i]
-        gW = dz.T @ bf16(acts[i]).astype(np.float64)
+        # dz enters both products rounded to bfloat16 (the tensor cores take
+        # bfloat16 operands); the bias gradient sums it in float
+        dzb = bf16(dz.astype(np.float32)).astype(np.float64)
+        gW = dzb.T @ bf16(acts[i]).astype(np.float64)
         gb = dz.sum(axis=0)
         grads.append((gW, gb))
         if i > 0:
-            da = dz @ bf16(W).astype(np.float64)
+            da = dzb @ bf16(W).astype(np.float64)
             z = zs[i - 1]
             gp = 0.5 * (1 + erf(z / np.sqrt(2))) + z * np.exp(-0.5 * z * z) / np.sqrt(2 * np.pi)
             dz = da * gp
