@@ -11,10 +11,11 @@
 // On the GPU:
 //
 //   mc_count    per cube and channel: case index, triangle count, and how many
-//               vertices the cube creates; per chunk of kMcThreads cubes the
-//               two sums;
-//   mc_scan     exclusive scan of the chunk sums (one block): each cube's first
-//               triangle and first created vertex;
+//               vertices the cube creates; per chunk of kMcThreads cubes and
+//               channel the two sums (one block reduction per chunk);
+//   mc_scan     exclusive scan of the chunk sums (one block, coalesced tiles);
+//               emit and index skip chunk-channels without triangles, so
+//               their work follows the surface, not the volume;
 //   mc_emit     per cube: face normals of its triangles; position, channel and
 //               source edge of the vertices it creates;
 //   mc_index    per cube: the vertex of every triangle slot;
@@ -257,20 +258,28 @@ __device__ __forceinline__ CubeRef cube_of(const McGeom &g, int chunk)
     return r;
 }
 
+// Per chunk (one block of kMcThreads cubes) and channel: the chunk's
+// triangle and created-vertex totals, packed as tri | vert << 32.  Each thread
+// walks its cube's channels in order (a vertex shared between channels
+// belongs to the first channel that intersects its edge), writes the case
+// indices, and keeps its counts per channel; one block reduction at the end.
 __global__ void __launch_bounds__(kMcThreads) k_mc_count(McGeom g, const McTables *__restrict__ tab,
                                                         unsigned char *__restrict__ cases,
-                                                        long long *__restrict__ blk_tri,
-                                                        long long *__restrict__ blk_vert)
+                                                        unsigned long long *__restrict__ blk)
 {
     __shared__ McTables s_tab;
-    __shared__ unsigned s_warp[kMcWarps];
+    __shared__ unsigned s_part[kMcWarps][LENIA_MAX_CHANNELS];
     load_tables(tab, s_tab);
     const int nchunks = g.slabs * g.nblk;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const CubeRef q = cube_of(g, chunk);
         const unsigned owned = q.valid ? s_tab.owned[boundary_class(g, q.gx, q.gy, q.gz, q.z0, q.z1)] : 0u;
         unsigned prev[kMcMaxFields] = {0u, 0u, 0u};
-        for (int c = 0; c < g.C; c++) {
+        unsigned packed[LENIA_MAX_CHANNELS] = {0u, 0u, 0u, 0u};  // nt | nn << 16 per channel
+#pragma unroll
+        for (int c = 0; c < LENIA_MAX_CHANNELS; c++) {
+            if (c >= g.C) break;
             unsigned nt = 0, nn = 0;
 #pragma unroll
             for (int f = 0; f < kMcMaxFields; f++) {
@@ -288,58 +297,100 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_count(McGeom g, const McTable
                 nn += __popc(owned & act & ~prev[f]);
                 if (g.share) prev[f] |= act;
             }
-            unsigned total;
-            block_scan(nt | nn << 16, s_warp, &total);
-            if (threadIdx.x == 0) {
-                const long long o = ((long long)q.s * g.C + c) * g.nblk + q.b;
-                blk_tri[o] = total & 0xffff;
-                blk_vert[o] = total >> 16;
-            }
+            packed[c] = nt | nn << 16;
         }
+        // block sums per channel (at most 5 triangles and 12 vertices per cube
+        // and field: 16 bits per count hold a chunk)
+#pragma unroll
+        for (int c = 0; c < LENIA_MAX_CHANNELS; c++) {
+            const unsigned w = __reduce_add_sync(0xffffffffu, packed[c]);
+            if (lane == 0) s_part[wid][c] = w;
+        }
+        __syncthreads();
+        if (threadIdx.x < g.C) {
+            const int c = threadIdx.x;
+            unsigned long long t = 0, v = 0;
+            for (int w = 0; w < kMcWarps; w++) {
+                t += s_part[w][c] & 0xffffu;
+                v += s_part[w][c] >> 16;
+            }
+            blk[((long long)q.s * g.C + c) * g.nblk + q.b] = t | v << 32;
+        }
+        __syncthreads();
     }
 }
 
-// Exclusive scan of the chunk sums in place (one block of 1024 threads);
-// totals[0..1] = triangles, vertices.
-__global__ void __launch_bounds__(1024) k_mc_scan(long long *tri, long long *vert, long long M, long long *totals)
+// Exclusive scan of the M packed chunk totals in place (one block of 1024
+// threads, tiles of 8192 with a running carry; each thread scans 8
+// consecutive values); totals[0..1] = triangles, vertices.  Packed addition
+// is exact while the triangle total stays below 2^32 (the host checks it).
+constexpr int kScanThreads = 1024;
+constexpr int kScanPer = 8;
+__global__ void __launch_bounds__(kScanThreads) k_mc_scan(unsigned long long *blk, long long M, long long *totals)
 {
-    __shared__ long long s_a[1024], s_b[1024];
-    const int t = threadIdx.x;
-    const long long per = (M + 1023) / 1024;
-    const long long beg = t * per, end = beg + per < M ? beg + per : M;
-    long long st = 0, sv = 0;
-    for (long long i = beg; i < end; i++) {
-        st += tri[i];
-        sv += vert[i];
-    }
-    s_a[t] = st;
-    s_b[t] = sv;
+    __shared__ unsigned long long s_warp[kScanThreads / 32];
+    __shared__ unsigned long long s_carry;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    if (t == 0) s_carry = 0;
     __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
-        const long long a = t >= o ? s_a[t - o] : 0, b = t >= o ? s_b[t - o] : 0;
+    for (long long base = 0; base < M; base += (long long)kScanThreads * kScanPer) {
+        unsigned long long v[kScanPer];
+        const long long i0 = base + (long long)t * kScanPer;
+#pragma unroll
+        for (int j = 0; j < kScanPer; j++) v[j] = i0 + j < M ? blk[i0 + j] : 0ull;
+        unsigned long long sum = 0;
+#pragma unroll
+        for (int j = 0; j < kScanPer; j++) sum += v[j];
+        // inclusive warp scan of the thread sums, then of the warp sums
+        unsigned long long x = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s_warp[wid] = x;
         __syncthreads();
-        s_a[t] += a;
-        s_b[t] += b;
+        if (wid == 0) {
+            unsigned long long w = s_warp[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            s_warp[lane] = w;
+        }
+        __syncthreads();
+        const unsigned long long carry = s_carry;
+        unsigned long long run = carry + (wid > 0 ? s_warp[wid - 1] : 0ull) + x - sum;
+#pragma unroll
+        for (int j = 0; j < kScanPer; j++) {
+            if (i0 + j < M) blk[i0 + j] = run;
+            run += v[j];
+        }
+        __syncthreads();
+        if (t == kScanThreads - 1) s_carry = run;
         __syncthreads();
     }
-    long long ba = s_a[t] - st, bb = s_b[t] - sv;
-    for (long long i = beg; i < end; i++) {
-        const long long x = tri[i], y = vert[i];
-        tri[i] = ba;
-        vert[i] = bb;
-        ba += x;
-        bb += y;
+    if (t == 0) {
+        totals[0] = (long long)(s_carry & 0xffffffffull);
+        totals[1] = (long long)(s_carry >> 32);
     }
-    if (t == 1023) {
-        totals[0] = s_a[t];
-        totals[1] = s_b[t];
-    }
+}
+
+// Triangles of chunk-channel o (blk holds the exclusive scan; the last one
+// ends at the total).
+__device__ __forceinline__ long long chunk_tris(const unsigned long long *blk, long long o, long long M,
+                                               const long long *totals)
+{
+    const long long beg = (long long)(blk[o] & 0xffffffffull);
+    const long long end = o + 1 < M ? (long long)(blk[o + 1] & 0xffffffffull) : totals[0];
+    return end - beg;
 }
 
 __global__ void __launch_bounds__(kMcThreads) k_mc_emit(McGeom g, const McTables *__restrict__ tab,
                                                        const unsigned char *__restrict__ cases,
-                                                       const long long *__restrict__ blk_tri,
-                                                       const long long *__restrict__ blk_vert,
+                                                       const unsigned long long *__restrict__ blk,
+                                                       const long long *__restrict__ totals,
                                                        int *__restrict__ tri_base, int *__restrict__ vert_base,
                                                        float *__restrict__ fn, float *__restrict__ pos,
                                                        int *__restrict__ vch, unsigned long long *__restrict__ vsrc)
@@ -348,11 +399,17 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_emit(McGeom g, const McTables
     __shared__ unsigned s_warp[kMcWarps];
     load_tables(tab, s_tab);
     const int nchunks = g.slabs * g.nblk;
+    const long long M = (long long)g.slabs * g.C * g.nblk;
     for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const CubeRef q = cube_of(g, chunk);
         const unsigned owned = q.valid ? s_tab.owned[boundary_class(g, q.gx, q.gy, q.gz, q.z0, q.z1)] : 0u;
         unsigned prev[kMcMaxFields] = {0u, 0u, 0u};
         for (int c = 0; c < g.C; c++) {
+            const long long o = ((long long)q.s * g.C + c) * g.nblk + q.b;
+            // a chunk-channel without triangles (the whole block takes the
+            // same branch) has no intersected edge in any of its cubes
+            // (cases 0 and 255 only): nothing to emit, nothing to add to prev
+            if (chunk_tris(blk, o, M, totals) == 0) continue;
             int cs[kMcMaxFields] = {0, 0, 0};
             unsigned newm[kMcMaxFields] = {0u, 0u, 0u};
             unsigned nt = 0, nn = 0;
@@ -369,9 +426,8 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_emit(McGeom g, const McTables
             unsigned total;
             const unsigned pre = block_scan(nt | nn << 16, s_warp, &total);
             if (nt == 0) continue;
-            const long long o = ((long long)q.s * g.C + c) * g.nblk + q.b;
-            long long tb = blk_tri[o] + (pre & 0xffff);
-            long long vb = blk_vert[o] + (pre >> 16);
+            long long tb = (long long)(blk[o] & 0xffffffffull) + (pre & 0xffff);
+            long long vb = (long long)(blk[o] >> 32) + (pre >> 16);
 #pragma unroll
             for (int f = 0; f < kMcMaxFields; f++) {
                 if (f >= g.F) break;
@@ -441,16 +497,20 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_index(McGeom g, const McTable
                                                         const unsigned char *__restrict__ cases,
                                                         const int *__restrict__ tri_base,
                                                         const int *__restrict__ vert_base,
+                                                        const unsigned long long *__restrict__ blk,
+                                                        const long long *__restrict__ totals,
                                                         unsigned *__restrict__ idx)
 {
     __shared__ McTables s_tab;
     load_tables(tab, s_tab);
     const int nchunks = g.slabs * g.nblk;
+    const long long M = (long long)g.slabs * g.C * g.nblk;
     const long long WH = (long long)g.W * g.H;
     for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const CubeRef q = cube_of(g, chunk);
         if (!q.valid) continue;
         for (int c = 0; c < g.C; c++) {
+            if (chunk_tris(blk, ((long long)q.s * g.C + c) * g.nblk + q.b, M, totals) == 0) continue;
             for (int f = 0; f < g.F; f++) {
                 const int cs = cases[fc_off(g, f, c) + q.p];
                 const unsigned long long tl = s_tab.tri[cs];
@@ -670,7 +730,8 @@ struct lenia_mesher {
     McTables *tab = nullptr;
     unsigned char *cases = nullptr;
     int *tri_base = nullptr, *vert_base = nullptr;
-    long long *blk_tri = nullptr, *blk_vert = nullptr, *totals = nullptr, *h_totals = nullptr;
+    unsigned long long *blk = nullptr;  // per chunk and channel: tri | vert << 32, then its exclusive scan
+    long long *totals = nullptr, *h_totals = nullptr;
     float *fn = nullptr, *pos = nullptr, *nrm = nullptr;
     int *vch = nullptr;
     unsigned long long *vsrc = nullptr;
@@ -788,7 +849,8 @@ lenia_status lenia_mesher_create(const LeniaMeshDesc *desc, lenia_mesher **out)
     for (int f = 0; f < kMcMaxFields; f++)
         for (int a = 0; a < 3; a++) g.off[f][a] = f < g.F ? d.offset[f][a] : 0.0f;
     const long long nchunks = (long long)g.slabs * g.nblk;
-    m->grid = (int)(nchunks < 8LL * nsm ? nchunks : 8LL * nsm);
+    // one chunk per block up to 32 blocks per SM (resident eight at a time)
+    m->grid = (int)(nchunks < 32LL * nsm ? nchunks : 32LL * nsm);
     const long long M = nchunks * g.C;
     McTables host;
     build_tables(&host);
@@ -801,8 +863,7 @@ lenia_status lenia_mesher_create(const LeniaMeshDesc *desc, lenia_mesher **out)
     alloc(m->cases, cubes);
     alloc(m->tri_base, sizeof(int) * cubes);
     alloc(m->vert_base, sizeof(int) * cubes);
-    alloc(m->blk_tri, sizeof(long long) * (size_t)M);
-    alloc(m->blk_vert, sizeof(long long) * (size_t)M);
+    alloc(m->blk, sizeof(unsigned long long) * (size_t)M);
     alloc(m->totals, 2 * sizeof(long long));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&m->h_totals, 2 * sizeof(long long));
     if (e == cudaSuccess) e = cudaMemcpy(m->tab, &host, sizeof(McTables), cudaMemcpyHostToDevice);
@@ -823,8 +884,7 @@ lenia_status lenia_mesher_destroy(lenia_mesher *m)
     dfree(m->cases);
     dfree(m->tri_base);
     dfree(m->vert_base);
-    dfree(m->blk_tri);
-    dfree(m->blk_vert);
+    dfree(m->blk);
     dfree(m->totals);
     if (m->h_totals) cudaFreeHost(m->h_totals);
     delete m;
@@ -845,8 +905,8 @@ lenia_status lenia_mesher_run(lenia_mesher *m, const float *const *fields, const
     m->stream = st;
     m->have_mesh = false;
     const long long M = (long long)g.slabs * g.nblk * g.C;
-    k_mc_count<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk_tri, m->blk_vert);
-    k_mc_scan<<<1, 1024, 0, st>>>(m->blk_tri, m->blk_vert, M, m->totals);
+    k_mc_count<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk);
+    k_mc_scan<<<1, kScanThreads, 0, st>>>(m->blk, M, m->totals);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(m->h_totals, m->totals, 2 * sizeof(long long), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -872,9 +932,10 @@ lenia_status lenia_mesher_run(lenia_mesher *m, const float *const *fields, const
         m->cap_v = cv;
     }
     if (nt > 0) {
-        k_mc_emit<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk_tri, m->blk_vert, m->tri_base,
+        k_mc_emit<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk, m->totals, m->tri_base,
                                                   m->vert_base, m->fn, m->pos, m->vch, m->vsrc);
-        k_mc_index<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vert_base, m->idx);
+        k_mc_index<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vert_base, m->blk, m->totals,
+                                                   m->idx);
         const long long nb = (nv + kMcThreads - 1) / kMcThreads;
         const int gn = (int)(nb < 64LL * m->grid ? (nb > 0 ? nb : 1) : 64LL * m->grid);
         k_mc_normals<<<gn, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vsrc, m->fn, m->nrm, nv);

@@ -25,6 +25,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <random>
 #include <string>
 #include <vector>
@@ -49,12 +50,13 @@ constexpr int kMlpLayers = 4;
 // rows, each landing as a column of 8 x 16-byte core matrices (the canonical
 // K-major layout without swizzle: core matrices adjacent in M/N 128 bytes
 // apart, adjacent in K `rows` x 16 bytes apart).  Thread 0 issues the copies,
-// thread 32 the MMAs; after the last MMA the four warps read the accumulator
-// (warp w: lanes 32w..32w+31 = rows) and run the epilogue.
+// thread 32 the MMAs; after the last MMA sixteen warps read the accumulator
+// (warp w: lanes 32(w % 4)..+31 = rows, every fourth 32-column group from
+// 32(w / 4)) and run the epilogue (its GELU evaluations are the long part).
 constexpr int kGemmM = 128;
 constexpr int kGemmKC = 64;      // K per stage
 constexpr int kGemmStages = 3;
-constexpr int kGemmThreads = 128;
+constexpr int kGemmThreads = 512;  // 16 warps: 4 per tensor-memory lane quadrant in the epilogue
 constexpr int kGemmHeader = 1024;
 constexpr unsigned long long kGemmWaitNs = 2000000000ull;  // 2 s per wait
 constexpr unsigned kGemmWaitPolls = 1u << 30;
@@ -65,6 +67,8 @@ struct TcGemm {
     int M, N, K;       // rows and columns of C, reduction length
     int Np;            // MMA N (N rounded up to 16)
     int mode;
+    int kper;                    // K per CTA row (blockIdx.y): a multiple of 64
+    float *ws;                   // split K (gridDim.y > 1): partial sums [y][M][N]
     const float *bias;           // kEpiHidden, kEpiLogit
     float *c32;                  // float32 result (z, logit, dW or dz)
     long long ldc;
@@ -163,8 +167,11 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_tc_gemm(TcGemm g, const __g
     const uint32_t stage_bytes = a_bytes + b_bytes;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * kGemmM;
+    // this CTA's share of K: [kbeg, kend), whole 64-element chunks except at K
     const int Kp = (g.K + 15) / 16 * 16;
-    const int nchunks = (Kp + kGemmKC - 1) / kGemmKC;
+    const int kbeg = blockIdx.y * g.kper;
+    const int kend = min(Kp, kbeg + g.kper);
+    const int nchunks = (kend - kbeg + kGemmKC - 1) / kGemmKC;
     const uint32_t ncols = g.Np <= 32 ? 32u : g.Np <= 64 ? 64u : g.Np <= 128 ? 128u : 256u;
     // kind::f16, D float32, A and B bfloat16, both K-major, N >> 3, M >> 4
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(g.Np >> 3) << 17) |
@@ -202,8 +209,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_tc_gemm(TcGemm g, const __g
                 break;
             }
             if (*(volatile int *)s_bad) break;
-            const int k0 = i * kGemmKC;
-            const int nk = min(8, (Kp - k0) / 8);  // 8-element k slices in this chunk
+            const int k0 = kbeg + i * kGemmKC;
+            const int nk = min(8, (kend - k0) / 8);  // 8-element k slices in this chunk
             unsigned char *sa = stages + (size_t)s * stage_bytes, *sb = sa + a_bytes;
             mbar_arrive_expect_tx(&full[s], (unsigned)nk * (kGemmM * 16u + (unsigned)g.Np * 16u));
             for (int c = 0; c < nk; c++) {
@@ -221,8 +228,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_tc_gemm(TcGemm g, const __g
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            const int k0 = i * kGemmKC;
-            const int nm = min(4, (Kp - k0) / 16);
+            const int k0 = kbeg + i * kGemmKC;
+            const int nm = min(4, (kend - k0) / 16);
             const uint32_t sa = smem_addr(stages + (size_t)s * stage_bytes), sb = sa + a_bytes;
             for (int j = 0; j < nm; j++) {
                 const uint64_t da = gemm_desc(sa + (uint32_t)j * 2u * kGemmM * 16u, kGemmM * 16u, 128u);
@@ -250,18 +257,21 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_tc_gemm(TcGemm g, const __g
     const bool bad = *(volatile int *)s_bad != 0;
 
     if (!bad) {
-        const int m = m0 + warp * 32 + lane;
+        const int quad = warp & 3, part = warp >> 2;
+        const int m = m0 + quad * 32 + lane;
         const bool row_ok = m < g.M;
-        for (int c0 = 0; c0 < g.Np; c0 += 32) {
+        for (int c0 = 32 * part; c0 < g.Np; c0 += 128) {
             uint32_t v[32];
-            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            tmem_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)c0, v);
             if (!row_ok) continue;
 #pragma unroll
             for (int j = 0; j < 32; j++) {
                 const int n = c0 + j;
                 if (n >= g.N) break;
                 const float acc = __uint_as_float(v[j]);
-                if (g.mode == kEpiHidden) {
+                if (g.ws) {
+                    g.ws[((long long)blockIdx.y * g.M + m) * g.N + n] = acc;
+                } else if (g.mode == kEpiHidden) {
                     const float z = acc + g.bias[n];
                     g.c32[(long long)m * g.ldc + n] = z;
                     const __nv_bfloat16 a = __float2bfloat16_rn(gelu(z));
@@ -293,6 +303,18 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_tc_gemm(TcGemm g, const __g
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(ncols) : "memory");
 }
 
+// c[m][n] = sum over s = 0, 1, ... of ws[s][m][n] (fixed order).
+__global__ void k_split_sum(const float *__restrict__ ws, int ns, int M, int N, float *__restrict__ c, long long ldc)
+{
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long mn = (long long)M * N;
+    if (i >= mn) return;
+    float s = ws[i];
+    for (int k = 1; k < ns; k++) s += ws[(long long)k * mn + i];
+    const int m = (int)(i / N), n = (int)(i - (long long)m * N);
+    c[(long long)m * ldc + n] = s;
+}
+
 size_t gemm_smem(int Np) { return kGemmHeader + (size_t)kGemmStages * (8u * kGemmM * 16u + 8u * (unsigned)Np * 16u); }
 
 // A bfloat16 matrix in global memory: rows x cols, row stride ld (a multiple of 8).
@@ -316,7 +338,11 @@ cudaError_t gemm_map(CUtensorMap *map, const Bf16Mat &m, int rows, int cols, int
 }
 
 // C = A B^T for the first M rows of A and N rows of B (each K columns wide).
-cudaError_t tc_gemm(const Bf16Mat &A, int M, const Bf16Mat &B, int N, int K, TcGemm g, cudaStream_t st)
+// ksplit > 1 (weight gradients only) splits K over that many CTA rows, each
+// writing its partial product to ws (ksplit x M x N floats); k_split_sum
+// then adds the partials in split order into g.c32.
+cudaError_t tc_gemm(const Bf16Mat &A, int M, const Bf16Mat &B, int N, int K, TcGemm g, cudaStream_t st,
+                    int ksplit = 1, float *ws = nullptr)
 {
     if (M < 1 || N < 1 || N > 256 || K < 1 || A.cols < K || B.cols < K || A.rows < M || B.rows < N)
         return cudaErrorInvalidValue;
@@ -324,6 +350,11 @@ cudaError_t tc_gemm(const Bf16Mat &A, int M, const Bf16Mat &B, int N, int K, TcG
     g.N = N;
     g.K = K;
     g.Np = round_up(N, 16);
+    const int Kp = round_up(K, 16);
+    if (ksplit < 1 || (ksplit > 1 && (!ws || g.mode != kEpiWeightGrad))) return cudaErrorInvalidValue;
+    g.kper = round_up((Kp + ksplit - 1) / ksplit, kGemmKC);
+    ksplit = (Kp + g.kper - 1) / g.kper;
+    g.ws = ksplit > 1 ? ws : nullptr;
     CUtensorMap ta, tb;
     cudaError_t e = gemm_map(&ta, A, M, K, kGemmM);
     if (e == cudaSuccess) e = gemm_map(&tb, B, N, K, g.Np);
@@ -331,8 +362,15 @@ cudaError_t tc_gemm(const Bf16Mat &A, int M, const Bf16Mat &B, int N, int K, TcG
     const size_t smem = gemm_smem(g.Np);
     e = cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_tc_gemm<<<(M + kGemmM - 1) / kGemmM, kGemmThreads, smem, st>>>(g, ta, tb);
-    return cudaGetLastError();
+    dim3 grid((M + kGemmM - 1) / kGemmM, ksplit);
+    k_tc_gemm<<<grid, kGemmThreads, smem, st>>>(g, ta, tb);
+    e = cudaGetLastError();
+    if (e == cudaSuccess && ksplit > 1) {
+        const long long n = (long long)M * N;
+        k_split_sum<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ws, ksplit, M, N, g.c32, g.ldc);
+        e = cudaGetLastError();
+    }
+    return e;
 }
 
 // dst[r][c] = bf16(src[r][c]) (or of src[c][r] with transpose) for r < rows,
@@ -428,6 +466,8 @@ struct lenia_mlp {
     Bf16Mat dzb[2], dzbt[2];
     Bf16Mat dzb_out, dzbt_out;           // dz of the logit layer (one column)
     float *dz_out = nullptr, *rowloss = nullptr, *loss = nullptr;
+    float *ws = nullptr;                 // split-K partial weight gradients
+    int ksplit = 1;                      // K (batch) splits of the weight gradients
     int *err = nullptr;
     int cap = 0;
     long long step = 0;
@@ -479,7 +519,7 @@ void free_acts(lenia_mlp *m)
     }
     free_mat(m->dzb_out);
     free_mat(m->dzbt_out);
-    float **bufs[] = {&m->dz_out, &m->rowloss};
+    float **bufs[] = {&m->dz_out, &m->rowloss, &m->ws};
     for (float **p : bufs) {
         if (*p) cudaFree(*p);
         *p = nullptr;
@@ -510,6 +550,13 @@ cudaError_t ensure_batch(lenia_mlp *m, int B)
     if (e == cudaSuccess) e = alloc_mat(m->dzbt_out, 1, cap);
     if (e == cudaSuccess) e = cudaMalloc((void **)&m->dz_out, sizeof(float) * (size_t)cap);
     if (e == cudaSuccess) e = cudaMalloc((void **)&m->rowloss, sizeof(float) * (size_t)cap);
+    // the weight gradients reduce over the batch: about 256 batch rows per CTA
+    // row, at most 64 CTA rows
+    m->ksplit = std::max(1, std::min(64, cap / 256));
+    int widest = 0;
+    for (int l = 0; l < kMlpLayers; l++) widest = std::max(widest, m->dims[l] * m->dims[l + 1]);
+    if (e == cudaSuccess && m->ksplit > 1)
+        e = cudaMalloc((void **)&m->ws, sizeof(float) * (size_t)m->ksplit * widest);
     if (e == cudaSuccess) m->cap = cap;
     return e;
 }
@@ -701,7 +748,7 @@ lenia_status lenia_mlp_gradients(lenia_mlp *m, const float *x, const float *y, i
         gw.c32 = m->grads + m->woff[l];
         gw.ldc = K;
         gw.err = m->err;
-        e = tc_gemm(dzbt, N, inT, K, B, gw, st);
+        e = tc_gemm(dzbt, N, inT, K, B, gw, st, std::min(m->ksplit, std::max(1, B / 256)), m->ws);
         if (e == cudaSuccess) {
             k_colsum<<<(N + 255) / 256, 256, 0, st>>>(dz, B, N, m->grads + m->boff[l]);
             e = cudaGetLastError();

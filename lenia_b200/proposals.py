@@ -169,9 +169,57 @@ def score(net, mu, sd, features: np.ndarray):
     return out["z"].cpu().numpy(), t
 
 
+def single_statistic_rule(features: np.ndarray, hits: np.ndarray):
+    """The non-learned early filter: among the 16 step-50 statistics (the
+    columns after the 63 kernel parameters), the one whose ranking (either
+    sign) best separates the training hits, by rank AUC.  Returns (column,
+    sign, training AUC)."""
+    best = (N_KERNELS * KERNEL_FEATURES, 1.0, 0.5)
+    if hits.all() or not hits.any():
+        return best
+    for col in range(N_KERNELS * KERNEL_FEATURES, features.shape[1]):
+        a = ranking_auc(features[:, col], hits)
+        for sign, auc in ((1.0, a), (-1.0, 1.0 - a)):
+            if auc > best[2]:
+                best = (col, sign, auc)
+    return best
+
+
+def ranking_auc(score: np.ndarray, hits: np.ndarray):
+    """Probability that a random hit scores above a random non-hit (ties
+    count half); None without both classes."""
+    if hits.all() or not hits.any():
+        return None
+    order = np.argsort(score, kind="stable")
+    ranks = np.empty(len(score))
+    ranks[order] = np.arange(len(score))
+    # average ranks of ties
+    s_sorted = score[order]
+    i = 0
+    while i < len(s_sorted):
+        j = i
+        while j + 1 < len(s_sorted) and s_sorted[j + 1] == s_sorted[i]:
+            j += 1
+        if j > i:
+            ranks[order[i:j + 1]] = (i + j) / 2.0
+        i = j + 1
+    npos, nneg = int(hits.sum()), int((~hits).sum())
+    return float((ranks[hits].sum() - npos * (npos - 1) / 2.0) / (npos * nneg))
+
+
 def study(n_train: int = 4096, n_test: int = 2048, width: int = 32, observe: int = 50, final: int = 400,
           keep: float = 0.2, seed: int = 17) -> Dict:
-    """The whole comparison; returns its numbers (GPU seconds, hits, rates)."""
+    """The whole comparison; returns its numbers (GPU seconds, hits, rates).
+
+    Four arms on the same test candidates, each timed on the GPU: uniform
+    (every candidate to the final step) and three early filters that run
+    every candidate to the observation step and continue the same number of
+    them, `keep` of the test set, from their saved states: the network's top
+    scores (learned), a uniform random choice (random), and the top of the
+    single step-50 statistic that best separates the training hits
+    (statistic).  Every continued run is the plain simulation of its
+    candidate; a hit of a filtered arm counts only when that run ends
+    persistent."""
     t0 = time.time()
     tr = simulate(candidates(n_train, seed, width), observe, final)
     net, mu, sd, t_train = train(tr.features, tr.hits, seed=seed)
@@ -179,34 +227,48 @@ def study(n_train: int = 4096, n_test: int = 2048, width: int = 32, observe: int
     te = simulate(test_wls, observe, final, keep_states=True)
     z, t_score = score(net, mu, sd, te.features)
     k = max(1, int(round(keep * n_test)))
-    chosen = np.argsort(-z, kind="stable")[:k]
-    labels_cont, t_cont = continue_runs([test_wls[i] for i in chosen], [te.states[i] for i in chosen],
-                                        te.init_totals[chosen], observe, final)
-    # the continued runs are the plain simulation of each chosen candidate
-    confirmed = labels_cont == "persistent"
-    agree = bool(np.all(labels_cont == te.labels[chosen]))
+    col, sign, stat_auc_train = single_statistic_rule(tr.features, tr.hits)
+    rng = np.random.default_rng(seed + 2)
+    picks = {
+        "learned": np.argsort(-z, kind="stable")[:k],
+        "random": np.sort(rng.choice(n_test, size=k, replace=False)),
+        "statistic": np.argsort(-sign * te.features[:, col], kind="stable")[:k],
+    }
     t_uniform = te.t_observe + te.t_finish
-    t_learned = te.t_observe + t_score + t_cont
-    hits_u, hits_l = int(te.hits.sum()), int(confirmed.sum())
+    hits_u = int(te.hits.sum())
     rate_u = hits_u / t_uniform
-    rate_l = hits_l / t_learned
-    order = np.argsort(-z)
-    auc_pairs = None
-    if 0 < hits_u < n_test:
-        ranks = np.empty(n_test)
-        ranks[order] = np.arange(n_test)
-        pos_r = ranks[te.hits]
-        auc_pairs = float(np.mean([(ranks[~te.hits] > r).mean() for r in pos_r]))
+    arms = {"uniform": {"hits": hits_u, "gpu_s": t_uniform, "hits_per_gpu_hour": 3600 * rate_u}}
+    agree = True
+    for name, chosen in picks.items():
+        labels_cont, t_cont = continue_runs([test_wls[i] for i in chosen], [te.states[i] for i in chosen],
+                                            te.init_totals[chosen], observe, final)
+        # the continued runs are the plain simulation of each chosen candidate
+        confirmed = labels_cont == "persistent"
+        agree = agree and bool(np.all(labels_cont == te.labels[chosen]))
+        t_arm = te.t_observe + t_cont + (t_score if name == "learned" else 0.0)
+        h = int(confirmed.sum())
+        arms[name] = {"hits": h, "gpu_s": t_arm, "hits_per_gpu_hour": 3600 * h / t_arm,
+                      "ratio_to_uniform": (h / t_arm) / rate_u if rate_u > 0 else None}
+    # the learned arm charged with its training: the label simulation and the
+    # network's training, spread over this one test set
+    t_learn_all = arms["learned"]["gpu_s"] + tr.t_observe + tr.t_finish + t_train
+    arms["learned"]["hits_per_gpu_hour_with_training"] = 3600 * arms["learned"]["hits"] / t_learn_all
     return {
         "candidates": {"train": n_train, "test": n_test, "width": width, "observe": observe, "final": final,
                        "keep_fraction": keep},
         "train_hit_rate": float(tr.hits.mean()), "test_hit_rate": float(te.hits.mean()),
         "gpu_s": {"train_simulation": tr.t_observe + tr.t_finish, "train_network": t_train,
-                  "uniform": t_uniform, "learned": t_learned, "score": t_score, "continue": t_cont},
-        "hits": {"uniform": hits_u, "learned": hits_l, "learned_confirmed_equal_uniform_labels": agree},
-        "hits_per_gpu_hour": {"uniform": 3600 * rate_u, "learned": 3600 * rate_l,
-                              "ratio": rate_l / rate_u if rate_u > 0 else None},
-        "ranking_auc": auc_pairs,
+                  "uniform": t_uniform, "learned": arms["learned"]["gpu_s"], "score": t_score},
+        "hits": {"uniform": hits_u, "learned": arms["learned"]["hits"],
+                 "learned_confirmed_equal_uniform_labels": agree},
+        "hits_per_gpu_hour": {"uniform": arms["uniform"]["hits_per_gpu_hour"],
+                              "learned": arms["learned"]["hits_per_gpu_hour"],
+                              "ratio": arms["learned"]["ratio_to_uniform"]},
+        "arms": arms,
+        "statistic_rule": {"column": int(col), "statistic": int(col - N_KERNELS * KERNEL_FEATURES),
+                           "sign": sign, "train_auc": stat_auc_train,
+                           "test_auc": ranking_auc(sign * te.features[:, col], te.hits)},
+        "ranking_auc": ranking_auc(z, te.hits),
         "wall_s": time.time() - t0,
     }
 

@@ -111,3 +111,6 @@ def test_proposal_study_runs_end_to_end():
     assert res["hits"]["learned_confirmed_equal_uniform_labels"]
     assert res["gpu_s"]["learned"] < res["gpu_s"]["uniform"]
     assert 0.0 <= res["test_hit_rate"] <= 1.0
+    # the two non-learned early filters continue as many candidates
+    for arm in ("random", "statistic"):
+        assert arm in res["arms"] and res["arms"][arm]["gpu_s"] < res["gpu_s"]["uniform"]
