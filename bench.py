@@ -452,6 +452,20 @@ def batch_measure(args, rank, n, stream, barrier, max_over_ranks):
     ms = max_over_ranks(e0.elapsed_time(e1)) / steps
     b.sync()
     launches = b.launches_per_step()
+    grouped = b.grouped_worlds()
+    # the same batch with every world on its own launches (the lanes), for
+    # comparison; the fields are the same either way
+    b.set_batched_launches(False)
+    b.set_stream(stream.cuda_stream)
+    b.step(2)
+    barrier()
+    e0.record(stream)
+    b.step(steps)
+    e1.record(stream)
+    barrier()
+    lanes_ms = max_over_ranks(e0.elapsed_time(e1)) / steps
+    lanes_launches = b.launches_per_step()
+    b.sync()
     b.close()
     plain = sub[:min(64, len(sub))]
     ws = []
@@ -472,11 +486,20 @@ def batch_measure(args, rank, n, stream, barrier, max_over_ranks):
     for w in ws:
         w.close()
     cells = sum(wl.desc.width ** 3 * wl.desc.channels for wl in wls)
-    return {"workload": f"{args.batch_worlds} worlds, sides 24-96 (config 3 mix), 3 channels, 9 kernels, "
+    # the whole-step byte model summed over the batch's worlds, against the
+    # measured copy bandwidth
+    peak, peak_kind = measured_peaks()
+    step_bytes = sum(step_bytes_per_cell(wl) * wl.desc.width ** 2 * wl.desc.height for wl in wls)
+    return {
+            "step_roofline": {"bytes_per_step": step_bytes, "achieved": step_bytes / (ms / 1000.0) / 1e9 / n,
+                              "peak": peak, "peak_kind": peak_kind, "unit": "GB/s per GPU",
+                              "frac": step_bytes / (ms / 1000.0) / 1e9 / n / peak},"workload": f"{args.batch_worlds} worlds, sides 24-96 (config 3 mix), 3 channels, 9 kernels, "
                         f"RT or advection per world, sharded over {n} GPU(s)",
             "world_steps_per_s": args.batch_worlds / (ms / 1000.0), "ms_per_step": ms,
             "cell_updates_per_s": cells / (ms / 1000.0), "graph_launches_per_step": 1,
-            "gpu_launches_per_step": launches,
+            "gpu_launches_per_step": launches, "worlds_in_batched_launches": grouped * n,
+            "per_world_launches": {"world_steps_per_s": args.batch_worlds / (lanes_ms / 1000.0),
+                                   "ms_per_step": lanes_ms, "gpu_launches_per_step": lanes_launches},
             "plain_world_steps_per_s_per_gpu": len(ws) / (plain_ms / 1000.0),
             "plain_sample_worlds": len(ws), "autotune_by_side": choices}
 

@@ -278,10 +278,17 @@ lenia_status lenia_load(const char *path, lenia_world **out, unsigned long long 
  * modes) stepped together: the reference has no counterpart beyond calling
  * its step once per world.  Each world keeps only the fields that live from
  * step to step (A, V, GA, SUM); the buffers of one step belong to a lane, a
- * stream whose worlds run one after another, and lanes run concurrently.  One
- * step of every world is captured once into a CUDA graph and replayed, so a
- * batch step is one graph launch.  Every world computes exactly what a world
- * of lenia_create computes (bit-identical fields). */
+ * stream whose worlds run one after another, and lanes run concurrently.
+ * Worlds that qualify (cubic grids of 24 .. 96 cells per side, FFT
+ * convolution, no debug outputs, snapshots, mass conservation, blur, F or
+ * ALPHA, transport by the dd = 1 gather or per cell) are instead stepped by
+ * batched launches: per stage one launch per grid size (the transforms) or
+ * one launch for all of them (growth from u_k, flow, transport), whose
+ * blocks each take one block of one world from a device work list, in waves
+ * whose per-step buffers share one scratch pool of at most 12 GB.  One step
+ * of every world is captured once into a CUDA graph and replayed, so a batch
+ * step is one graph launch.  Every world computes exactly what a world of
+ * lenia_create computes (bit-identical fields). */
 typedef struct lenia_batch lenia_batch;
 
 /* descs[n_worlds]; kernels: every world's kernels one after another,
@@ -309,6 +316,13 @@ lenia_status lenia_batch_sync(lenia_batch *b);
 lenia_status lenia_batch_autotune(lenia_batch *b, int modes, LeniaTuneResult *per_world);
 /* Kernel launches one batch step contains (all worlds). */
 int lenia_batch_launches_per_step(const lenia_batch *b);
+/* No counterpart in the reference.  on = 0 steps every world through its own
+ * launches on the lanes, on = 1 (the default) lets the worlds that qualify
+ * take the batched launches; the step graphs are captured again.  The fields
+ * are the same either way.  Synchronous. */
+lenia_status lenia_batch_set_batched_launches(lenia_batch *b, int on);
+/* Worlds the batched launches step (the rest run on the lanes). */
+int lenia_batch_grouped_worlds(const lenia_batch *b);
 const char *lenia_batch_last_error(const lenia_batch *b);
 
 /* ---- Statistics for labelling runs --------------------------------------

@@ -182,6 +182,8 @@ def load() -> ctypes.CDLL:
         "lenia_batch_sync": ([P], ctypes.c_int),
         "lenia_batch_autotune": ([P, ctypes.c_int, ctypes.POINTER(LeniaTuneResult)], ctypes.c_int),
         "lenia_batch_launches_per_step": ([P], ctypes.c_int),
+        "lenia_batch_set_batched_launches": ([P, ctypes.c_int], ctypes.c_int),
+        "lenia_batch_grouped_worlds": ([P], ctypes.c_int),
         "lenia_world_stats": ([P, ctypes.c_float, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
         "lenia_batch_stats": ([P, ctypes.c_float, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
         "lenia_batch_last_error": ([P], ctypes.c_char_p),

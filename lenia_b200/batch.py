@@ -2,8 +2,10 @@
 partition of a batch across GPUs.
 
 `Batch` steps many worlds of mixed sizes, channels, kernel sets and modes
-with one CUDA-graph launch per step; each world's fields are bit-identical
-to those of a `World` stepped alone.  `shard_worlds` splits a batch across
+with one CUDA-graph launch per step (inside it, batched launches that each
+cover many worlds through device work lists, and per-world launches for the
+worlds those do not take); each world's fields are bit-identical to those of
+a `World` stepped alone.  `shard_worlds` splits a batch across
 ranks (one process per GPU): worlds are independent, so the ranks exchange
 nothing while stepping.
 """
@@ -131,3 +133,13 @@ class Batch:
 
     def launches_per_step(self) -> int:
         return int(self._lib.lenia_batch_launches_per_step(self._h))
+
+    def set_batched_launches(self, on: bool = True) -> None:
+        """Batched launches (one per stage and grid size over the worlds that
+        qualify) on or off; off steps every world through its own launches.
+        The fields are the same either way."""
+        self._check(self._lib.lenia_batch_set_batched_launches(self._h, 1 if on else 0))
+
+    def grouped_worlds(self) -> int:
+        """Worlds stepped by the batched launches."""
+        return int(self._lib.lenia_batch_grouped_worlds(self._h))

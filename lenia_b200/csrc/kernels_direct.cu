@@ -535,21 +535,17 @@ __device__ __forceinline__ float growth_value(const GrowthJobs &jobs, const floa
     return l;
 }
 
-// The kernels grouped by target channel c1, in kernel order within a group.
-struct ChannelOrder {
-    int k[kMaxKernels];
-};
-
 // One channel at a time: its kernels' growth and u summed in kernel order
 // (the additions of the all-channel form, so the fields are identical), then
 // its H, U_SUM and BACK written; only one channel's sums are live.
 // Five blocks of 256 per SM (48 registers, no spills).
-__global__ void __launch_bounds__(256, 5)
-    k_growth_from_u(Dims d, GrowthJobs jobs, ChannelOrder ord, const float *__restrict__ lut_rows,
-                    const float *__restrict__ U, const float *__restrict__ A, float *__restrict__ Hout,
-                    float *__restrict__ Uout, float *__restrict__ BACK, int *err_flag)
+__device__ __forceinline__ void growth_from_u_body(const Dims &d, const GrowthJobs &jobs, const ChannelOrder &ord,
+                                                   const float *__restrict__ lut_rows, const float *__restrict__ U,
+                                                   const float *__restrict__ A, float *__restrict__ Hout,
+                                                   float *__restrict__ Uout, float *__restrict__ BACK, int *err_flag,
+                                                   long long block)
 {
-    const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const long long i = (block * blockDim.x + threadIdx.x) * 4;
     if (i >= d.N) return;
     int bad = 0;
     // u of the next two kernels (in channel order) is loaded ahead of the
@@ -598,6 +594,25 @@ __global__ void __launch_bounds__(256, 5)
         }
     }
     if (bad && err_flag) atomicOr(err_flag, 1);
+}
+
+__global__ void __launch_bounds__(256, 5)
+    k_growth_from_u(const __grid_constant__ Dims d, const __grid_constant__ GrowthJobs jobs,
+                    const __grid_constant__ ChannelOrder ord, const float *__restrict__ lut_rows,
+                    const float *__restrict__ U, const float *__restrict__ A, float *__restrict__ Hout,
+                    float *__restrict__ Uout, float *__restrict__ BACK, int *err_flag)
+{
+    growth_from_u_body(d, jobs, ord, lut_rows, U, A, Hout, Uout, BACK, err_flag, blockIdx.x);
+}
+
+// The same over a batch of worlds: block b of the launch is block
+// items[b].block of world items[b].world's own launch.
+__global__ void __launch_bounds__(256, 5) k_growth_from_u_multi(const BatchWorldDev *__restrict__ ws,
+                                                                const WorkItem *__restrict__ items)
+{
+    const WorkItem it = items[blockIdx.x];
+    const BatchWorldDev &w = ws[it.world];
+    growth_from_u_body(w.p.d, w.gj, w.ord, w.lut_rows, w.U, w.A, w.H, w.U_SUM, w.BACK, w.err, it.block);
 }
 
 int round_up(int v, int m) { return (v + m - 1) / m * m; }
@@ -860,12 +875,10 @@ size_t direct_smem(const DirectConv *dc) { return dc->smem; }
 int direct_stages(const DirectConv *dc) { return dc->ns; }
 int direct_radius(const DirectConv *dc) { return dc->R; }
 
-cudaError_t launch_growth_from_u(const Dims &d, const GrowthJobs &jobs, const float *lut_rows, const float *U,
-                                 const float *A, float *H, float *U_SUM, float *BACK, int *err_flag, cudaStream_t st)
+// Stable grouping of the kernels by target channel; kernels aimed past the
+// last channel go last and, as in the all-channel form, reach no output.
+ChannelOrder channel_order(const GrowthJobs &jobs)
 {
-    const long long threads = d.N / 4;  // N is a multiple of 4 (the width is)
-    // stable grouping by target channel; kernels aimed past the last channel
-    // go last and, as in the all-channel form, reach no output
     ChannelOrder ord{};
     int n = 0;
     for (int c = 0; c <= kMaxChannels; c++)
@@ -873,8 +886,25 @@ cudaError_t launch_growth_from_u(const Dims &d, const GrowthJobs &jobs, const fl
             const int t = jobs.c1[k] >= 0 && jobs.c1[k] < kMaxChannels ? jobs.c1[k] : kMaxChannels;
             if (t == c) ord.k[n++] = k;
         }
-    k_growth_from_u<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(d, jobs, ord, lut_rows, U, A, H, U_SUM, BACK,
-                                                                      err_flag);
+    return ord;
+}
+
+// 256 threads of four cells each (N is a multiple of 4: the width is).
+int growth_from_u_blocks(const Dims &d) { return (int)((d.N / 4 + 255) / 256); }
+
+cudaError_t launch_growth_from_u(const Dims &d, const GrowthJobs &jobs, const float *lut_rows, const float *U,
+                                 const float *A, float *H, float *U_SUM, float *BACK, int *err_flag, cudaStream_t st)
+{
+    const ChannelOrder ord = channel_order(jobs);
+    k_growth_from_u<<<(unsigned)growth_from_u_blocks(d), 256, 0, st>>>(d, jobs, ord, lut_rows, U, A, H, U_SUM, BACK,
+                                                                       err_flag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_growth_from_u_multi(const BatchWorldDev *ws, const WorkItem *items, int n_items, cudaStream_t st)
+{
+    if (n_items == 0) return cudaSuccess;
+    k_growth_from_u_multi<<<(unsigned)n_items, 256, 0, st>>>(ws, items);
     return cudaGetLastError();
 }
 

@@ -66,19 +66,36 @@ __device__ __forceinline__ bool gb_source(const Dims &d, int border, int &x, int
 // Torus/wall halo faces of a staged tile (the TMA copy left zeros there).
 // Only the cells the gradients read are patched: x0-1..x0+32, y0-1..y0+8,
 // z0-1..z0+kFlowZ, with exactly one coordinate one step outside the grid.
+// Each grid face the staged box reaches is walked over its in-grid cells
+// (edges and corners keep the copy's zeros), so a block patches at most a
+// few hundred cells per field instead of testing its whole box.
 __device__ void patch_faces(float *tile, const float *f, const Dims &d, int border, int x0, int y0, int z0)
 {
     const int tid = threadIdx.x + threadIdx.y * kFX;
-    constexpr int RX = kFX + 2, RY = kTY, RZ = kTZ;
-    for (int e = tid; e < RX * RY * RZ; e += kFX * kFY) {
-        const int rx = e % RX, ry = (e / RX) % RY, rz = e / (RX * RY);
-        int x = x0 - 1 + rx, y = y0 - 1 + ry, z = z0 - 1 + rz;
-        const int ox = (x < 0) | (x >= d.W), oy = (y < 0) | (y >= d.H), oz = (z < 0) | (z >= d.D);
-        if (ox + oy + oz != 1) continue;
-        if (x < -1 || x > d.W || y < -1 || y > d.H || z < -1 || z > d.D) continue;
-        const int t = (rx + 3) + ry * kTX + rz * kTX * kTY;
-        tile[t] = gb_source(d, border, x, y, z) ? __ldg(f + x + y * d.W + z * d.W * d.H) : 0.0f;
-    }
+    const int lo[3] = {x0 - 1, y0 - 1, z0 - 1};
+    const int hi[3] = {x0 + kFX, y0 + kFY, z0 + kFlowZ};  // inclusive
+    const int ext[3] = {d.W, d.H, d.D};
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+            const int g = side == 0 ? -1 : ext[a];  // the face layer outside the grid
+            if (g < lo[a] || g > hi[a]) continue;
+            const int a1 = a == 0 ? 1 : 0, a2 = a == 2 ? 1 : 2;
+            const int l1 = lo[a1] > 0 ? lo[a1] : 0, h1 = hi[a1] < ext[a1] - 1 ? hi[a1] : ext[a1] - 1;
+            const int l2 = lo[a2] > 0 ? lo[a2] : 0, h2 = hi[a2] < ext[a2] - 1 ? hi[a2] : ext[a2] - 1;
+            const int n1 = h1 - l1 + 1, n2 = h2 - l2 + 1;
+            if (n1 <= 0 || n2 <= 0) continue;
+            for (int e = tid; e < n1 * n2; e += kFX * kFY) {
+                int c[3];
+                c[a] = g;
+                c[a1] = l1 + e % n1;
+                c[a2] = l2 + e / n1;
+                const int t = (c[0] - x0 + 4) + (c[1] - y0 + 1) * kTX + (c[2] - z0 + 1) * kTX * kTY;
+                int x = c[0], y = c[1], z = c[2];
+                tile[t] = gb_source(d, border, x, y, z) ? __ldg(f + x + y * d.W + z * d.W * d.H) : 0.0f;
+            }
+        }
 }
 
 // True when any staged value is infinite, NaN or so large that a Sobel
@@ -86,9 +103,14 @@ __device__ void patch_faces(float *tile, const float *f, const Dims &d, int bord
 // multiply-then-add path.
 __device__ __forceinline__ bool tile_unsafe(const float *tile)
 {
+    static_assert(kTile % 4 == 0 && (kTile * 4) % 16 == 0, "tiles are read as float4");
     const int tid = threadIdx.x + threadIdx.y * kFX;
+    const float4 *t4 = reinterpret_cast<const float4 *>(tile);
     int bad = 0;
-    for (int e = tid; e < kTile; e += kFX * kFY) bad |= !(fabsf(tile[e]) < 1.0e30f);
+    for (int e = tid; e < kTile / 4; e += kFX * kFY) {
+        const float4 v = t4[e];
+        bad |= !(fabsf(v.x) < 1.0e30f) | !(fabsf(v.y) < 1.0e30f) | !(fabsf(v.z) < 1.0e30f) | !(fabsf(v.w) < 1.0e30f);
+    }
     return __syncthreads_or(bad) != 0;
 }
 
@@ -145,24 +167,29 @@ __device__ __forceinline__ void load_plane(const float *tile, int c, float (&v)[
         for (int dx = -1; dx <= 1; dx++) v[(dy + 1) * 3 + dx + 1] = tile[c + dx + dy * kTX];
 }
 
-__global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p, FlowBuffers b,
-                                                   const __grid_constant__ CUtensorMap tm_sum,
-                                                   const __grid_constant__ CUtensorMap tm_h)
+// The block (bx, by) of a world's flow launch: bx over the x-y tiles, by
+// over the z tiles (OWN_GRID: the launch's own blockIdx, read where used).
+// tm_sum / tm_h: the world's tensor maps (kernel parameters, or a batch's
+// world table in global memory).
+template <bool OWN_GRID>
+__device__ __forceinline__ void flow_body(const StepParams &p, const FlowBuffers &b, const CUtensorMap *tm_sum,
+                                          const CUtensorMap *tm_h, int bx_arg, int by_arg)
 {
+    const int bx = OWN_GRID ? (int)blockIdx.x : bx_arg, by = OWN_GRID ? (int)blockIdx.y : by_arg;
     extern __shared__ __align__(128) float flow_smem[];
     __shared__ __align__(8) uint64_t bars[2];
-    float *const tiles[2] = {flow_smem, flow_smem + kTile};
     const Dims &d = p.d;
     const int C = p.C;
     const int N = d.N;
     const int tx = threadIdx.x, ty = threadIdx.y;
     const bool leader = tx == 0 && ty == 0;
     const int tiles_x = (d.W + kFX - 1) / kFX;
-    const int x0 = (blockIdx.x % tiles_x) * kFX;
-    const int y0 = (blockIdx.x / tiles_x) * kFY;
-    const int z0 = blockIdx.y * kFlowZ;
+    const int x0 = (bx % tiles_x) * kFX;
+    const int y0 = (bx / tiles_x) * kFY;
+    const int z0 = by * kFlowZ;
     const int x = x0 + tx, y = y0 + ty;
     const bool col_in = x < d.W && y < d.H;
+    const float posx = (float)x + 0.5f, posy = (float)y + 0.5f, posz0 = (float)z0 + 0.5f;
     const int sobel = p.gradient_mode == kGradSobel;
     const float ta = p.theta_a;
     const bool patch = p.sobel_border != kBorderNone &&
@@ -182,8 +209,8 @@ __global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p
         const int buf = f & 1;
         fence_proxy_async();
         mbar_arrive_expect_tx(&bars[buf], kTile * 4);
-        if (f == 0) tma_load_3d(tiles[buf], &tm_sum, x0 - 4, y0 - 1, z0 - 1, &bars[buf]);
-        else tma_load_4d(tiles[buf], &tm_h, x0 - 4, y0 - 1, z0 - 1, f - 1, &bars[buf]);
+        if (f == 0) tma_load_3d(flow_smem + buf * kTile, tm_sum, x0 - 4, y0 - 1, z0 - 1, &bars[buf]);
+        else tma_load_4d(flow_smem + buf * kTile, tm_h, x0 - 4, y0 - 1, z0 - 1, f - 1, &bars[buf]);
     };
 
     // Waits for field f's tile, patches its faces and decides the path:
@@ -191,7 +218,7 @@ __global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p
     // wait ran out (block-wide): the timeout is recorded and the copies in
     // flight (fields f and f + 1) are drained; the block then returns.
     auto land = [&](int f) -> int {
-        float *tile = tiles[f & 1];
+        float *tile = flow_smem + (f & 1) * kTile;
         if (!block_wait(&bars[f & 1], (unsigned)(f >> 1) & 1u, p.wait_polls)) {
             mbar_wait(&bars[f & 1], (unsigned)(f >> 1) & 1u, kDrainPolls);
             if (f + 1 <= C) mbar_wait(&bars[(f + 1) & 1], (unsigned)((f + 1) >> 1) & 1u, kDrainPolls);
@@ -242,7 +269,7 @@ __global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p
         float win[3][9];
 #pragma unroll
         for (int lz = 0; lz < kFlowZ; lz++) {
-            grad(tiles[0], literal, lz, win, na[lz]);
+            grad(flow_smem, literal, lz, win, na[lz]);
             const int z = z0 + lz;
             if (b.NA && col_in && z < d.D) {
                 const int i = x + y * d.W + z * d.W * d.H;
@@ -256,7 +283,7 @@ __global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p
     }
     // fields 1..C: the gradient of H channel c = f - 1 and the flow epilogue
     for (int f = 1; f <= C; f++) {
-        float *tile = tiles[f & 1];
+        float *tile = flow_smem + (f & 1) * kTile;
         if (f < C) issue(f + 1);
         // per-cell inputs of this channel, loaded while the tile lands
         float v3[3][kFlowZ], gal[kFlowZ];
@@ -331,7 +358,8 @@ __global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p
                 for (int q = 0; q < 3; q++) b.F[q * C * N + ci] = f3[q];
             }
             float vv[3] = {v3[0][lz], v3[1][lz], v3[2][lz]};
-            const float pos[3] = {(float)x + 0.5f, (float)y + 0.5f, (float)z + 0.5f};
+            // (float)z + 0.5f, exactly: every term is a small whole or half number
+            const float pos[3] = {posx, posy, posz0 + (float)lz};
             if (p.mu_vel) {
 #pragma unroll
                 for (int q = 0; q < 3; q++) vv[q] = (vv[q] + f3[q]) * p.v_damp;
@@ -360,6 +388,57 @@ __global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p
         fence_proxy_async();
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p, FlowBuffers b,
+                                                   const __grid_constant__ CUtensorMap tm_sum,
+                                                   const __grid_constant__ CUtensorMap tm_h)
+{
+    flow_body<true>(p, b, &tm_sum, &tm_h, 0, 0);
+}
+
+// Copies a world's parameter block into shared memory (whole 4-byte words).
+template <typename T>
+__device__ __forceinline__ void copy_to_shared(T *dst, const T *src)
+{
+    static_assert(sizeof(T) % 4 == 0, "copied as 4-byte words");
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int nthr = blockDim.x * blockDim.y;
+    for (int i = tid; i < (int)(sizeof(T) / 4); i += nthr)
+        reinterpret_cast<unsigned *>(dst)[i] = reinterpret_cast<const unsigned *>(src)[i];
+}
+
+// A tensor map written to global memory before the launch, made visible to
+// the copy engine's reads of it.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap *m)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(m) : "memory");
+}
+
+// The flow of a batch of worlds: block b is block items[b].block of world
+// items[b].world's own launch (x-y tile fastest); the world's parameters
+// are read into shared memory first.
+__global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow_multi(const BatchWorldDev *__restrict__ ws,
+                                                                         const WorkItem *__restrict__ items)
+{
+    __shared__ StepParams sp;
+    __shared__ FlowBuffers sb;
+    const WorkItem it = items[blockIdx.x];
+    const BatchWorldDev *w = ws + it.world;
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        // the copy engine's descriptor reads start while the parameters load
+        asm volatile("prefetch.tensormap [%0];\n" ::"l"(&w->tm_sum) : "memory");
+        asm volatile("prefetch.tensormap [%0];\n" ::"l"(&w->tm_h) : "memory");
+    }
+    copy_to_shared(&sp, &w->p);
+    copy_to_shared(&sb, &w->fb);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        tensormap_acquire(&w->tm_sum);
+        tensormap_acquire(&w->tm_h);
+    }
+    const int gx = w->flow_gx;
+    __syncthreads();
+    flow_body<false>(sp, sb, &w->tm_sum, &w->tm_h, it.block % gx, it.block / gx);
 }
 
 namespace {
@@ -410,16 +489,42 @@ cudaError_t encode_tensor_map(CUtensorMap *map, const float *base, int rank, con
     return encode_tensor_map_typed(map, base, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (int)sizeof(float), rank, dims, box);
 }
 
-cudaError_t launch_flow(const StepParams &p, const FlowBuffers &b, cudaStream_t st)
+int flow_blocks(const Dims &d, int *gx)
+{
+    const int tiles_x = (d.W + kFX - 1) / kFX, tiles_y = (d.H + kFY - 1) / kFY;
+    if (gx) *gx = tiles_x * tiles_y;
+    return tiles_x * tiles_y * ((d.D + kFlowZ - 1) / kFlowZ);
+}
+
+cudaError_t launch_flow_multi(const BatchWorldDev *ws, const WorkItem *items, int n_items, cudaStream_t st)
+{
+    if (n_items == 0) return cudaSuccess;
+    const size_t smem = 2 * kTile * sizeof(float);
+    cudaError_t e = cudaFuncSetAttribute(k_flow_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_flow_multi<<<(unsigned)n_items, dim3(kFX, kFY), smem, st>>>(ws, items);
+    return cudaGetLastError();
+}
+
+// The flow launch's tensor maps: SUM (x, y, z) and H (x, y, z, channel),
+// tiles of 40 x 10 x (kFlowZ + 2).
+cudaError_t flow_tensor_maps(const StepParams &p, const FlowBuffers &b, CUtensorMap *tm_sum, CUtensorMap *tm_h)
 {
     const Dims &d = p.d;
-    CUtensorMap tm_sum, tm_h;
     const unsigned long long dsum[3] = {(unsigned long long)d.W, (unsigned long long)d.H, (unsigned long long)d.D};
     const unsigned long long dh[4] = {(unsigned long long)d.W, (unsigned long long)d.H, (unsigned long long)d.D,
                                       (unsigned long long)p.C};
     const unsigned box[4] = {kTX, kTY, kTZ, 1};
-    cudaError_t e = encode_tensor_map(&tm_sum, b.SUM, 3, dsum, box);
-    if (e == cudaSuccess) e = encode_tensor_map(&tm_h, b.H, 4, dh, box);
+    cudaError_t e = encode_tensor_map(tm_sum, b.SUM, 3, dsum, box);
+    if (e == cudaSuccess) e = encode_tensor_map(tm_h, b.H, 4, dh, box);
+    return e;
+}
+
+cudaError_t launch_flow(const StepParams &p, const FlowBuffers &b, cudaStream_t st)
+{
+    const Dims &d = p.d;
+    CUtensorMap tm_sum, tm_h;
+    cudaError_t e = flow_tensor_maps(p, b, &tm_sum, &tm_h);
     if (e != cudaSuccess) return e;
     const int tiles_x = (d.W + kFX - 1) / kFX, tiles_y = (d.H + kFY - 1) / kFY;
     dim3 grid(tiles_x * tiles_y, (d.D + kFlowZ - 1) / kFlowZ);

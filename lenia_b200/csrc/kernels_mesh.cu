@@ -275,29 +275,31 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_count(McGeom g, const McTable
     for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const CubeRef q = cube_of(g, chunk);
         const unsigned owned = q.valid ? s_tab.owned[boundary_class(g, q.gx, q.gy, q.gz, q.z0, q.z1)] : 0u;
-        unsigned prev[kMcMaxFields] = {0u, 0u, 0u};
         unsigned packed[LENIA_MAX_CHANNELS] = {0u, 0u, 0u, 0u};  // nt | nn << 16 per channel
+#pragma unroll 1
+        for (int f = 0; f < g.F; f++) {
+            // every channel's corners in flight at once, then the cases in
+            // channel order (a shared vertex belongs to the first channel
+            // that cuts its edge)
+            float v[LENIA_MAX_CHANNELS][8];
 #pragma unroll
-        for (int c = 0; c < LENIA_MAX_CHANNELS; c++) {
-            if (c >= g.C) break;
-            unsigned nt = 0, nn = 0;
+            for (int c = 0; c < LENIA_MAX_CHANNELS; c++)
+                if (c < g.C && q.valid) load_corners(g.fld[f] + c * g.N, g.halo[f] + c * g.N, g, q.gx, q.gy, q.gz, v[c]);
+            unsigned prev = 0u;
 #pragma unroll
-            for (int f = 0; f < kMcMaxFields; f++) {
-                if (f >= g.F) break;
+            for (int c = 0; c < LENIA_MAX_CHANNELS; c++) {
+                if (c >= g.C) break;
                 int cs = 0;
                 if (q.valid) {
-                    float v[8];
-                    load_corners(g.fld[f] + c * g.N, g.halo[f] + c * g.N, g, q.gx, q.gy, q.gz, v);
 #pragma unroll
-                    for (int i = 0; i < 8; i++) cs |= (v[i] > g.iso) << i;
+                    for (int i = 0; i < 8; i++) cs |= (v[c][i] > g.iso) << i;
                     cases[fc_off(g, f, c) + q.p] = (unsigned char)cs;
                 }
                 const unsigned act = active_edges(cs);
-                nt += tri_count(s_tab.tri[cs]);
-                nn += __popc(owned & act & ~prev[f]);
-                if (g.share) prev[f] |= act;
+                const unsigned nn = __popc(owned & act & ~prev);
+                if (g.share) prev |= act;
+                packed[c] += (unsigned)tri_count(s_tab.tri[cs]) | nn << 16;
             }
-            packed[c] = nt | nn << 16;
         }
         // block sums per channel (at most 5 triangles and 12 vertices per cube
         // and field: 16 bits per count hold a chunk)
@@ -322,16 +324,24 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_count(McGeom g, const McTable
 
 // Exclusive scan of the M packed chunk totals in place (one block of 1024
 // threads, tiles of 8192 with a running carry; each thread scans 8
-// consecutive values); totals[0..1] = triangles, vertices.  Packed addition
-// is exact while the triangle total stays below 2^32 (the host checks it).
+// consecutive values), and the list of chunk-channels with triangles, in
+// order; totals[0..2] = triangles, vertices, listed chunk-channels.  Packed
+// addition is exact while the triangle total stays below 2^32 (the host
+// checks it).
 constexpr int kScanThreads = 1024;
 constexpr int kScanPer = 8;
-__global__ void __launch_bounds__(kScanThreads) k_mc_scan(unsigned long long *blk, long long M, long long *totals)
+__global__ void __launch_bounds__(kScanThreads) k_mc_scan(unsigned long long *blk, long long M, long long *totals,
+                                                         long long *list)
 {
     __shared__ unsigned long long s_warp[kScanThreads / 32];
+    __shared__ unsigned s_lwarp[kScanThreads / 32];
     __shared__ unsigned long long s_carry;
+    __shared__ long long s_lcarry;
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-    if (t == 0) s_carry = 0;
+    if (t == 0) {
+        s_carry = 0;
+        s_lcarry = 0;
+    }
     __syncthreads();
     for (long long base = 0; base < M; base += (long long)kScanThreads * kScanPer) {
         unsigned long long v[kScanPer];
@@ -339,58 +349,74 @@ __global__ void __launch_bounds__(kScanThreads) k_mc_scan(unsigned long long *bl
 #pragma unroll
         for (int j = 0; j < kScanPer; j++) v[j] = i0 + j < M ? blk[i0 + j] : 0ull;
         unsigned long long sum = 0;
+        unsigned nz = 0;  // chunk-channels of this thread with triangles
 #pragma unroll
-        for (int j = 0; j < kScanPer; j++) sum += v[j];
-        // inclusive warp scan of the thread sums, then of the warp sums
+        for (int j = 0; j < kScanPer; j++) {
+            sum += v[j];
+            nz += (v[j] & 0xffffffffull) != 0;
+        }
+        // inclusive warp scans of the thread sums and counts, then of the
+        // warp sums
         unsigned long long x = sum;
+        unsigned xn = nz;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
+            const unsigned yn = __shfl_up_sync(0xffffffffu, xn, o);
+            if (lane >= o) {
+                x += y;
+                xn += yn;
+            }
         }
-        if (lane == 31) s_warp[wid] = x;
+        if (lane == 31) {
+            s_warp[wid] = x;
+            s_lwarp[wid] = xn;
+        }
         __syncthreads();
         if (wid == 0) {
             unsigned long long w = s_warp[lane];
+            unsigned wn = s_lwarp[lane];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= o) w += y;
+                const unsigned yn = __shfl_up_sync(0xffffffffu, wn, o);
+                if (lane >= o) {
+                    w += y;
+                    wn += yn;
+                }
             }
             s_warp[lane] = w;
+            s_lwarp[lane] = wn;
         }
         __syncthreads();
-        const unsigned long long carry = s_carry;
-        unsigned long long run = carry + (wid > 0 ? s_warp[wid - 1] : 0ull) + x - sum;
+        unsigned long long run = s_carry + (wid > 0 ? s_warp[wid - 1] : 0ull) + x - sum;
+        long long lrun = s_lcarry + (wid > 0 ? s_lwarp[wid - 1] : 0u) + xn - nz;
 #pragma unroll
         for (int j = 0; j < kScanPer; j++) {
-            if (i0 + j < M) blk[i0 + j] = run;
+            if (i0 + j < M) {
+                blk[i0 + j] = run;
+                if ((v[j] & 0xffffffffull) != 0) list[lrun++] = i0 + j;
+            }
             run += v[j];
         }
         __syncthreads();
-        if (t == kScanThreads - 1) s_carry = run;
+        if (t == kScanThreads - 1) {
+            s_carry = run;
+            s_lcarry = lrun;
+        }
         __syncthreads();
     }
     if (t == 0) {
         totals[0] = (long long)(s_carry & 0xffffffffull);
         totals[1] = (long long)(s_carry >> 32);
+        totals[2] = s_lcarry;
     }
-}
-
-// Triangles of chunk-channel o (blk holds the exclusive scan; the last one
-// ends at the total).
-__device__ __forceinline__ long long chunk_tris(const unsigned long long *blk, long long o, long long M,
-                                               const long long *totals)
-{
-    const long long beg = (long long)(blk[o] & 0xffffffffull);
-    const long long end = o + 1 < M ? (long long)(blk[o + 1] & 0xffffffffull) : totals[0];
-    return end - beg;
 }
 
 __global__ void __launch_bounds__(kMcThreads) k_mc_emit(McGeom g, const McTables *__restrict__ tab,
                                                        const unsigned char *__restrict__ cases,
                                                        const unsigned long long *__restrict__ blk,
-                                                       const long long *__restrict__ totals,
+                                                       const long long *__restrict__ list,
                                                        int *__restrict__ tri_base, int *__restrict__ vert_base,
                                                        float *__restrict__ fn, float *__restrict__ pos,
                                                        int *__restrict__ vch, unsigned long long *__restrict__ vsrc)
@@ -398,18 +424,14 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_emit(McGeom g, const McTables
     __shared__ McTables s_tab;
     __shared__ unsigned s_warp[kMcWarps];
     load_tables(tab, s_tab);
-    const int nchunks = g.slabs * g.nblk;
-    const long long M = (long long)g.slabs * g.C * g.nblk;
-    for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
-        const CubeRef q = cube_of(g, chunk);
+    // one chunk-channel with triangles per block (the other chunk-channels'
+    // cubes are all case 0 or 255: no edge is cut there)
+    {
+        const long long o = list[blockIdx.x];
+        const int c = (int)((o / g.nblk) % g.C);
+        const CubeRef q = cube_of(g, (int)(o / ((long long)g.nblk * g.C)) * g.nblk + (int)(o % g.nblk));
         const unsigned owned = q.valid ? s_tab.owned[boundary_class(g, q.gx, q.gy, q.gz, q.z0, q.z1)] : 0u;
-        unsigned prev[kMcMaxFields] = {0u, 0u, 0u};
-        for (int c = 0; c < g.C; c++) {
-            const long long o = ((long long)q.s * g.C + c) * g.nblk + q.b;
-            // a chunk-channel without triangles (the whole block takes the
-            // same branch) has no intersected edge in any of its cubes
-            // (cases 0 and 255 only): nothing to emit, nothing to add to prev
-            if (chunk_tris(blk, o, M, totals) == 0) continue;
+        {
             int cs[kMcMaxFields] = {0, 0, 0};
             unsigned newm[kMcMaxFields] = {0u, 0u, 0u};
             unsigned nt = 0, nn = 0;
@@ -417,15 +439,18 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_emit(McGeom g, const McTables
             for (int f = 0; f < kMcMaxFields; f++) {
                 if (f >= g.F) break;
                 cs[f] = q.valid ? cases[fc_off(g, f, c) + q.p] : 0;
+                // edges the cube's earlier channels cut (they own those vertices)
+                unsigned prev = 0u;
+                if (g.share && q.valid)
+                    for (int c2 = 0; c2 < c; c2++) prev |= active_edges(cases[fc_off(g, f, c2) + q.p]);
                 const unsigned act = active_edges(cs[f]);
-                newm[f] = owned & act & ~prev[f];
-                if (g.share) prev[f] |= act;
+                newm[f] = owned & act & ~prev;
                 nt += tri_count(s_tab.tri[cs[f]]);
                 nn += __popc(newm[f]);
             }
             unsigned total;
             const unsigned pre = block_scan(nt | nn << 16, s_warp, &total);
-            if (nt == 0) continue;
+            if (nt == 0) return;
             long long tb = (long long)(blk[o] & 0xffffffffull) + (pre & 0xffff);
             long long vb = (long long)(blk[o] >> 32) + (pre >> 16);
 #pragma unroll
@@ -497,20 +522,19 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_index(McGeom g, const McTable
                                                         const unsigned char *__restrict__ cases,
                                                         const int *__restrict__ tri_base,
                                                         const int *__restrict__ vert_base,
-                                                        const unsigned long long *__restrict__ blk,
-                                                        const long long *__restrict__ totals,
+                                                        const long long *__restrict__ list,
                                                         unsigned *__restrict__ idx)
 {
     __shared__ McTables s_tab;
     load_tables(tab, s_tab);
-    const int nchunks = g.slabs * g.nblk;
-    const long long M = (long long)g.slabs * g.C * g.nblk;
     const long long WH = (long long)g.W * g.H;
-    for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
-        const CubeRef q = cube_of(g, chunk);
-        if (!q.valid) continue;
-        for (int c = 0; c < g.C; c++) {
-            if (chunk_tris(blk, ((long long)q.s * g.C + c) * g.nblk + q.b, M, totals) == 0) continue;
+    // one chunk-channel with triangles per block
+    {
+        const long long o = list[blockIdx.x];
+        const int c = (int)((o / g.nblk) % g.C);
+        const CubeRef q = cube_of(g, (int)(o / ((long long)g.nblk * g.C)) * g.nblk + (int)(o % g.nblk));
+        if (!q.valid) return;
+        {
             for (int f = 0; f < g.F; f++) {
                 const int cs = cases[fc_off(g, f, c) + q.p];
                 const unsigned long long tl = s_tab.tri[cs];
@@ -731,6 +755,7 @@ struct lenia_mesher {
     unsigned char *cases = nullptr;
     int *tri_base = nullptr, *vert_base = nullptr;
     unsigned long long *blk = nullptr;  // per chunk and channel: tri | vert << 32, then its exclusive scan
+    long long *list = nullptr;          // chunk-channels with triangles, in order
     long long *totals = nullptr, *h_totals = nullptr;
     float *fn = nullptr, *pos = nullptr, *nrm = nullptr;
     int *vch = nullptr;
@@ -864,8 +889,9 @@ lenia_status lenia_mesher_create(const LeniaMeshDesc *desc, lenia_mesher **out)
     alloc(m->tri_base, sizeof(int) * cubes);
     alloc(m->vert_base, sizeof(int) * cubes);
     alloc(m->blk, sizeof(unsigned long long) * (size_t)M);
-    alloc(m->totals, 2 * sizeof(long long));
-    if (e == cudaSuccess) e = cudaMallocHost((void **)&m->h_totals, 2 * sizeof(long long));
+    alloc(m->list, sizeof(long long) * (size_t)M);
+    alloc(m->totals, 3 * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&m->h_totals, 3 * sizeof(long long));
     if (e == cudaSuccess) e = cudaMemcpy(m->tab, &host, sizeof(McTables), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         lenia_mesher_destroy(m);
@@ -885,6 +911,7 @@ lenia_status lenia_mesher_destroy(lenia_mesher *m)
     dfree(m->tri_base);
     dfree(m->vert_base);
     dfree(m->blk);
+    dfree(m->list);
     dfree(m->totals);
     if (m->h_totals) cudaFreeHost(m->h_totals);
     delete m;
@@ -906,12 +933,12 @@ lenia_status lenia_mesher_run(lenia_mesher *m, const float *const *fields, const
     m->have_mesh = false;
     const long long M = (long long)g.slabs * g.nblk * g.C;
     k_mc_count<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk);
-    k_mc_scan<<<1, kScanThreads, 0, st>>>(m->blk, M, m->totals);
+    k_mc_scan<<<1, kScanThreads, 0, st>>>(m->blk, M, m->totals, m->list);
     cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(m->h_totals, m->totals, 2 * sizeof(long long), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m->h_totals, m->totals, 3 * sizeof(long long), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return mcuda(m, e, "mesher count");
-    const long long nt = m->h_totals[0], nv = m->h_totals[1];
+    const long long nt = m->h_totals[0], nv = m->h_totals[1], nlist = m->h_totals[2];
     if (3 * nt > 0xffffffffLL || nv > 0x7fffffffLL)
         return mfail(m, LENIA_ERR_UNSUPPORTED, "mesh of %lld triangles exceeds 32-bit indices", nt);
     if (nt > m->cap_t || nv > m->cap_v) {
@@ -932,10 +959,10 @@ lenia_status lenia_mesher_run(lenia_mesher *m, const float *const *fields, const
         m->cap_v = cv;
     }
     if (nt > 0) {
-        k_mc_emit<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk, m->totals, m->tri_base,
+        k_mc_emit<<<(unsigned)nlist, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk, m->list, m->tri_base,
                                                   m->vert_base, m->fn, m->pos, m->vch, m->vsrc);
-        k_mc_index<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vert_base, m->blk, m->totals,
-                                                   m->idx);
+        k_mc_index<<<(unsigned)nlist, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vert_base, m->list,
+                                                           m->idx);
         const long long nb = (nv + kMcThreads - 1) / kMcThreads;
         const int gn = (int)(nb < 64LL * m->grid ? (nb > 0 ? nb : 1) : 64LL * m->grid);
         k_mc_normals<<<gn, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vsrc, m->fn, m->nrm, nv);

@@ -44,8 +44,32 @@ struct RowShape {
     using PM = PadMat<W>;
 };
 
-template <int W>
-__global__ void __launch_bounds__(kFastRowThreads) k_fwd_rows_s(FwdRowJobs jobs, const float2 *__restrict__ tw_x)
+// Job accessors: the by-value job structs of one world's launch, or the
+// device job lists of a batched launch (one entry per pair / plane).
+__device__ __forceinline__ const float *row_in(const FwdRowJobs &j, int p, int h) { return j.in[2 * p + h]; }
+__device__ __forceinline__ float2 *row_out(const FwdRowJobs &j, int p, int h) { return j.out[2 * p + h]; }
+__device__ __forceinline__ const float *row_in(const RowPairList &j, int p, int h) { return j.j[p].in[h]; }
+__device__ __forceinline__ float2 *row_out(const RowPairList &j, int p, int h) { return j.j[p].out[h]; }
+__device__ __forceinline__ const float2 *plane_src(const PlaneJobs &j, int i) { return j.src[i]; }
+__device__ __forceinline__ float2 *plane_dst(const PlaneJobs &j, int i) { return j.dst[i]; }
+__device__ __forceinline__ const float *plane_kc(const PlaneJobs &j, int i) { return j.kc[i]; }
+__device__ __forceinline__ const float2 *plane_src(const PlaneJobList &j, int i) { return j.j[i].src; }
+__device__ __forceinline__ float2 *plane_dst(const PlaneJobList &j, int i) { return j.j[i].dst; }
+__device__ __forceinline__ const float *plane_kc(const PlaneJobList &j, int i) { return j.j[i].kc; }
+// inverse rows: field h (0, 1) of pair p, null when the pair has one field
+__device__ __forceinline__ const float2 *inv_spec(const BlurJobs &j, int p, int h)
+{
+    return 2 * p + h < j.nfields ? j.spec[2 * p + h] : nullptr;
+}
+__device__ __forceinline__ float *inv_out(const BlurJobs &j, int p, int h)
+{
+    return 2 * p + h < j.nfields ? j.out[2 * p + h] : nullptr;
+}
+__device__ __forceinline__ const float2 *inv_spec(const InvPairList &j, int p, int h) { return j.j[p].spec[h]; }
+__device__ __forceinline__ float *inv_out(const InvPairList &j, int p, int h) { return j.j[p].out[h]; }
+
+template <int W, typename J>
+__global__ void __launch_bounds__(kFastRowThreads) k_fwd_rows_s(J jobs, const float2 *__restrict__ tw_x)
 {
     using S = RowShape<W>;
     constexpr int H = W, D = W, TY = S::TY, KX = W / 2 + 1;
@@ -55,10 +79,10 @@ __global__ void __launch_bounds__(kFastRowThreads) k_fwd_rows_s(FwdRowJobs jobs,
     const int z = blockIdx.x / (H / TY);
     const int y0 = (blockIdx.x % (H / TY)) * TY;
     const int pair = blockIdx.y;
-    const float *fa = jobs.in[2 * pair];
-    const float *fb = jobs.in[2 * pair + 1];
-    float2 *oa = jobs.out[2 * pair];
-    float2 *ob = jobs.out[2 * pair + 1];
+    const float *fa = row_in(jobs, pair, 0);
+    const float *fb = row_in(jobs, pair, 1);
+    float2 *oa = row_out(jobs, pair, 0);
+    float2 *ob = row_out(jobs, pair, 1);
     for (int i = threadIdx.x; i < W; i += kFastRowThreads) tw[i] = tw_x[i];
     pdl_trigger();
     pdl_wait();
@@ -181,8 +205,8 @@ __device__ __forceinline__ void plane_last_stage(const float2 *buf, float2 *__re
     }
 }
 
-template <int W>
-__global__ void __launch_bounds__(kFastPlaneThreads) k_planes_s(PlaneJobs jobs, const float2 *__restrict__ tw_y,
+template <int W, typename J>
+__global__ void __launch_bounds__(kFastPlaneThreads) k_planes_s(J jobs, const float2 *__restrict__ tw_y,
                                                                 const float2 *__restrict__ tw_z, int sign)
 {
     constexpr int H = W, D = W;
@@ -193,9 +217,9 @@ __global__ void __launch_bounds__(kFastPlaneThreads) k_planes_s(PlaneJobs jobs, 
     float2 *buf = smem + H + D;
     const int kx = blockIdx.x;
     const int job = blockIdx.y;
-    const float4 *src = reinterpret_cast<const float4 *>(jobs.src[job] + (long long)kx * D * H);
-    float4 *dst = reinterpret_cast<float4 *>(jobs.dst[job] + (long long)kx * D * H);
-    const float *kc = jobs.kc[job];
+    const float4 *src = reinterpret_cast<const float4 *>(plane_src(jobs, job) + (long long)kx * D * H);
+    float4 *dst = reinterpret_cast<float4 *>(plane_dst(jobs, job) + (long long)kx * D * H);
+    const float *kc = plane_kc(jobs, job);
     for (int i = threadIdx.x; i < H; i += kFastPlaneThreads) twy[i] = tw_y[i];
     for (int i = threadIdx.x; i < D; i += kFastPlaneThreads) twz[i] = tw_z[i];
     pdl_trigger();
@@ -675,8 +699,8 @@ __global__ void __launch_bounds__(kGwWarps * 32) k_growth_warp(GrowthJobs jobs, 
     if (bad && err_flag) atomicOr(err_flag, 1);
 }
 
-template <int W>
-__global__ void __launch_bounds__(kFastRowThreads) k_blur_rows_s(BlurJobs jobs, const float2 *__restrict__ tw_x)
+template <int W, typename J>
+__global__ void __launch_bounds__(kFastRowThreads) k_blur_rows_s(J jobs, const float2 *__restrict__ tw_x)
 {
     using S = RowShape<W>;
     constexpr int H = W, TY = S::TY, T = S::T;
@@ -692,14 +716,15 @@ __global__ void __launch_bounds__(kFastRowThreads) k_blur_rows_s(BlurJobs jobs, 
     for (int i = threadIdx.x; i < W; i += kFastRowThreads) tw[i] = tw_x[i];
     pdl_trigger();
     pdl_wait();
-    const int f0 = 2 * pair, f1 = 2 * pair + 1 < jobs.nfields ? 2 * pair + 1 : -1;
-    load_packed_rows_s<W>(buf, jobs.spec[f0], f1 >= 0 ? jobs.spec[f1] : nullptr, z, y0);
+    const float2 *s1 = inv_spec(jobs, pair, 1);
+    float *o0 = inv_out(jobs, pair, 0), *o1 = inv_out(jobs, pair, 1);
+    load_packed_rows_s<W>(buf, inv_spec(jobs, pair, 0), s1, z, y0);
     __syncthreads();
     static_fft<W, TY, false, W, kFastRowThreads>(buf, tw, +1);
     for (int e = threadIdx.x; e < T; e += kFastRowThreads) {
         const float2 zz = buf[S::PM::at(e / W, e % W)];
-        jobs.out[f0][base + e] = zz.x / nf;
-        if (f1 >= 0) jobs.out[f1][base + e] = zz.y / nf;
+        o0[base + e] = zz.x / nf;
+        if (s1) o1[base + e] = zz.y / nf;
     }
 }
 
@@ -714,9 +739,10 @@ cudaError_t fwd_rows_w(const Dims &d, const float2 *tw, const FwdRowJobs &jobs, 
 {
     using S = RowShape<W>;
     const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2);
-    cudaError_t e = smem_attr((const void *)k_fwd_rows_s<W>, smem);
+    cudaError_t e = smem_attr((const void *)k_fwd_rows_s<W, FwdRowJobs>, smem);
     if (e != cudaSuccess) return e;
-    return launch_pdl(k_fwd_rows_s<W>, dim3(W * (W / S::TY), jobs.npairs), dim3(kFastRowThreads), smem, st, jobs, tw);
+    return launch_pdl(k_fwd_rows_s<W, FwdRowJobs>, dim3(W * (W / S::TY), jobs.npairs), dim3(kFastRowThreads), smem, st,
+                      jobs, tw);
 }
 
 template <int W>
@@ -743,10 +769,10 @@ cudaError_t planes_w(const Dims &d, const float2 *twy, const float2 *twz, const 
         return launch_pdl(k_planes_stream_s<W>, dim3(units < resident ? units : resident), dim3(kFastPlaneThreads),
                           smem, st, jobs, twy, twz, sign);
     } else {
-        cudaError_t e = smem_attr((const void *)k_planes_s<W>, smem);
+        cudaError_t e = smem_attr((const void *)k_planes_s<W, PlaneJobs>, smem);
         if (e != cudaSuccess) return e;
-        return launch_pdl(k_planes_s<W>, dim3(W / 2 + 1, jobs.njobs), dim3(kFastPlaneThreads), smem, st, jobs, twy,
-                          twz, sign);
+        return launch_pdl(k_planes_s<W, PlaneJobs>, dim3(W / 2 + 1, jobs.njobs), dim3(kFastPlaneThreads), smem, st,
+                          jobs, twy, twz, sign);
     }
 }
 
@@ -801,10 +827,44 @@ cudaError_t blur_rows_w(const float2 *tw, const BlurJobs &jobs, cudaStream_t st)
 {
     using S = RowShape<W>;
     const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2);
-    cudaError_t e = smem_attr((const void *)k_blur_rows_s<W>, smem);
+    cudaError_t e = smem_attr((const void *)k_blur_rows_s<W, BlurJobs>, smem);
     if (e != cudaSuccess) return e;
-    return launch_pdl(k_blur_rows_s<W>, dim3(W * (W / S::TY), (jobs.nfields + 1) / 2), dim3(kFastRowThreads), smem,
-                      st, jobs, tw);
+    return launch_pdl(k_blur_rows_s<W, BlurJobs>, dim3(W * (W / S::TY), (jobs.nfields + 1) / 2),
+                      dim3(kFastRowThreads), smem, st, jobs, tw);
+}
+
+// Batched forms: the same kernels over device job lists (grid y = entries).
+template <int W>
+cudaError_t fwd_rows_list_w(const float2 *tw, RowPairList jobs, cudaStream_t st)
+{
+    using S = RowShape<W>;
+    const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2);
+    cudaError_t e = smem_attr((const void *)k_fwd_rows_s<W, RowPairList>, smem);
+    if (e != cudaSuccess || jobs.n == 0) return e;
+    k_fwd_rows_s<W, RowPairList><<<dim3(W * (W / S::TY), jobs.n), kFastRowThreads, smem, st>>>(jobs, tw);
+    return cudaGetLastError();
+}
+
+template <int W>
+cudaError_t planes_list_w(const float2 *twy, const float2 *twz, PlaneJobList jobs, int sign, cudaStream_t st)
+{
+    static_assert(!planes_persistent<W>(), "batched plane passes take one plane per block");
+    const size_t smem = (size_t)(2 * W + PadMat<W>::size(W)) * sizeof(float2);
+    cudaError_t e = smem_attr((const void *)k_planes_s<W, PlaneJobList>, smem);
+    if (e != cudaSuccess || jobs.n == 0) return e;
+    k_planes_s<W, PlaneJobList><<<dim3(W / 2 + 1, jobs.n), kFastPlaneThreads, smem, st>>>(jobs, twy, twz, sign);
+    return cudaGetLastError();
+}
+
+template <int W>
+cudaError_t inv_rows_list_w(const float2 *tw, InvPairList jobs, cudaStream_t st)
+{
+    using S = RowShape<W>;
+    const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2);
+    cudaError_t e = smem_attr((const void *)k_blur_rows_s<W, InvPairList>, smem);
+    if (e != cudaSuccess || jobs.n == 0) return e;
+    k_blur_rows_s<W, InvPairList><<<dim3(W * (W / S::TY), jobs.n), kFastRowThreads, smem, st>>>(jobs, tw);
+    return cudaGetLastError();
 }
 
 }  // namespace
@@ -860,6 +920,52 @@ cudaError_t launch_planes_fast(const Dims &d, const float2 *tw_y, const float2 *
 }
 
 bool fast_split_planes_supported(const Dims &d) { return d.W == d.H && d.W == 256; }
+
+// Grid sizes of the batched launches: the size-specialised kernels with one
+// plane per block.
+#define LENIA_LIST_SIZES(X) X(24) X(32) X(36) X(44) X(48) X(64) X(96)
+
+bool list_size_supported(int W)
+{
+    switch (W) {
+#define CASE(n) case n:
+        LENIA_LIST_SIZES(CASE)
+#undef CASE
+        return true;
+    default: return false;
+    }
+}
+
+cudaError_t launch_fwd_rows_list(int W, const float2 *tw_x, RowPairList jobs, cudaStream_t st)
+{
+    switch (W) {
+#define CASE(n) case n: return fwd_rows_list_w<n>(tw_x, jobs, st);
+        LENIA_LIST_SIZES(CASE)
+#undef CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_planes_list(int W, const float2 *tw_y, const float2 *tw_z, PlaneJobList jobs, int sign,
+                               cudaStream_t st)
+{
+    switch (W) {
+#define CASE(n) case n: return planes_list_w<n>(tw_y, tw_z, jobs, sign, st);
+        LENIA_LIST_SIZES(CASE)
+#undef CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_inv_rows_list(int W, const float2 *tw_x_inv, InvPairList jobs, cudaStream_t st)
+{
+    switch (W) {
+#define CASE(n) case n: return inv_rows_list_w<n>(tw_x_inv, jobs, st);
+        LENIA_LIST_SIZES(CASE)
+#undef CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
 
 cudaError_t launch_planes_split_fast(const Dims &d, const float2 *tw_y, const float2 *tw_z, const PlaneJobs &jobs,
                                      int sign, cudaStream_t st)

@@ -132,14 +132,17 @@ __device__ __forceinline__ void transport_epilogue(const StepParams &p, const Tr
     b.SUM[i] = stam * 0.0f + ttsum * stas;
 }
 
-__global__ void __launch_bounds__(256) k_transport(StepParams p, TransportBuffers b)
+__device__ __forceinline__ void transport_cell_body(const StepParams &p, const TransportBuffers &b, long long block)
 {
     const Dims &d = p.d;
     const long long N = d.N;
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long i = block * blockDim.x + threadIdx.x;
     if (i >= N) return;
     const int C = p.C;
-    const int x = (int)(i % d.W), y = (int)((i / d.W) % d.H), z = (int)(i / ((long long)d.W * d.H));
+    // N < 2^31 (at most 256^3 cells): the cell's coordinates by two 32-bit divisions
+    const unsigned ui = (unsigned)i, plane = (unsigned)d.W * (unsigned)d.H;
+    const unsigned uz = ui / plane, rem = ui - uz * plane, uy = rem / (unsigned)d.W;
+    const int x = (int)(rem - uy * (unsigned)d.W), y = (int)uy, z = (int)uz;
     const float px = (float)x + 0.5f, py = (float)y + 0.5f, pz = (float)z + 0.5f;
     const int dd = p.dd;
     float tt[kMaxChannels];
@@ -265,6 +268,12 @@ __global__ void __launch_bounds__(256) k_transport(StepParams p, TransportBuffer
     transport_epilogue(p, b, tt, x, y, z, i);
 }
 
+__global__ void __launch_bounds__(256) k_transport(const __grid_constant__ StepParams p,
+                                                   const __grid_constant__ TransportBuffers b)
+{
+    transport_cell_body(p, b, blockIdx.x);
+}
+
 // ------------------------------------------------------------------
 // RT / SRT as a tiled destination gather.  A block owns 32 x 8 x TZ cells
 // (thread = one x, y column of TZ cells).  Per channel one thread copies MU
@@ -324,11 +333,15 @@ constexpr int kTBufs = LENIA_TRANSPORT_BUFS;  // 2: channel c + 1 lands while c 
 #define LENIA_TRANSPORT_PREGA 1
 #endif
 constexpr bool kTransportPrefetchGA = LENIA_TRANSPORT_PREGA;
+#ifndef LENIA_TRANSPORT_PREFETCH_NEXT
+#define LENIA_TRANSPORT_PREFETCH_NEXT 1
+#endif
+constexpr bool kTransportPrefetchNext = LENIA_TRANSPORT_PREFETCH_NEXT;
 
 template <int DD, bool TORUS, bool CLIP1>
-__global__ void __launch_bounds__(kTX *kTY, LENIA_TRANSPORT_MINB) k_transport_tiled(StepParams p, TransportBuffers b,
-                                                              const __grid_constant__ CUtensorMap tm_mu,
-                                                              const __grid_constant__ CUtensorMap tm_arr)
+__device__ __forceinline__ void transport_tiled_body(const StepParams &p, const TransportBuffers &b,
+                                                     const CUtensorMap *tm_mu, const CUtensorMap *tm_arr, int bx,
+                                                     int by)
 {
     constexpr int SX = kTBoxX, SY = kTY + 2 * DD, SZ = kTZ + 2 * DD, SV = SX * SY * SZ;
     constexpr int OX = 4 - DD;  // staged x of source offset -DD from the tile's first column
@@ -344,9 +357,9 @@ __global__ void __launch_bounds__(kTX *kTY, LENIA_TRANSPORT_MINB) k_transport_ti
     const int tx = threadIdx.x, ty = threadIdx.y;
     const bool leader = tx == 0 && ty == 0;
     const int tiles_x = (d.W + kTX - 1) / kTX;
-    const int x0 = (blockIdx.x % tiles_x) * kTX;
-    const int y0 = (blockIdx.x / tiles_x) * kTY;
-    const int z0 = blockIdx.y * kTZ;
+    const int x0 = (bx % tiles_x) * kTX;
+    const int y0 = (bx / tiles_x) * kTY;
+    const int z0 = by * kTZ;
     const int x = x0 + tx, y = y0 + ty;
     const float px = (float)x + 0.5f, py = (float)y + 0.5f;
     const bool srt = p.mode_type == kModeSRT;
@@ -384,10 +397,18 @@ __global__ void __launch_bounds__(kTX *kTY, LENIA_TRANSPORT_MINB) k_transport_ti
         fence_proxy_async();
         mbar_arrive_expect_tx(bar, 4 * SV * 4);
         const int gx = x0 - 4, gy = y0 - DD, gz = z0 - DD;
-        tma_load_4d(buf, &tm_mu, gx, gy, gz, c, bar);
-        tma_load_4d(buf + SV, &tm_mu, gx, gy, gz, C + c, bar);
-        tma_load_4d(buf + 2 * SV, &tm_mu, gx, gy, gz, 2 * C + c, bar);
-        tma_load_4d(buf + 3 * SV, &tm_arr, gx, gy, gz, c, bar);
+        tma_load_4d(buf, tm_mu, gx, gy, gz, c, bar);
+        tma_load_4d(buf + SV, tm_mu, gx, gy, gz, C + c, bar);
+        tma_load_4d(buf + 2 * SV, tm_mu, gx, gy, gz, 2 * C + c, bar);
+        tma_load_4d(buf + 3 * SV, tm_arr, gx, gy, gz, c, bar);
+        // the next channel's tiles move to L2 while this one is used, so
+        // that its copy (issued once this one is done) reads L2
+        if (kTransportPrefetchNext && c + 1 < crt) {
+            tma_prefetch_4d(tm_mu, gx, gy, gz, c + 1);
+            tma_prefetch_4d(tm_mu, gx, gy, gz, C + c + 1);
+            tma_prefetch_4d(tm_mu, gx, gy, gz, 2 * C + c + 1);
+            tma_prefetch_4d(tm_arr, gx, gy, gz, c + 1);
+        }
     };
     // the periodic face layers of channel c's tiles: for each grid face the
     // tile crosses, the cells of its DD layers whose other coordinates are in
@@ -521,6 +542,124 @@ __global__ void __launch_bounds__(kTX *kTY, LENIA_TRANSPORT_MINB) k_transport_ti
     }
 }
 
+template <int DD, bool TORUS, bool CLIP1>
+__global__ void __launch_bounds__(kTX *kTY, LENIA_TRANSPORT_MINB) k_transport_tiled(const __grid_constant__ StepParams p,
+                                                              const __grid_constant__ TransportBuffers b,
+                                                              const __grid_constant__ CUtensorMap tm_mu,
+                                                              const __grid_constant__ CUtensorMap tm_arr)
+{
+    transport_tiled_body<DD, TORUS, CLIP1>(p, b, &tm_mu, &tm_arr, blockIdx.x, blockIdx.y);
+}
+
+template <typename T>
+__device__ __forceinline__ void copy_words_to_shared(T *dst, const T *src)
+{
+    static_assert(sizeof(T) % 4 == 0, "copied as 4-byte words");
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int nthr = blockDim.x * blockDim.y;
+    for (int i = tid; i < (int)(sizeof(T) / 4); i += nthr)
+        reinterpret_cast<unsigned *>(dst)[i] = reinterpret_cast<const unsigned *>(src)[i];
+}
+
+// Batched transport (RT, dd = 1, the tiled gather): block b is block
+// items[b].block of world items[b].world's own launch (x-y tile fastest);
+// the world's parameters are read into shared memory first.
+template <bool TORUS, bool CLIP1>
+__global__ void __launch_bounds__(kTX *kTY, LENIA_TRANSPORT_MINB) k_transport_rt_multi(
+    const BatchWorldDev *__restrict__ ws, const WorkItem *__restrict__ items)
+{
+    __shared__ StepParams sp;
+    __shared__ TransportBuffers sb;
+    const WorkItem it = items[blockIdx.x];
+    const BatchWorldDev *w = ws + it.world;
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        asm volatile("prefetch.tensormap [%0];\n" ::"l"(&w->tm_mu) : "memory");
+        asm volatile("prefetch.tensormap [%0];\n" ::"l"(&w->tm_arr) : "memory");
+    }
+    copy_words_to_shared(&sp, &w->p);
+    copy_words_to_shared(&sb, &w->tb);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(&w->tm_mu) : "memory");
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(&w->tm_arr) : "memory");
+    }
+    const int gx = w->transport_gx;
+    __syncthreads();
+    transport_tiled_body<1, TORUS, CLIP1>(sp, sb, &w->tm_mu, &w->tm_arr, it.block % gx, it.block / gx);
+}
+
+// Batched per-cell transport (advection, and whatever the tiled gather does
+// not take): block b is block items[b].block of world items[b].world's launch.
+__global__ void __launch_bounds__(256) k_transport_cell_multi(const BatchWorldDev *__restrict__ ws,
+                                                              const WorkItem *__restrict__ items)
+{
+    __shared__ StepParams sp;
+    __shared__ TransportBuffers sb;
+    const WorkItem it = items[blockIdx.x];
+    const BatchWorldDev *w = ws + it.world;
+    copy_words_to_shared(&sp, &w->p);
+    copy_words_to_shared(&sb, &w->tb);
+    __syncthreads();
+    transport_cell_body(sp, sb, it.block);
+}
+
+int transport_rt_blocks(const Dims &d, int *gx)
+{
+    const int tiles_x = (d.W + kTX - 1) / kTX, tiles_y = (d.H + kTY - 1) / kTY;
+    if (gx) *gx = tiles_x * tiles_y;
+    return tiles_x * tiles_y * ((d.D + kTZ - 1) / kTZ);
+}
+
+int transport_adv_blocks(const Dims &d) { return (int)((d.N + 255) / 256); }
+
+cudaError_t launch_transport_rt_multi(const BatchWorldDev *ws, const WorkItem *items, int n_items, bool torus,
+                                      bool clip1, cudaStream_t st)
+{
+    if (n_items == 0) return cudaSuccess;
+    auto go = [&](auto kern) -> cudaError_t {
+        const int sv = kTBoxX * (kTY + 2) * (kTZ + 2);
+        const size_t ga = kTransportPrefetchGA ? (size_t)kMaxChannels * kTZ * kTX * kTY : 0;
+        const size_t smem = (kTBufs * 4 * (size_t)sv + ga) * sizeof(float);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        kern<<<(unsigned)n_items, dim3(kTX, kTY), smem, st>>>(ws, items);
+        return cudaGetLastError();
+    };
+    if (torus) return clip1 ? go(k_transport_rt_multi<true, true>) : go(k_transport_rt_multi<true, false>);
+    return clip1 ? go(k_transport_rt_multi<false, true>) : go(k_transport_rt_multi<false, false>);
+}
+
+cudaError_t launch_transport_adv_multi(const BatchWorldDev *ws, const WorkItem *items, int n_items, cudaStream_t st)
+{
+    if (n_items == 0) return cudaSuccess;
+    k_transport_cell_multi<<<(unsigned)n_items, 256, 0, st>>>(ws, items);
+    return cudaGetLastError();
+}
+
+// The tiled gather's tensor maps: MU (x, y, z, 3C) and ARR (x, y, z, C),
+// tiles of kTBoxX x (kTY + 2 dd) x (kTZ + 2 dd).
+cudaError_t transport_tensor_maps(const StepParams &p, const TransportBuffers &b, int dd, CUtensorMap *tm_mu,
+                                  CUtensorMap *tm_arr)
+{
+    const Dims &d = p.d;
+    const unsigned long long dmu[4] = {(unsigned long long)d.W, (unsigned long long)d.H, (unsigned long long)d.D,
+                                       3ull * p.C};
+    const unsigned long long darr[4] = {(unsigned long long)d.W, (unsigned long long)d.H, (unsigned long long)d.D,
+                                        (unsigned long long)p.C};
+    const unsigned box[4] = {(unsigned)kTBoxX, (unsigned)(kTY + 2 * dd), (unsigned)(kTZ + 2 * dd), 1u};
+    cudaError_t e = encode_tensor_map(tm_mu, b.MU, 4, dmu, box);
+    if (e == cudaSuccess) e = encode_tensor_map(tm_arr, b.ARR, 4, darr, box);
+    return e;
+}
+
+// The transport kernel a world's step uses: 1 = the tiled gather with dd = 1
+// (the form the batched launches take), 2 = tiled with dd = 2, 0 = per cell.
+int transport_form(const StepParams &p)
+{
+    const int crt = p.rt_all_channels ? p.C : (p.C < 3 ? p.C : 3);
+    if ((p.mode_type == kModeRT || p.mode_type == kModeSRT) && p.dd >= 1 && p.dd <= 2 && crt > 0) return p.dd;
+    return 0;
+}
+
 cudaError_t launch_transport(const StepParams &p, const TransportBuffers &b, cudaStream_t st)
 {
     const int crt = p.rt_all_channels ? p.C : (p.C < 3 ? p.C : 3);
@@ -529,15 +668,9 @@ cudaError_t launch_transport(const StepParams &p, const TransportBuffers &b, cud
         const int tiles_x = (d.W + kTX - 1) / kTX, tiles_y = (d.H + kTY - 1) / kTY;
         dim3 grid(tiles_x * tiles_y, (d.D + kTZ - 1) / kTZ), block(kTX, kTY);
         const bool torus = p.border == kBorderTorus;
-        const unsigned long long dmu[4] = {(unsigned long long)d.W, (unsigned long long)d.H,
-                                           (unsigned long long)d.D, 3ull * p.C};
-        const unsigned long long darr[4] = {(unsigned long long)d.W, (unsigned long long)d.H,
-                                            (unsigned long long)d.D, (unsigned long long)p.C};
         auto go = [&](auto kern, int dd) -> cudaError_t {
-            const unsigned box[4] = {(unsigned)kTBoxX, (unsigned)(kTY + 2 * dd), (unsigned)(kTZ + 2 * dd), 1u};
             CUtensorMap tm_mu, tm_arr;
-            cudaError_t e = encode_tensor_map(&tm_mu, b.MU, 4, dmu, box);
-            if (e == cudaSuccess) e = encode_tensor_map(&tm_arr, b.ARR, 4, darr, box);
+            cudaError_t e = transport_tensor_maps(p, b, dd, &tm_mu, &tm_arr);
             if (e != cudaSuccess) return e;
             const int sv = kTBoxX * (kTY + 2 * dd) * (kTZ + 2 * dd);
             const size_t ga = (kTransportPrefetchGA && dd == 1) ? (size_t)kMaxChannels * kTZ * kTX * kTY : 0;

@@ -505,15 +505,11 @@ struct WorldScratch {
 
 // ---------------------------------------------------------------- stages
 
-lenia_status stage_growth(lenia_world *w)
+// The growth stage's jobs of a world (kernel spectra, targets, weights,
+// growth-table rows, channel flags).
+GrowthJobs growth_jobs(const lenia_world *w)
 {
     const Dims &d = w->d;
-    cudaStream_t st = w->stream;
-    cudaError_t e;
-    if (w->snapshots) {
-        std::swap(w->H, w->H_RB);
-        std::swap(w->U_SUM, w->U_SUM_RB);
-    }
     GrowthJobs gj;
     memset(&gj, 0, sizeof(gj));
     gj.K = w->K;
@@ -535,6 +531,67 @@ lenia_status stage_growth(lenia_world *w)
         gj.m[k] = w->kernels[k].m;
         gj.s[k] = w->kernels[k].s;
     }
+    return gj;
+}
+
+// The flow stage's buffers of a world (its current grid).
+FlowBuffers flow_buffers(const lenia_world *w)
+{
+    FlowBuffers b;
+    memset(&b, 0, sizeof(b));
+    const bool cd = w->desc.gradient_mode == LENIA_GRADIENT_CENTRAL_DIFF;
+    // Without the blur, U_S and SUM_S are plain copies of H and SUM
+    // (the intended h_sum_blur copy): read H and SUM directly.
+    b.H = (cd && w->blur_valid) ? w->U_S : w->H;
+    b.SUM = (cd && w->blur_valid) ? w->SUM_S : w->SUM;
+    b.A = w->A;
+    b.GA = w->GA;
+    b.V = w->V;
+    b.MU = w->MU;
+    b.F = (w->debug || needs_F(w->desc)) ? w->F : nullptr;
+    b.ALPHA = (w->debug || w->desc.osc_div_flow) ? w->ALPHA : nullptr;
+    b.err = w->err_flag;
+    if (w->debug) {
+        b.NA = w->NA;
+        b.NU = w->NU;
+        b.PREALPHA = w->PREALPHA;
+    }
+    return b;
+}
+
+// The transport stage's buffers of a world (current grid A, new grid A_next).
+TransportBuffers transport_buffers(const lenia_world *w)
+{
+    TransportBuffers b;
+    memset(&b, 0, sizeof(b));
+    const bool use_grid =
+        w->desc.growth_type == LENIA_GROWTH_NOGROWTH || w->desc.growth_type == LENIA_GROWTH_TRANSPOSITION;
+    b.A = w->A;
+    b.A_out = w->A_next;
+    b.ARR = use_grid ? w->A : w->BACK;
+    b.MU = w->MU;
+    b.H = w->H;
+    b.V = w->V;
+    b.F = w->F;
+    b.ALPHA = w->ALPHA;
+    b.GA = w->GA;
+    b.SUM = w->SUM;
+    b.BACK = w->BACK;
+    b.TT = w->debug ? w->TT : nullptr;
+    b.err = w->err_flag;
+    return b;
+}
+
+lenia_status stage_growth(lenia_world *w)
+{
+    const Dims &d = w->d;
+    cudaStream_t st = w->stream;
+    cudaError_t e;
+    if (w->snapshots) {
+        std::swap(w->H, w->H_RB);
+        std::swap(w->U_SUM, w->U_SUM_RB);
+    }
+    const GrowthJobs gj = growth_jobs(w);
     if (w->conv_mode != LENIA_CONV_FFT) {
         // direct convolution on the tensor cores, then the growth from u_k
         if (!w->dconv && w->K > 0) return fail(w, LENIA_ERR_INVALID_ARG, "direct convolution has no plan");
@@ -705,26 +762,8 @@ lenia_status stage_flow(lenia_world *w)
 {
     lenia_status s = ensure_optional(w);
     if (s != LENIA_OK) return s;
-    StepParams p = step_params(w);
-    FlowBuffers b;
-    memset(&b, 0, sizeof(b));
-    const bool cd = w->desc.gradient_mode == LENIA_GRADIENT_CENTRAL_DIFF;
-    // Without the blur, U_S and SUM_S are plain copies of H and SUM
-    // (the intended h_sum_blur copy): read H and SUM directly.
-    b.H = (cd && w->blur_valid) ? w->U_S : w->H;
-    b.SUM = (cd && w->blur_valid) ? w->SUM_S : w->SUM;
-    b.A = w->A;
-    b.GA = w->GA;
-    b.V = w->V;
-    b.MU = w->MU;
-    b.F = (w->debug || needs_F(w->desc)) ? w->F : nullptr;
-    b.ALPHA = (w->debug || w->desc.osc_div_flow) ? w->ALPHA : nullptr;
-    b.err = w->err_flag;
-    if (w->debug) {
-        b.NA = w->NA;
-        b.NU = w->NU;
-        b.PREALPHA = w->PREALPHA;
-    }
+    const StepParams p = step_params(w);
+    const FlowBuffers b = flow_buffers(w);
     cudaError_t e;
     {
         ProfScope ps(w, KID_FLOW);
@@ -737,24 +776,8 @@ lenia_status stage_flow(lenia_world *w)
 
 lenia_status stage_transport(lenia_world *w)
 {
-    StepParams p = step_params(w);
-    TransportBuffers b;
-    memset(&b, 0, sizeof(b));
-    const bool use_grid =
-        w->desc.growth_type == LENIA_GROWTH_NOGROWTH || w->desc.growth_type == LENIA_GROWTH_TRANSPOSITION;
-    b.A = w->A;
-    b.A_out = w->A_next;
-    b.ARR = use_grid ? w->A : w->BACK;
-    b.MU = w->MU;
-    b.H = w->H;
-    b.V = w->V;
-    b.F = w->F;
-    b.ALPHA = w->ALPHA;
-    b.GA = w->GA;
-    b.SUM = w->SUM;
-    b.BACK = w->BACK;
-    b.TT = w->debug ? w->TT : nullptr;
-    b.err = w->err_flag;
+    const StepParams p = step_params(w);
+    const TransportBuffers b = transport_buffers(w);
     cudaError_t e;
     {
         ProfScope ps(w, KID_TRANSPORT);
@@ -1368,6 +1391,33 @@ struct BatchLane {
     std::vector<int> worlds;
 };
 
+// Worlds stepped by the batched launches (one launch per stage and grid size
+// over all worlds of a wave, see capture_grouped): a wave is a set of worlds
+// whose per-step buffers fit the shared scratch pool at once; waves run one
+// after another and reuse the pool.
+struct GroupSize {                 // the jobs of one grid size in a wave
+    int W = 0;
+    const float2 *tw_x_fwd = nullptr, *tw_x_inv = nullptr, *tw_y_fwd = nullptr, *tw_y_inv = nullptr;
+    RowPairJob *fwd = nullptr;     // forward rows of the current grid (per parity)
+    int n_fwd = 0;
+    PlaneJob *planes_fwd = nullptr, *planes_inv = nullptr;
+    int n_planes_fwd = 0, n_planes_inv = 0;
+    InvPairJob *inv = nullptr;
+    int n_inv = 0;
+};
+struct GroupWave {
+    std::vector<int> worlds;
+    std::vector<GroupSize> sizes;
+    BatchWorldDev *ws = nullptr;   // world table
+    WorkItem *growth = nullptr, *flow = nullptr, *rt[4] = {}, *adv = nullptr;  // rt: [torus * 2 + clip1]
+    int n_growth = 0, n_flow = 0, n_rt[4] = {}, n_adv = 0;
+};
+struct GroupPlan {                 // per step parity (the grid and its double buffer swap)
+    std::vector<GroupWave> waves;
+    std::vector<void *> allocs;    // device tables of this plan
+    int launches = 0;
+};
+
 struct lenia_batch {
     std::vector<lenia_world *> worlds;
     std::vector<BatchLane> lanes;
@@ -1377,6 +1427,15 @@ struct lenia_batch {
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     int parity = 0;
     std::string err;
+    // batched launches
+    std::vector<char> grouped;      // per world: stepped by the batched launches
+    GroupPlan plan[2];
+    unsigned char *pool = nullptr;  // shared per-step scratch of a wave
+    size_t pool_bytes = 0;
+    cudaStream_t group_stream = nullptr;
+    cudaEvent_t group_join = nullptr;
+    int lane_launches[2] = {0, 0};
+    bool group_on = true;           // lenia_batch_set_batched_launches
 };
 
 namespace {
@@ -1392,11 +1451,23 @@ lenia_status bfail(lenia_batch *b, lenia_status s, const char *fmt, ...)
     return s;
 }
 
+void free_plan(GroupPlan &p)
+{
+    for (void *q : p.allocs)
+        if (q) cudaFree(q);
+    p = GroupPlan();
+}
+
 void free_batch(lenia_batch *b)
 {
     if (b->stream) cudaStreamSynchronize(b->stream);
     for (cudaGraphExec_t &g : b->exec)
         if (g) cudaGraphExecDestroy(g);
+    if (b->group_stream) cudaStreamSynchronize(b->group_stream);
+    for (GroupPlan &p : b->plan) free_plan(p);
+    if (b->pool) cudaFree(b->pool);
+    if (b->group_join) cudaEventDestroy(b->group_join);
+    if (b->group_stream) cudaStreamDestroy(b->group_stream);
     for (lenia_world *w : b->worlds) {
         free_world(w);
         delete w;
@@ -1424,29 +1495,282 @@ lenia_status step_once(lenia_world *w)
     return stage_transport(w);
 }
 
+// ---- batched launches ---------------------------------------------------
+//
+// Worlds that take the batched launches: cubic grids of a size with
+// one-block-per-plane transforms (24 .. 96), the FFT convolution (stepped in
+// its split form, inverse rows storing u_k then the growth from u_k: the
+// same bits as the fused form), no debug outputs, snapshots, mass
+// conservation, blur, F or ALPHA, and a transport that is the tiled gather
+// with dd = 1 or the per-cell kernel.  Per wave and stage one launch per
+// grid size (transforms) or one launch over all the wave's worlds (growth
+// from u_k, flow, transport), each block working on one block of one world
+// through a device work list.
+
+constexpr size_t kWaveScratchBytes = 12ull << 30;  // per-step buffers of one wave
+
+size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+bool group_eligible(const lenia_world *w)
+{
+    const LeniaWorldDesc &s = w->desc;
+    if (w->d.W != w->d.H || !list_size_supported(w->d.W)) return false;
+    if (w->conv_mode != LENIA_CONV_FFT || w->K < 1 || w->C < 1) return false;
+    if (w->debug || w->snapshots || s.conserve_mass) return false;
+    if (s.gradient_mode == LENIA_GRADIENT_CENTRAL_DIFF && s.blur_central_diff) return false;
+    if (needs_F(s) || s.osc_div_flow) return false;
+    return transport_form(step_params(w)) != 2;
+}
+
+// The per-step buffers of a world in a wave: H, U_SUM, BACK, MU, u_k, the
+// channels' half spectra and the kernels' inverse half spectra.
+size_t group_scratch_bytes(const lenia_world *w)
+{
+    const size_t N = (size_t)w->d.N, CN = (size_t)w->C * N, HS = (size_t)w->d.HS;
+    return 3 * align256(CN * 4) + align256(3 * CN * 4) + align256((size_t)w->K * N * 4) +
+           align256((size_t)w->C * HS * 8) + align256((size_t)w->K * HS * 8);
+}
+
+template <typename T>
+T *plan_copy(GroupPlan &plan, const std::vector<T> &v, cudaError_t &e)
+{
+    if (e != cudaSuccess || v.empty()) return nullptr;
+    T *p = nullptr;
+    e = cudaMalloc((void **)&p, sizeof(T) * v.size());
+    if (e != cudaSuccess) return nullptr;
+    plan.allocs.push_back(p);
+    e = cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+    return p;
+}
+
+// Builds the batched launches' tables for the worlds' current grids (the
+// step of graph `which`): waves, the scratch pool, world tables, job lists
+// and work items.
+lenia_status build_plan(lenia_batch *b, int which)
+{
+    GroupPlan &plan = b->plan[which];
+    free_plan(plan);
+    const int n = (int)b->worlds.size();
+    b->grouped.assign(n, 0);
+    std::vector<int> ids;
+    for (int i = 0; i < n && b->group_on; i++)
+        if (group_eligible(b->worlds[i])) ids.push_back(i);
+    std::stable_sort(ids.begin(), ids.end(), [&](int a, int c) { return b->worlds[a]->d.N > b->worlds[c]->d.N; });
+    size_t used = 0, need = 0;
+    for (int i : ids) {
+        const size_t sb = group_scratch_bytes(b->worlds[i]);
+        if (plan.waves.empty() || (used + sb > kWaveScratchBytes && !plan.waves.back().worlds.empty())) {
+            plan.waves.emplace_back();
+            used = 0;
+        }
+        plan.waves.back().worlds.push_back(i);
+        used += sb;
+        need = std::max(need, used);
+    }
+    cudaError_t e = cudaSuccess;
+    if (need > b->pool_bytes) {
+        if (b->pool) cudaFree(b->pool);
+        b->pool = nullptr;
+        b->pool_bytes = 0;
+        e = cudaMalloc((void **)&b->pool, need);
+        if (e != cudaSuccess) return bfail(b, LENIA_ERR_OOM, "batched launches: scratch pool of %zu bytes", need);
+        b->pool_bytes = need;
+    }
+    for (GroupWave &wv : plan.waves) {
+        std::vector<BatchWorldDev> table(wv.worlds.size());
+        std::vector<WorkItem> growth, flow, rt[4], adv;
+        struct SizeJobs {
+            std::vector<RowPairJob> fwd;
+            std::vector<PlaneJob> pf, pi;
+            std::vector<InvPairJob> inv;
+        };
+        std::vector<int> sizes;
+        std::vector<SizeJobs> jobs;
+        unsigned char *base = b->pool;
+        for (size_t j = 0; j < wv.worlds.size() && e == cudaSuccess; j++) {
+            lenia_world *w = b->worlds[wv.worlds[j]];
+            const Dims &d = w->d;
+            const size_t N = (size_t)d.N, CN = (size_t)w->C * N, HS = (size_t)d.HS;
+            auto take = [&](size_t bytes) {
+                unsigned char *q = base;
+                base += align256(bytes);
+                return q;
+            };
+            float *H = (float *)take(CN * 4), *U_SUM = (float *)take(CN * 4), *BACK = (float *)take(CN * 4);
+            float *MU = (float *)take(3 * CN * 4), *U = (float *)take((size_t)w->K * N * 4);
+            float2 *XS = (float2 *)take((size_t)w->C * HS * 8), *S = (float2 *)take((size_t)w->K * HS * 8);
+            BatchWorldDev &t = table[j];
+            memset((void *)&t, 0, sizeof(t));
+            t.p = step_params(w);
+            t.fb = flow_buffers(w);
+            t.fb.H = H;
+            t.fb.MU = MU;
+            t.tb = transport_buffers(w);
+            if (t.tb.ARR == w->BACK) t.tb.ARR = BACK;
+            t.tb.MU = MU;
+            t.tb.H = H;
+            t.tb.BACK = BACK;
+            t.gj = growth_jobs(w);
+            for (int k = 0; k < w->K; k++) t.gj.spec[k] = S + (size_t)k * HS;
+            t.ord = channel_order(t.gj);
+            t.lut_rows = w->lut_rows;
+            t.U = U;
+            t.A = w->A;
+            t.H = H;
+            t.U_SUM = U_SUM;
+            t.BACK = BACK;
+            t.err = w->err_flag;
+            const int wj = (int)j;
+            e = flow_tensor_maps(t.p, t.fb, &t.tm_sum, &t.tm_h);
+            const int nf = flow_blocks(d, &t.flow_gx);
+            for (int blk = 0; blk < nf; blk++) flow.push_back({wj, blk});
+            for (int blk = 0, ng = growth_from_u_blocks(d); blk < ng; blk++) growth.push_back({wj, blk});
+            if (transport_form(t.p) == 1) {
+                if (e == cudaSuccess) e = transport_tensor_maps(t.p, t.tb, 1, &t.tm_mu, &t.tm_arr);
+                const int nt = transport_rt_blocks(d, &t.transport_gx);
+                const int v = (t.p.border == kBorderTorus ? 2 : 0) + (t.p.clip == 1.0f ? 1 : 0);
+                for (int blk = 0; blk < nt; blk++) rt[v].push_back({wj, blk});
+            } else {
+                for (int blk = 0, nt = transport_adv_blocks(d); blk < nt; blk++) adv.push_back({wj, blk});
+            }
+            // the transforms, paired as a single world's launches pair them
+            const size_t si = std::find(sizes.begin(), sizes.end(), d.W) - sizes.begin();
+            if (si == sizes.size()) {
+                sizes.push_back(d.W);
+                jobs.emplace_back();
+                GroupSize g;
+                g.W = d.W;
+                g.tw_x_fwd = w->tw_x_fwd;
+                g.tw_x_inv = w->tw_x_inv;
+                g.tw_y_fwd = w->tw_y_fwd;
+                g.tw_y_inv = w->tw_y_inv;
+                wv.sizes.push_back(g);
+            }
+            SizeJobs &sj = jobs[si];
+            for (int c = 0; c < w->C; c += 2) {
+                RowPairJob r;
+                r.in[0] = w->A + (size_t)c * N;
+                r.out[0] = XS + (size_t)c * HS;
+                r.in[1] = c + 1 < w->C ? w->A + (size_t)(c + 1) * N : nullptr;
+                r.out[1] = c + 1 < w->C ? XS + (size_t)(c + 1) * HS : nullptr;
+                sj.fwd.push_back(r);
+            }
+            for (int c = 0; c < w->C; c++) sj.pf.push_back({XS + (size_t)c * HS, XS + (size_t)c * HS, nullptr});
+            const size_t kh = (size_t)d.KX * (d.D / 2 + 1) * (d.H / 2 + 1);
+            for (int k = 0; k < w->K; k++)
+                sj.pi.push_back({XS + (size_t)w->kernels[k].c0 * HS, S + (size_t)k * HS, w->Kc + k * kh});
+            for (int k = 0; k < w->K; k += 2) {
+                InvPairJob q;
+                q.spec[0] = S + (size_t)k * HS;
+                q.out[0] = U + (size_t)k * N;
+                q.spec[1] = k + 1 < w->K ? S + (size_t)(k + 1) * HS : nullptr;
+                q.out[1] = k + 1 < w->K ? U + (size_t)(k + 1) * N : nullptr;
+                sj.inv.push_back(q);
+            }
+        }
+        wv.ws = plan_copy(plan, table, e);
+        wv.growth = plan_copy(plan, growth, e);
+        wv.n_growth = (int)growth.size();
+        wv.flow = plan_copy(plan, flow, e);
+        wv.n_flow = (int)flow.size();
+        for (int v = 0; v < 4; v++) {
+            wv.rt[v] = plan_copy(plan, rt[v], e);
+            wv.n_rt[v] = (int)rt[v].size();
+            plan.launches += wv.n_rt[v] > 0;
+        }
+        wv.adv = plan_copy(plan, adv, e);
+        wv.n_adv = (int)adv.size();
+        plan.launches += 2 + (wv.n_adv > 0);
+        for (size_t si = 0; si < sizes.size(); si++) {
+            GroupSize &g = wv.sizes[si];
+            g.fwd = plan_copy(plan, jobs[si].fwd, e);
+            g.n_fwd = (int)jobs[si].fwd.size();
+            g.planes_fwd = plan_copy(plan, jobs[si].pf, e);
+            g.n_planes_fwd = (int)jobs[si].pf.size();
+            g.planes_inv = plan_copy(plan, jobs[si].pi, e);
+            g.n_planes_inv = (int)jobs[si].pi.size();
+            g.inv = plan_copy(plan, jobs[si].inv, e);
+            g.n_inv = (int)jobs[si].inv.size();
+            plan.launches += 4;
+        }
+        if (e != cudaSuccess) break;
+    }
+    if (e != cudaSuccess) {
+        free_plan(plan);
+        b->grouped.assign(n, 0);
+        return bfail(b, e == cudaErrorMemoryAllocation ? LENIA_ERR_OOM : LENIA_ERR_CUDA, "batched launches: %s",
+                     cudaGetErrorString(e));
+    }
+    for (int i : ids) b->grouped[i] = 1;
+    return LENIA_OK;
+}
+
+// The batched launches of one step on stream st.
+cudaError_t launch_plan(const GroupPlan &plan, cudaStream_t st)
+{
+    cudaError_t e = cudaSuccess;
+    for (const GroupWave &wv : plan.waves) {
+        for (const GroupSize &g : wv.sizes)
+            if (e == cudaSuccess) e = launch_fwd_rows_list(g.W, g.tw_x_fwd, RowPairList{g.fwd, g.n_fwd}, st);
+        for (const GroupSize &g : wv.sizes)
+            if (e == cudaSuccess)
+                e = launch_planes_list(g.W, g.tw_y_fwd, g.tw_x_fwd, PlaneJobList{g.planes_fwd, g.n_planes_fwd}, -1, st);
+        for (const GroupSize &g : wv.sizes)
+            if (e == cudaSuccess)
+                e = launch_planes_list(g.W, g.tw_y_inv, g.tw_x_inv, PlaneJobList{g.planes_inv, g.n_planes_inv}, +1, st);
+        for (const GroupSize &g : wv.sizes)
+            if (e == cudaSuccess) e = launch_inv_rows_list(g.W, g.tw_x_inv, InvPairList{g.inv, g.n_inv}, st);
+        if (e == cudaSuccess) e = launch_growth_from_u_multi(wv.ws, wv.growth, wv.n_growth, st);
+        if (e == cudaSuccess) e = launch_flow_multi(wv.ws, wv.flow, wv.n_flow, st);
+        for (int v = 0; v < 4; v++)
+            if (e == cudaSuccess) e = launch_transport_rt_multi(wv.ws, wv.rt[v], wv.n_rt[v], v >= 2, v & 1, st);
+        if (e == cudaSuccess) e = launch_transport_adv_multi(wv.ws, wv.adv, wv.n_adv, st);
+    }
+    return e;
+}
+
 // Captures one step of every world, lanes forked from and joined to the
-// batch stream, into exec[which].
+// batch stream, into exec[which]; worlds that take the batched launches run
+// on the group stream beside the lanes.
 lenia_status capture_step(lenia_batch *b, int which)
 {
-    cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed);
+    lenia_status s = build_plan(b, which);
+    if (s != LENIA_OK) return s;
+    // captured on the batch's own stream (the caller's stream, which the
+    // graph is launched on, may be one that cannot be captured)
+    cudaStream_t cs = b->own_stream;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
     if (e != cudaSuccess) return bfail(b, LENIA_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
-    lenia_status s = LENIA_OK;
-    e = cudaEventRecord(b->fork, b->stream);
+    e = cudaEventRecord(b->fork, cs);
+    int lane_launches = 0;
+    if (e == cudaSuccess && !b->plan[which].waves.empty()) {
+        e = cudaStreamWaitEvent(b->group_stream, b->fork, 0);
+        if (e == cudaSuccess) e = launch_plan(b->plan[which], b->group_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(b->group_join, b->group_stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, b->group_join, 0);
+    }
     for (size_t l = 0; l < b->lanes.size() && e == cudaSuccess && s == LENIA_OK; l++) {
         BatchLane &lane = b->lanes[l];
         e = cudaStreamWaitEvent(lane.stream, b->fork, 0);
         for (int i : lane.worlds) {
             if (e != cudaSuccess || s != LENIA_OK) break;
+            if (b->grouped[i]) continue;
             lenia_world *w = b->worlds[i];
             w->stream = lane.stream;
             s = step_once(w);
+            lane_launches += w->launches;
             if (s != LENIA_OK) b->err = "world " + std::to_string(i) + ": " + w->err;
         }
         if (e == cudaSuccess) e = cudaEventRecord(lane.join, lane.stream);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, lane.join, 0);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, lane.join, 0);
     }
+    b->lane_launches[which] = lane_launches;
+    // the batched launches wrote the worlds' next grids
+    for (size_t i = 0; i < b->worlds.size(); i++)
+        if (b->grouped[i]) std::swap(b->worlds[i]->A, b->worlds[i]->A_next);
+
     cudaGraph_t graph = nullptr;
-    const cudaError_t e2 = cudaStreamEndCapture(b->stream, &graph);
+    const cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
     for (lenia_world *w : b->worlds) w->stream = b->stream;
     if (s != LENIA_OK) {
         if (graph) cudaGraphDestroy(graph);
@@ -1507,6 +1831,8 @@ lenia_status lenia_batch_create(const LeniaWorldDesc *descs, const LeniaKernelPa
     cudaError_t e = cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking);
     b->stream = b->own_stream;
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->group_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->group_join, cudaEventDisableTiming);
     lenia_status s = LENIA_OK;
     for (BatchLane &lane : b->lanes) {
         if (e != cudaSuccess || s != LENIA_OK) break;
@@ -1695,12 +2021,34 @@ lenia_status lenia_batch_stats(lenia_batch *b, float fill_threshold, double *out
     return LENIA_OK;
 }
 
-int lenia_batch_launches_per_step(const lenia_batch *b)
+lenia_status lenia_batch_set_batched_launches(lenia_batch *b, int on)
+{
+    if (!b) return LENIA_ERR_INVALID_ARG;
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return bfail(b, LENIA_ERR_CUDA, "set_batched_launches: %s", cudaGetErrorString(e));
+    b->group_on = on != 0;
+    for (cudaGraphExec_t &g : b->exec)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    lenia_status s = capture_step(b, b->parity);
+    if (s == LENIA_OK) s = capture_step(b, b->parity ^ 1);
+    return s;
+}
+
+int lenia_batch_grouped_worlds(const lenia_batch *b)
 {
     if (!b) return 0;
     int n = 0;
-    for (const lenia_world *w : b->worlds) n += w->launches;
+    for (char g : b->grouped) n += g != 0;
     return n;
+}
+
+int lenia_batch_launches_per_step(const lenia_batch *b)
+{
+    if (!b) return 0;
+    return b->lane_launches[b->parity] + b->plan[b->parity].launches;
 }
 
 const char *lenia_batch_last_error(const lenia_batch *b) { return b ? b->err.c_str() : "null batch"; }

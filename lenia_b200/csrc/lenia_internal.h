@@ -2,6 +2,7 @@
 // kernels of the 3D Flow Lenia step.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -126,6 +127,84 @@ struct TransportBuffers {
     float *TT;           // debug: pre-clamp TT, or null
     int *err;            // bit 2 set when a tile copy did not complete in time
 };
+
+// ---- batches of worlds as one launch per stage -------------------------
+// Job lists in device memory: one launch transforms the fields of many
+// worlds of one grid size (each entry is what a single world's launch would
+// take; entries of different worlds never share a transform).
+struct RowPairJob {       // forward rows: two real fields -> half spectra
+    const float *in[2];   // in[1] may be null
+    float2 *out[2];
+};
+struct PlaneJob {         // plane pass of one half spectrum
+    const float2 *src;
+    float2 *dst;
+    const float *kc;      // octant kernel spectrum, or null
+};
+struct InvPairJob {       // inverse rows: two half spectra -> fields / N
+    const float2 *spec[2];  // spec[1] may be null
+    float *out[2];
+};
+struct RowPairList { const RowPairJob *j; int n; };
+struct PlaneJobList { const PlaneJob *j; int n; };
+struct InvPairList { const InvPairJob *j; int n; };
+
+// The kernels grouped by target channel c1, in kernel order within a group
+// (the order of the growth from u_k).
+struct ChannelOrder {
+    int k[kMaxKernels];
+};
+
+// Everything a world's growth-from-u, flow and transport launches take, in
+// device memory for the batched launches (tensor maps first: 64-byte aligned).
+struct alignas(64) BatchWorldDev {
+    CUtensorMap tm_sum, tm_h;    // flow: SUM and H tiles
+    CUtensorMap tm_mu, tm_arr;   // transport: MU and ARR tiles
+    StepParams p;
+    FlowBuffers fb;
+    TransportBuffers tb;
+    GrowthJobs gj;
+    ChannelOrder ord;
+    const float *lut_rows, *U, *A;
+    float *H, *U_SUM, *BACK;
+    int *err;
+    int flow_gx;                 // flow blocks along x*y (the launch's x extent for this world)
+    int transport_gx;            // transport (tiled) blocks along x*y
+};
+
+// One block of a batched launch: world index and the block's index within
+// that world's own launch (flattened x fastest).
+struct WorkItem {
+    int world;
+    int block;
+};
+
+// Batched launches (kernels_*.cu): grid sizes W < 128 (the one-block-per-plane
+// transforms); the job lists, world table and work items live in device memory.
+bool list_size_supported(int W);
+cudaError_t launch_fwd_rows_list(int W, const float2 *tw_x, RowPairList jobs, cudaStream_t st);
+cudaError_t launch_planes_list(int W, const float2 *tw_y, const float2 *tw_z, PlaneJobList jobs, int sign,
+                               cudaStream_t st);
+cudaError_t launch_inv_rows_list(int W, const float2 *tw_x_inv, InvPairList jobs, cudaStream_t st);
+cudaError_t launch_growth_from_u_multi(const BatchWorldDev *ws, const WorkItem *items, int n_items, cudaStream_t st);
+cudaError_t launch_flow_multi(const BatchWorldDev *ws, const WorkItem *items, int n_items, cudaStream_t st);
+// RT with dd = 1 (the tiled gather) for worlds sharing torus/clip-1 flags; ADV per cell
+cudaError_t launch_transport_rt_multi(const BatchWorldDev *ws, const WorkItem *items, int n_items, bool torus,
+                                      bool clip1, cudaStream_t st);
+cudaError_t launch_transport_adv_multi(const BatchWorldDev *ws, const WorkItem *items, int n_items, cudaStream_t st);
+// Tensor maps of a world's flow and tiled-transport launches (for the world
+// table of the batched launches); the transport kernel form of a world
+// (1: tiled, dd = 1; 2: tiled, dd = 2; 0: per cell).
+cudaError_t flow_tensor_maps(const StepParams &p, const FlowBuffers &b, CUtensorMap *tm_sum, CUtensorMap *tm_h);
+cudaError_t transport_tensor_maps(const StepParams &p, const TransportBuffers &b, int dd, CUtensorMap *tm_mu,
+                                  CUtensorMap *tm_arr);
+int transport_form(const StepParams &p);
+// Blocks of a world's own launches (the work-item counts of the batched ones).
+int flow_blocks(const Dims &d, int *gx);
+int transport_rt_blocks(const Dims &d, int *gx);
+int transport_adv_blocks(const Dims &d);
+int growth_from_u_blocks(const Dims &d);
+ChannelOrder channel_order(const GrowthJobs &jobs);
 
 // Programmatic dependent launch between the kernels of a step (forward rows,
 // planes, growth, flow, transport): a kernel lets the next one launch once

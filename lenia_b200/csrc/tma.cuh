@@ -85,6 +85,15 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
+// Asks L2 for a tile (no shared memory, no barrier): a later tma_load_4d of
+// the same box then reads L2 instead of DRAM.
+__device__ __forceinline__ void tma_prefetch_4d(const CUtensorMap *map, int x, int y, int z, int w)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];\n" ::"l"((uint64_t)map),
+                 "r"(x), "r"(y), "r"(z), "r"(w)
+                 : "memory");
+}
+
 // Host: encodes a tiled float32 tensor map over a dense array of `rank`
 // dimensions (dims[0] fastest) with a box of `box` elements per dimension,
 // zero fill out of bounds.  Returns cudaErrorInvalidValue when the driver

@@ -101,7 +101,51 @@ def test_batch_matches_worlds_stepped_alone():
             for name in ("A", "V", "GA", "SUM"):
                 got, want = b.get(i, name), w.get(name)
                 assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (i, name, steps)
-    assert b.launches_per_step() >= 6 * len(wls)
+    # every world takes the batched launches: fewer launches than worlds x stages
+    assert b.grouped_worlds() == len(wls)
+    assert 0 < b.launches_per_step() < 6 * len(wls)
+    for w in alone:
+        w.close()
+    b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("batched", [True, False])
+def test_config3_mix_matches_worlds_stepped_alone(batched):
+    """Every config-3 size (24 .. 96), RT and advection, plus two worlds the
+    batched launches do not take (dd = 2, and central differences with the
+    blur), stepped in one batch with the batched launches on and off: every
+    world bit for bit as stepped alone."""
+    import dataclasses
+    from lenia_b200.batch import Batch
+    from lenia_b200.world import World
+    wls = P.config3(16, seed=21)
+    extra = P.config3(2, seed=22, sizes=(32,))
+    extra[0] = P.Workload(dataclasses.replace(extra[0].desc, mode_type=P.MODE_RT, sigma=1.2, dd=2.0),
+                          extra[0].kernels, extra[0].A0)
+    extra[1] = P.Workload(dataclasses.replace(extra[1].desc, blur_central_diff=True), extra[1].kernels, extra[1].A0)
+    wls = wls + extra
+    b = Batch([wl.desc for wl in wls], [wl.kernels for wl in wls], lanes=4)
+    if not batched:
+        b.set_batched_launches(False)
+    for i, wl in enumerate(wls):
+        b.set_state(i, wl.A0)
+    assert b.grouped_worlds() == (16 if batched else 0)
+    alone = []
+    for wl in wls:
+        w = World(wl.desc, wl.kernels)
+        w.set_state(wl.A0.ravel())
+        alone.append(w)
+    for steps in (1, 2):
+        b.step(steps)
+        for w in alone:
+            w.step(steps)
+        b.sync()
+        for i, w in enumerate(alone):
+            for name in ("A", "V", "GA", "SUM"):
+                got, want = b.get(i, name), w.get(name)
+                assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (i, wls[i].desc.width, name,
+                                                                                     steps)
     for w in alone:
         w.close()
     b.close()
