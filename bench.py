@@ -623,7 +623,7 @@ def run_ours(args):
     barrier()
     mesh_ms = m0.elapsed_time(m1) / mesh_runs
     mesh = {"ms_per_mesh": mesh_ms, "cubes_per_s": C * N / (mesh_ms / 1000.0),
-            "vertices": mesher.n_vertices, "triangles": mesher.n_triangles, "gpu_launches_per_mesh": 5}
+            "vertices": mesher.n_vertices, "triangles": mesher.n_triangles, "gpu_launches_per_mesh": 6}
     mesher.close()
 
     # config 1's schedule: 500 steps with mesh snapshots, the grid of every

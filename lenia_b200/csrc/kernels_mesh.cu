@@ -88,7 +88,7 @@ __host__ __device__ constexpr unsigned mc_edge_desc(int e)
                       mc_off(e, 2) << 10);
 }
 
-__device__ __forceinline__ unsigned active_edges(int cs)
+__host__ __device__ __forceinline__ unsigned active_edges(int cs)
 {
     unsigned m = 0;
 #pragma unroll
@@ -104,6 +104,7 @@ struct McTables {
     unsigned short owned[64];
     unsigned edge[12];              // mc_edge_desc
     unsigned char axis_edges[12];   // mc_axis_edge(ax, j) at 4 * ax + j
+    unsigned short act[256];        // per case: active_edges(case)
 };
 
 constexpr int kMcMaxFields = 3;
@@ -150,9 +151,10 @@ __device__ __forceinline__ void load_corners(const float *f, const float *halo, 
 {
     const int W = g.W, WH = g.W * g.H;
     if (gx + 1 < g.W && gy + 1 < g.H && gz + 1 < g.D) {
-        const float *p = f + gx + gy * W + (long long)gz * WH;
+        // cells < 2^27: 32-bit offsets
+        const float *p = f + (gx + gy * W + gz * WH);
 #pragma unroll
-        for (int i = 0; i < 8; i++) v[i] = __ldg(p + mc_cx(i) + mc_cy(i) * W + (long long)mc_cz(i) * WH);
+        for (int i = 0; i < 8; i++) v[i] = __ldg(p + (mc_cx(i) + mc_cy(i) * W + mc_cz(i) * WH));
         return;
     }
 #pragma unroll
@@ -162,7 +164,7 @@ __device__ __forceinline__ void load_corners(const float *f, const float *halo, 
         if (x >= g.W) x -= g.W;
         if (y >= g.H) y -= g.H;
         if (z >= g.D) z -= g.D;
-        v[i] = out > 1 ? 0.0f : __ldg((out ? halo : f) + x + y * W + (long long)z * WH);
+        v[i] = out > 1 ? 0.0f : __ldg((out ? halo : f) + (x + y * W + z * WH));
     }
 }
 
@@ -234,273 +236,332 @@ __device__ __forceinline__ unsigned block_scan(unsigned v, unsigned *s_warp, uns
     return base + x - v;
 }
 
-// Cube of chunk `chunk`, thread threadIdx.x: slab s, chunk b in the slab.
+// Cube k of chunk `chunk`: slab s, chunk b in the slab, coordinates, index.
 struct CubeRef {
     int s, b, z0, z1, gx, gy, gz;
     long long p;
     bool valid;
 };
 
-__device__ __forceinline__ CubeRef cube_of(const McGeom &g, int chunk)
+__device__ __forceinline__ CubeRef cube_at(const McGeom &g, int chunk, unsigned k)
 {
     CubeRef r;
     r.s = chunk / g.nblk;
     r.b = chunk - r.s * g.nblk;
     slab_range(g, r.s, r.z0, r.z1);
-    const long long WH = (long long)g.W * g.H;
-    const long long i = (long long)r.b * kMcThreads + threadIdx.x;
-    r.valid = i < WH * (r.z1 - r.z0);
-    r.p = r.z0 * WH + (r.valid ? i : 0);
-    r.gz = (int)(r.p / WH);
-    const int rem = (int)(r.p - r.gz * WH);
-    r.gy = rem / g.W;
-    r.gx = rem - r.gy * g.W;
+    // cells < 2^27 (512^3): 32-bit unsigned index arithmetic
+    const unsigned WH = (unsigned)g.W * (unsigned)g.H;
+    const unsigned i = (unsigned)r.b * kMcThreads + k;
+    r.valid = i < WH * (unsigned)(r.z1 - r.z0);
+    const unsigned p = (unsigned)r.z0 * WH + (r.valid ? i : 0u);
+    r.p = p;
+    const unsigned gz = p / WH, rem = p - gz * WH, gy = rem / (unsigned)g.W;
+    r.gz = (int)gz;
+    r.gy = (int)gy;
+    r.gx = (int)(rem - gy * (unsigned)g.W);
     return r;
 }
 
-// Per chunk (one block of kMcThreads cubes) and channel: the chunk's
-// triangle and created-vertex totals, packed as tri | vert << 32.  Each thread
-// walks its cube's channels in order (a vertex shared between channels
-// belongs to the first channel that intersects its edge), writes the case
-// indices, and keeps its counts per channel; one block reduction at the end.
-__global__ void __launch_bounds__(kMcThreads) k_mc_count(McGeom g, const McTables *__restrict__ tab,
+// Cube threadIdx.x of chunk `chunk` (one cube per thread of a block).
+__device__ __forceinline__ CubeRef cube_of(const McGeom &g, int chunk) { return cube_at(g, chunk, threadIdx.x); }
+
+#ifndef LENIA_MC_COUNT_MINB
+#define LENIA_MC_COUNT_MINB 3
+#endif
+// Per chunk (kMcThreads consecutive cubes of a slab) and channel: the
+// chunk's triangle and created-vertex totals, packed as tri | vert << 32.
+// One warp per chunk: lane l takes cubes l, l + 32, ... of it, walks each
+// cube's channels in order (a vertex shared between channels belongs to the
+// first channel that intersects its edge), writes the case indices and keeps
+// its counts per channel; one warp reduction per channel at the end, so no
+// block barrier waits on the slowest warp.
+__global__ void __launch_bounds__(kMcThreads, LENIA_MC_COUNT_MINB) k_mc_count(McGeom g, const McTables *__restrict__ tab,
                                                         unsigned char *__restrict__ cases,
                                                         unsigned long long *__restrict__ blk)
 {
     __shared__ McTables s_tab;
-    __shared__ unsigned s_part[kMcWarps][LENIA_MAX_CHANNELS];
     load_tables(tab, s_tab);
     const int nchunks = g.slabs * g.nblk;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
-        const CubeRef q = cube_of(g, chunk);
-        const unsigned owned = q.valid ? s_tab.owned[boundary_class(g, q.gx, q.gy, q.gz, q.z0, q.z1)] : 0u;
-        unsigned packed[LENIA_MAX_CHANNELS] = {0u, 0u, 0u, 0u};  // nt | nn << 16 per channel
+    const unsigned lane = threadIdx.x & 31;
+    const int nwarps = gridDim.x * kMcWarps;
+    for (int chunk = blockIdx.x * kMcWarps + (int)(threadIdx.x >> 5); chunk < nchunks; chunk += nwarps) {
+        // nt | nn << 16 per channel: a lane's 8 cubes and the warp's 256
+        // (at most 5 triangles and 12 vertices per cube and field) fit
+        unsigned packed[LENIA_MAX_CHANNELS] = {0u, 0u, 0u, 0u};
 #pragma unroll 1
-        for (int f = 0; f < g.F; f++) {
-            // every channel's corners in flight at once, then the cases in
-            // channel order (a shared vertex belongs to the first channel
-            // that cuts its edge)
-            float v[LENIA_MAX_CHANNELS][8];
+        for (unsigned j = 0; j < kMcThreads / 32; j++) {
+            const CubeRef q = cube_at(g, chunk, j * 32 + lane);
+            const unsigned owned = q.valid ? s_tab.owned[boundary_class(g, q.gx, q.gy, q.gz, q.z0, q.z1)] : 0u;
+#pragma unroll 1
+            for (int f = 0; f < g.F; f++) {
+                // every channel's corners in flight at once, then the cases
+                // in channel order
+                float v[LENIA_MAX_CHANNELS][8];
 #pragma unroll
-            for (int c = 0; c < LENIA_MAX_CHANNELS; c++)
-                if (c < g.C && q.valid) load_corners(g.fld[f] + c * g.N, g.halo[f] + c * g.N, g, q.gx, q.gy, q.gz, v[c]);
-            unsigned prev = 0u;
+                for (int c = 0; c < LENIA_MAX_CHANNELS; c++)
+                    if (c < g.C && q.valid)
+                        load_corners(g.fld[f] + c * g.N, g.halo[f] + c * g.N, g, q.gx, q.gy, q.gz, v[c]);
+                unsigned prev = 0u;
 #pragma unroll
-            for (int c = 0; c < LENIA_MAX_CHANNELS; c++) {
-                if (c >= g.C) break;
-                int cs = 0;
-                if (q.valid) {
+                for (int c = 0; c < LENIA_MAX_CHANNELS; c++) {
+                    if (c >= g.C) break;
+                    int cs = 0;
+                    if (q.valid) {
 #pragma unroll
-                    for (int i = 0; i < 8; i++) cs |= (v[c][i] > g.iso) << i;
-                    cases[fc_off(g, f, c) + q.p] = (unsigned char)cs;
+                        for (int i = 0; i < 8; i++) cs |= (v[c][i] > g.iso) << i;
+                        cases[fc_off(g, f, c) + q.p] = (unsigned char)cs;
+                    }
+                    const unsigned act = s_tab.act[cs];
+                    const unsigned nn = __popc(owned & act & ~prev);
+                    if (g.share) prev |= act;
+                    packed[c] += (unsigned)tri_count(s_tab.tri[cs]) | nn << 16;
                 }
-                const unsigned act = active_edges(cs);
-                const unsigned nn = __popc(owned & act & ~prev);
-                if (g.share) prev |= act;
-                packed[c] += (unsigned)tri_count(s_tab.tri[cs]) | nn << 16;
             }
         }
-        // block sums per channel (at most 5 triangles and 12 vertices per cube
-        // and field: 16 bits per count hold a chunk)
+        const int s = chunk / g.nblk, b = chunk - s * g.nblk;
+        unsigned long long mine = 0;
 #pragma unroll
         for (int c = 0; c < LENIA_MAX_CHANNELS; c++) {
             const unsigned w = __reduce_add_sync(0xffffffffu, packed[c]);
-            if (lane == 0) s_part[wid][c] = w;
+            if (lane == (unsigned)c) mine = (unsigned long long)(w & 0xffffu) | (unsigned long long)(w >> 16) << 32;
         }
-        __syncthreads();
-        if (threadIdx.x < g.C) {
-            const int c = threadIdx.x;
-            unsigned long long t = 0, v = 0;
-            for (int w = 0; w < kMcWarps; w++) {
-                t += s_part[w][c] & 0xffffu;
-                v += s_part[w][c] >> 16;
-            }
-            blk[((long long)q.s * g.C + c) * g.nblk + q.b] = t | v << 32;
-        }
-        __syncthreads();
+        if (lane < (unsigned)g.C) blk[((long long)s * g.C + lane) * g.nblk + b] = mine;
     }
 }
 
-// Exclusive scan of the M packed chunk totals in place (one block of 1024
-// threads, tiles of 8192 with a running carry; each thread scans 8
-// consecutive values), and the list of chunk-channels with triangles, in
-// order; totals[0..2] = triangles, vertices, listed chunk-channels.  Packed
-// addition is exact while the triangle total stays below 2^32 (the host
-// checks it).
+// Exclusive scan of the M packed chunk totals in place, and the list of
+// chunk-channels with triangles in order; totals[0..2] = triangles, vertices,
+// listed chunk-channels.  Packed addition is exact while the triangle total
+// stays below 2^32 (the host checks it).  Two launches over tiles of
+// kScanTile values (each thread scans kScanPer consecutive values):
+// k_mc_scan_tiles scans every tile on its own and lists its chunk-channels
+// with triangles at the tile's slot of a scratch list; k_mc_scan_add adds
+// the totals of the tiles before each tile and moves its list entries to
+// their final places.
 constexpr int kScanThreads = 1024;
 constexpr int kScanPer = 8;
-__global__ void __launch_bounds__(kScanThreads) k_mc_scan(unsigned long long *blk, long long M, long long *totals,
-                                                         long long *list)
+constexpr int kScanTile = kScanThreads * kScanPer;
+
+__global__ void __launch_bounds__(kScanThreads) k_mc_scan_tiles(unsigned long long *__restrict__ blk, long long M,
+                                                               unsigned long long *__restrict__ tile_tot,
+                                                               long long *__restrict__ tile_cnt,
+                                                               long long *__restrict__ list_tmp)
 {
     __shared__ unsigned long long s_warp[kScanThreads / 32];
     __shared__ unsigned s_lwarp[kScanThreads / 32];
-    __shared__ unsigned long long s_carry;
-    __shared__ long long s_lcarry;
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-    if (t == 0) {
-        s_carry = 0;
-        s_lcarry = 0;
+    const long long base = (long long)blockIdx.x * kScanTile;
+    const long long i0 = base + (long long)t * kScanPer;
+    unsigned long long v[kScanPer];
+#pragma unroll
+    for (int j = 0; j < kScanPer; j++) v[j] = i0 + j < M ? blk[i0 + j] : 0ull;
+    unsigned long long sum = 0;
+    unsigned nz = 0;  // chunk-channels of this thread with triangles
+#pragma unroll
+    for (int j = 0; j < kScanPer; j++) {
+        sum += v[j];
+        nz += (v[j] & 0xffffffffull) != 0;
+    }
+    // inclusive warp scans of the thread sums and counts, then of the warp sums
+    unsigned long long x = sum;
+    unsigned xn = nz;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+        const unsigned yn = __shfl_up_sync(0xffffffffu, xn, o);
+        if (lane >= o) {
+            x += y;
+            xn += yn;
+        }
+    }
+    if (lane == 31) {
+        s_warp[wid] = x;
+        s_lwarp[wid] = xn;
     }
     __syncthreads();
-    for (long long base = 0; base < M; base += (long long)kScanThreads * kScanPer) {
-        unsigned long long v[kScanPer];
-        const long long i0 = base + (long long)t * kScanPer;
-#pragma unroll
-        for (int j = 0; j < kScanPer; j++) v[j] = i0 + j < M ? blk[i0 + j] : 0ull;
-        unsigned long long sum = 0;
-        unsigned nz = 0;  // chunk-channels of this thread with triangles
-#pragma unroll
-        for (int j = 0; j < kScanPer; j++) {
-            sum += v[j];
-            nz += (v[j] & 0xffffffffull) != 0;
-        }
-        // inclusive warp scans of the thread sums and counts, then of the
-        // warp sums
-        unsigned long long x = sum;
-        unsigned xn = nz;
+    if (wid == 0) {
+        unsigned long long w = s_warp[lane];
+        unsigned wn = s_lwarp[lane];
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
-            const unsigned yn = __shfl_up_sync(0xffffffffu, xn, o);
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
+            const unsigned yn = __shfl_up_sync(0xffffffffu, wn, o);
             if (lane >= o) {
-                x += y;
-                xn += yn;
+                w += y;
+                wn += yn;
             }
         }
-        if (lane == 31) {
-            s_warp[wid] = x;
-            s_lwarp[wid] = xn;
-        }
-        __syncthreads();
-        if (wid == 0) {
-            unsigned long long w = s_warp[lane];
-            unsigned wn = s_lwarp[lane];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
-                const unsigned yn = __shfl_up_sync(0xffffffffu, wn, o);
-                if (lane >= o) {
-                    w += y;
-                    wn += yn;
-                }
-            }
-            s_warp[lane] = w;
-            s_lwarp[lane] = wn;
-        }
-        __syncthreads();
-        unsigned long long run = s_carry + (wid > 0 ? s_warp[wid - 1] : 0ull) + x - sum;
-        long long lrun = s_lcarry + (wid > 0 ? s_lwarp[wid - 1] : 0u) + xn - nz;
-#pragma unroll
-        for (int j = 0; j < kScanPer; j++) {
-            if (i0 + j < M) {
-                blk[i0 + j] = run;
-                if ((v[j] & 0xffffffffull) != 0) list[lrun++] = i0 + j;
-            }
-            run += v[j];
-        }
-        __syncthreads();
-        if (t == kScanThreads - 1) {
-            s_carry = run;
-            s_lcarry = lrun;
-        }
-        __syncthreads();
+        s_warp[lane] = w;
+        s_lwarp[lane] = wn;
     }
-    if (t == 0) {
-        totals[0] = (long long)(s_carry & 0xffffffffull);
-        totals[1] = (long long)(s_carry >> 32);
-        totals[2] = s_lcarry;
+    __syncthreads();
+    unsigned long long run = (wid > 0 ? s_warp[wid - 1] : 0ull) + x - sum;
+    long long lrun = (long long)(wid > 0 ? s_lwarp[wid - 1] : 0u) + xn - nz;
+#pragma unroll
+    for (int j = 0; j < kScanPer; j++) {
+        if (i0 + j < M) {
+            blk[i0 + j] = run;
+            if ((v[j] & 0xffffffffull) != 0) list_tmp[base + lrun++] = i0 + j;
+        }
+        run += v[j];
+    }
+    if (t == kScanThreads - 1) {
+        tile_tot[blockIdx.x] = run;
+        tile_cnt[blockIdx.x] = lrun;
     }
 }
 
+__global__ void __launch_bounds__(kScanThreads) k_mc_scan_add(unsigned long long *__restrict__ blk, long long M,
+                                                             const unsigned long long *__restrict__ tile_tot,
+                                                             const long long *__restrict__ tile_cnt,
+                                                             const long long *__restrict__ list_tmp,
+                                                             long long *__restrict__ list, long long *totals)
+{
+    __shared__ unsigned long long s_off;
+    __shared__ long long s_loff;
+    const int t = threadIdx.x, lane = t & 31;
+    const int b = blockIdx.x;
+    if (t < 32) {
+        // the totals of the tiles before this one, in tile order per lane
+        // (integer sums: the order does not change them)
+        unsigned long long off = 0;
+        long long loff = 0;
+        for (int k = lane; k < b; k += 32) {
+            off += tile_tot[k];
+            loff += tile_cnt[k];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            off += __shfl_down_sync(0xffffffffu, off, o);
+            loff += __shfl_down_sync(0xffffffffu, loff, o);
+        }
+        if (lane == 0) {
+            s_off = off;
+            s_loff = loff;
+            if (b == (int)gridDim.x - 1) {
+                const unsigned long long all = off + tile_tot[b];
+                totals[0] = (long long)(all & 0xffffffffull);
+                totals[1] = (long long)(all >> 32);
+                totals[2] = loff + tile_cnt[b];
+            }
+        }
+    }
+    __syncthreads();
+    const unsigned long long off = s_off;
+    const long long loff = s_loff, base = (long long)b * kScanTile;
+    for (int k = t; k < kScanTile; k += kScanThreads)
+        if (base + k < M) blk[base + k] += off;
+    const long long n = tile_cnt[b];
+    for (long long k = t; k < n; k += kScanThreads) list[loff + k] = list_tmp[base + k];
+}
+
+// Chunk-channel `o` of the listed ones: its channel c and chunk index (slab
+// major), from o = (slab * C + c) * nblk + chunk-in-slab.
+__device__ __forceinline__ void listed_chunk(const McGeom &g, unsigned o, int &c, int &chunk)
+{
+    const unsigned nb = (unsigned)g.nblk, sc = o / nb;
+    c = (int)(sc % (unsigned)g.C);
+    chunk = (int)((sc / (unsigned)g.C) * nb + (o - sc * nb));
+}
+
+// Triangles (face normals) and created vertices of the listed chunk-channels
+// (the others' cubes are all case 0 or 255: no edge is cut there).  The
+// blocks walk the list, whose length the scan left in totals[2], with stride
+// gridDim.x.  Writes past the output capacity (cap_t triangles, cap_v
+// vertices) are skipped: the host compares the totals with the capacity
+// afterwards and runs the pass again into larger buffers.
 __global__ void __launch_bounds__(kMcThreads) k_mc_emit(McGeom g, const McTables *__restrict__ tab,
                                                        const unsigned char *__restrict__ cases,
                                                        const unsigned long long *__restrict__ blk,
                                                        const long long *__restrict__ list,
+                                                       const long long *__restrict__ totals,
                                                        int *__restrict__ tri_base, int *__restrict__ vert_base,
                                                        float *__restrict__ fn, float *__restrict__ pos,
-                                                       int *__restrict__ vch, unsigned long long *__restrict__ vsrc)
+                                                       int *__restrict__ vch, unsigned long long *__restrict__ vsrc,
+                                                       long long cap_t, long long cap_v)
 {
     __shared__ McTables s_tab;
     __shared__ unsigned s_warp[kMcWarps];
+    const long long nlist = totals[2];
+    if (blockIdx.x >= nlist) return;
     load_tables(tab, s_tab);
-    // one chunk-channel with triangles per block (the other chunk-channels'
-    // cubes are all case 0 or 255: no edge is cut there)
-    {
-        const long long o = list[blockIdx.x];
-        const int c = (int)((o / g.nblk) % g.C);
-        const CubeRef q = cube_of(g, (int)(o / ((long long)g.nblk * g.C)) * g.nblk + (int)(o % g.nblk));
+    for (long long li = blockIdx.x; li < nlist; li += gridDim.x) {
+        const unsigned o = (unsigned)list[li];
+        int c, chunk;
+        listed_chunk(g, o, c, chunk);
+        const CubeRef q = cube_of(g, chunk);
         const unsigned owned = q.valid ? s_tab.owned[boundary_class(g, q.gx, q.gy, q.gz, q.z0, q.z1)] : 0u;
-        {
-            int cs[kMcMaxFields] = {0, 0, 0};
-            unsigned newm[kMcMaxFields] = {0u, 0u, 0u};
-            unsigned nt = 0, nn = 0;
+        int cs[kMcMaxFields] = {0, 0, 0};
+        unsigned newm[kMcMaxFields] = {0u, 0u, 0u};
+        unsigned nt = 0, nn = 0;
 #pragma unroll
-            for (int f = 0; f < kMcMaxFields; f++) {
-                if (f >= g.F) break;
-                cs[f] = q.valid ? cases[fc_off(g, f, c) + q.p] : 0;
-                // edges the cube's earlier channels cut (they own those vertices)
-                unsigned prev = 0u;
-                if (g.share && q.valid)
-                    for (int c2 = 0; c2 < c; c2++) prev |= active_edges(cases[fc_off(g, f, c2) + q.p]);
-                const unsigned act = active_edges(cs[f]);
-                newm[f] = owned & act & ~prev;
-                nt += tri_count(s_tab.tri[cs[f]]);
-                nn += __popc(newm[f]);
+        for (int f = 0; f < kMcMaxFields; f++) {
+            if (f >= g.F) break;
+            cs[f] = q.valid ? cases[fc_off(g, f, c) + q.p] : 0;
+            // edges the cube's earlier channels cut (they own those vertices)
+            unsigned prev = 0u;
+            if (g.share && q.valid)
+                for (int c2 = 0; c2 < c; c2++) prev |= s_tab.act[cases[fc_off(g, f, c2) + q.p]];
+            const unsigned act = s_tab.act[cs[f]];
+            newm[f] = owned & act & ~prev;
+            nt += tri_count(s_tab.tri[cs[f]]);
+            nn += __popc(newm[f]);
+        }
+        unsigned total;
+        const unsigned pre = block_scan(nt | nn << 16, s_warp, &total);
+        if (nt == 0) continue;
+        long long tb = (long long)(blk[o] & 0xffffffffull) + (pre & 0xffff);
+        long long vb = (long long)(blk[o] >> 32) + (pre >> 16);
+#pragma unroll
+        for (int f = 0; f < kMcMaxFields; f++) {
+            if (f >= g.F) break;
+            const unsigned long long tl = s_tab.tri[cs[f]];
+            const int ntf = tri_count(tl);
+            if (ntf == 0) continue;
+            tri_base[fc_off(g, f, c) + q.p] = (int)tb;
+            if (newm[f]) vert_base[fc_off(g, f, c) + q.p] = (int)vb;
+            float v[8];
+            load_corners(g.fld[f] + c * g.N, g.halo[f] + c * g.N, g, q.gx, q.gy, q.gz, v);
+            for (int t = 0; t < ntf; t++) {
+                if (tb + t >= cap_t) break;
+                const float3 A = edge_vertex(g, f, s_tab.edge[slot_edge(tl, 3 * t)], v, q.gx, q.gy, q.gz);
+                const float3 B = edge_vertex(g, f, s_tab.edge[slot_edge(tl, 3 * t + 1)], v, q.gx, q.gy, q.gz);
+                const float3 C = edge_vertex(g, f, s_tab.edge[slot_edge(tl, 3 * t + 2)], v, q.gx, q.gy, q.gz);
+                const float ux = B.x - A.x, uy = B.y - A.y, uz = B.z - A.z;
+                const float wx = C.x - A.x, wy = C.y - A.y, wz = C.z - A.z;
+                float *fo = fn + 3 * (tb + t);
+                fo[0] = uy * wz - uz * wy;
+                fo[1] = uz * wx - ux * wz;
+                fo[2] = ux * wy - uy * wx;
             }
-            unsigned total;
-            const unsigned pre = block_scan(nt | nn << 16, s_warp, &total);
-            if (nt == 0) return;
-            long long tb = (long long)(blk[o] & 0xffffffffull) + (pre & 0xffff);
-            long long vb = (long long)(blk[o] >> 32) + (pre >> 16);
-#pragma unroll
-            for (int f = 0; f < kMcMaxFields; f++) {
-                if (f >= g.F) break;
-                const unsigned long long tl = s_tab.tri[cs[f]];
-                const int ntf = tri_count(tl);
-                if (ntf == 0) continue;
-                tri_base[fc_off(g, f, c) + q.p] = (int)tb;
-                if (newm[f]) vert_base[fc_off(g, f, c) + q.p] = (int)vb;
-                float v[8];
-                load_corners(g.fld[f] + c * g.N, g.halo[f] + c * g.N, g, q.gx, q.gy, q.gz, v);
-                for (int t = 0; t < ntf; t++) {
-                    const float3 A = edge_vertex(g, f, s_tab.edge[slot_edge(tl, 3 * t)], v, q.gx, q.gy, q.gz);
-                    const float3 B = edge_vertex(g, f, s_tab.edge[slot_edge(tl, 3 * t + 1)], v, q.gx, q.gy, q.gz);
-                    const float3 C = edge_vertex(g, f, s_tab.edge[slot_edge(tl, 3 * t + 2)], v, q.gx, q.gy, q.gz);
-                    const float ux = B.x - A.x, uy = B.y - A.y, uz = B.z - A.z;
-                    const float wx = C.x - A.x, wy = C.y - A.y, wz = C.z - A.z;
-                    float *fo = fn + 3 * (tb + t);
-                    fo[0] = uy * wz - uz * wy;
-                    fo[1] = uz * wx - ux * wz;
-                    fo[2] = ux * wy - uy * wx;
-                }
-                if (newm[f]) {
-                    unsigned seen = 0;
-                    for (int k = 0; k < 3 * ntf; k++) {
-                        const int e = slot_edge(tl, k);
-                        if ((seen >> e) & 1) continue;
-                        seen |= 1u << e;
-                        if (!((newm[f] >> e) & 1)) continue;
+            if (newm[f]) {
+                unsigned seen = 0;
+                for (int k = 0; k < 3 * ntf; k++) {
+                    const int e = slot_edge(tl, k);
+                    if ((seen >> e) & 1) continue;
+                    seen |= 1u << e;
+                    if (!((newm[f] >> e) & 1)) continue;
+                    if (vb < cap_v) {
                         const float3 P = edge_vertex(g, f, s_tab.edge[e], v, q.gx, q.gy, q.gz);
                         pos[3 * vb] = P.x;
                         pos[3 * vb + 1] = P.y;
                         pos[3 * vb + 2] = P.z;
                         vch[vb] = c + g.C * f;
                         vsrc[vb] = (unsigned long long)(fc_off(g, f, c) + q.p) << 4 | (unsigned)e;
-                        vb++;
                     }
+                    vb++;
                 }
-                tb += ntf;
             }
+            tb += ntf;
         }
     }
 }
 
 // Creator of the vertex on local edge e of cube (gx, gy, gz): the first cube
 // around the edge in scan order inside the slab.  Returns the creator's
-// linear index and its local edge.
+// linear index, its coordinates and its local edge.
 __device__ __forceinline__ long long edge_creator(const McGeom &g, const McTables &t, int e, int gx, int gy, int gz,
-                                                  int z0, int z1, int *e_out)
+                                                  int z0, int z1, int *e_out, int &ox, int &oy, int &oz)
 {
     const unsigned ed = t.edge[e];
     const int ax = (ed >> 6) & 3;
@@ -511,69 +572,75 @@ __device__ __forceinline__ long long edge_creator(const McGeom &g, const McTable
         const int x = Gx - (int)((d2 >> 8) & 1), y = Gy - (int)((d2 >> 9) & 1), z = Gz - (int)((d2 >> 10) & 1);
         if (x >= 0 && x < g.W && y >= 0 && y < g.H && z >= z0 && z < z1) {
             *e_out = e2;
+            ox = x;
+            oy = y;
+            oz = z;
             return x + (long long)y * g.W + (long long)z * g.W * g.H;
         }
     }
     *e_out = e;  // unreachable: the cube itself is always a candidate
+    ox = gx;
+    oy = gy;
+    oz = gz;
     return gx + (long long)gy * g.W + (long long)gz * g.W * g.H;
 }
 
+// Vertex indices of the listed chunk-channels' triangles (the blocks walk
+// the list as in k_mc_emit; triangles past cap_t are skipped).
 __global__ void __launch_bounds__(kMcThreads) k_mc_index(McGeom g, const McTables *__restrict__ tab,
                                                         const unsigned char *__restrict__ cases,
                                                         const int *__restrict__ tri_base,
                                                         const int *__restrict__ vert_base,
                                                         const long long *__restrict__ list,
-                                                        unsigned *__restrict__ idx)
+                                                        const long long *__restrict__ totals,
+                                                        unsigned *__restrict__ idx, long long cap_t)
 {
     __shared__ McTables s_tab;
+    const long long nlist = totals[2];
+    if (blockIdx.x >= nlist) return;
     load_tables(tab, s_tab);
-    const long long WH = (long long)g.W * g.H;
-    // one chunk-channel with triangles per block
-    {
-        const long long o = list[blockIdx.x];
-        const int c = (int)((o / g.nblk) % g.C);
-        const CubeRef q = cube_of(g, (int)(o / ((long long)g.nblk * g.C)) * g.nblk + (int)(o % g.nblk));
-        if (!q.valid) return;
-        {
-            for (int f = 0; f < g.F; f++) {
-                const int cs = cases[fc_off(g, f, c) + q.p];
-                const unsigned long long tl = s_tab.tri[cs];
-                const int nt = tri_count(tl);
-                if (nt == 0) continue;
-                const long long tb = tri_base[fc_off(g, f, c) + q.p];
-                for (int k = 0; k < 3 * nt; k++) {
-                    const int e = slot_edge(tl, k);
-                    // channel that created the vertex
-                    int c0 = c;
-                    if (g.share)
-                        for (int c2 = 0; c2 < c; c2++)
-                            if ((active_edges(cases[fc_off(g, f, c2) + q.p]) >> e) & 1) {
-                                c0 = c2;
-                                break;
-                            }
-                    int eo;
-                    const long long op = edge_creator(g, s_tab, e, q.gx, q.gy, q.gz, q.z0, q.z1, &eo);
-                    const int oz = (int)(op / WH), rem = (int)(op - oz * WH);
-                    const int oy = rem / g.W, ox = rem - oy * g.W;
-                    const int ocs = cases[fc_off(g, f, c0) + op];
-                    unsigned oprev = 0;
-                    if (g.share)
-                        for (int c2 = 0; c2 < c0; c2++) oprev |= active_edges(cases[fc_off(g, f, c2) + op]);
-                    const unsigned onew =
-                        s_tab.owned[boundary_class(g, ox, oy, oz, q.z0, q.z1)] & active_edges(ocs) & ~oprev;
-                    // rank of eo among the creator's new vertices, in first-slot order
-                    const unsigned long long otl = s_tab.tri[ocs];
-                    unsigned seen = 0;
-                    int r = 0;
-                    for (int k2 = 0; k2 < 3 * tri_count(otl); k2++) {
-                        const int e2 = slot_edge(otl, k2);
-                        if ((seen >> e2) & 1) continue;
-                        seen |= 1u << e2;
-                        if (e2 == eo) break;
-                        r += (onew >> e2) & 1;
-                    }
-                    idx[3 * tb + k] = (unsigned)(vert_base[fc_off(g, f, c0) + op] + r);
+    for (long long li = blockIdx.x; li < nlist; li += gridDim.x) {
+        int c, chunk;
+        listed_chunk(g, (unsigned)list[li], c, chunk);
+        const CubeRef q = cube_of(g, chunk);
+        if (!q.valid) continue;
+        for (int f = 0; f < g.F; f++) {
+            const int cs = cases[fc_off(g, f, c) + q.p];
+            const unsigned long long tl = s_tab.tri[cs];
+            const int nt = tri_count(tl);
+            if (nt == 0) continue;
+            const long long tb = tri_base[fc_off(g, f, c) + q.p];
+            if (tb + nt > cap_t) continue;
+            for (int k = 0; k < 3 * nt; k++) {
+                const int e = slot_edge(tl, k);
+                // channel that created the vertex
+                int c0 = c;
+                if (g.share)
+                    for (int c2 = 0; c2 < c; c2++)
+                        if ((s_tab.act[cases[fc_off(g, f, c2) + q.p]] >> e) & 1) {
+                            c0 = c2;
+                            break;
+                        }
+                int eo, ox, oy, oz;
+                const long long op = edge_creator(g, s_tab, e, q.gx, q.gy, q.gz, q.z0, q.z1, &eo, ox, oy, oz);
+                const int ocs = cases[fc_off(g, f, c0) + op];
+                unsigned oprev = 0;
+                if (g.share)
+                    for (int c2 = 0; c2 < c0; c2++) oprev |= s_tab.act[cases[fc_off(g, f, c2) + op]];
+                const unsigned onew =
+                    s_tab.owned[boundary_class(g, ox, oy, oz, q.z0, q.z1)] & s_tab.act[ocs] & ~oprev;
+                // rank of eo among the creator's new vertices, in first-slot order
+                const unsigned long long otl = s_tab.tri[ocs];
+                unsigned seen = 0;
+                int r = 0;
+                for (int k2 = 0; k2 < 3 * tri_count(otl); k2++) {
+                    const int e2 = slot_edge(otl, k2);
+                    if ((seen >> e2) & 1) continue;
+                    seen |= 1u << e2;
+                    if (e2 == eo) break;
+                    r += (onew >> e2) & 1;
                 }
+                idx[3 * tb + k] = (unsigned)(vert_base[fc_off(g, f, c0) + op] + r);
             }
         }
     }
@@ -584,21 +651,26 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_normals(McGeom g, const McTab
                                                           const int *__restrict__ tri_base,
                                                           const unsigned long long *__restrict__ vsrc,
                                                           const float *__restrict__ fn, float *__restrict__ nrm,
-                                                          long long nv)
+                                                          const long long *__restrict__ totals, long long cap_t,
+                                                          long long cap_v)
 {
     __shared__ McTables s_tab;
+    // the vertex count the scan left in totals[1] (vertices past cap_v skipped)
+    const long long nv = totals[1] < cap_v ? totals[1] : cap_v;
+    if ((long long)blockIdx.x * blockDim.x >= nv) return;
     load_tables(tab, s_tab);
-    const long long WH = (long long)g.W * g.H;
+    const unsigned WH = (unsigned)g.W * (unsigned)g.H;
     for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nv;
          v += (long long)gridDim.x * blockDim.x) {
         const unsigned long long src = vsrc[v];
         const int e0 = (int)(src & 15);
-        const long long cp = (long long)(src >> 4);
-        const int fc0 = (int)(cp / g.N);
-        const int f = fc0 / g.C, c0 = fc0 - f * g.C;
-        const long long p0 = cp - fc0 * g.N;
-        const int gz = (int)(p0 / WH), rem = (int)(p0 - gz * WH);
-        const int gy = rem / g.W, gx = rem - gy * g.W;
+        // cube slots < F C N < 2^31: 32-bit unsigned index arithmetic
+        const unsigned cp = (unsigned)(src >> 4);
+        const unsigned fc0 = cp / (unsigned)g.N;
+        const int f = (int)fc0 / g.C, c0 = (int)fc0 - f * g.C;
+        const unsigned p0 = cp - fc0 * (unsigned)g.N;
+        const unsigned uz = p0 / WH, rem = p0 - uz * WH, uy = rem / (unsigned)g.W;
+        const int gz = (int)uz, gy = (int)uy, gx = (int)(rem - uy * (unsigned)g.W);
         int s = gz / (g.D / g.slabs);
         if (s > g.slabs - 1) s = g.slabs - 1;
         int z0, z1;
@@ -609,7 +681,7 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_normals(McGeom g, const McTab
         float nx = 0.0f, ny = 0.0f, nz = 0.0f;
         const int c_end = g.share ? g.C : c0 + 1;
         for (int c = c0; c < c_end; c++) {
-            if (c > c0 && !((active_edges(cases[fc_off(g, f, c) + p0]) >> e0) & 1)) continue;
+            if (c > c0 && !((s_tab.act[cases[fc_off(g, f, c) + p0]] >> e0) & 1)) continue;
             for (int j = 0; j < 4; j++) {
                 const int e2 = s_tab.axis_edges[4 * ax + j];
                 const unsigned d2 = s_tab.edge[e2];
@@ -620,7 +692,7 @@ __global__ void __launch_bounds__(kMcThreads) k_mc_normals(McGeom g, const McTab
                 const unsigned long long tl = s_tab.tri[cases[fc_off(g, f, c) + qp]];
                 const int nt = tri_count(tl);
                 const long long tb = tri_base[fc_off(g, f, c) + qp];
-                for (int t = 0; t < nt; t++) {
+                for (int t = 0; t < nt && tb + t < cap_t; t++) {
                     if (slot_edge(tl, 3 * t) == e2 || slot_edge(tl, 3 * t + 1) == e2 ||
                         slot_edge(tl, 3 * t + 2) == e2) {
                         const float *f = fn + 3 * (tb + t);
@@ -738,6 +810,7 @@ void build_tables(McTables *t)
         t->tri[cs] = w;
     }
     for (int cls = 0; cls < 64; cls++) t->owned[cls] = owned_edges(cls);
+    for (int cs = 0; cs < 256; cs++) t->act[cs] = (unsigned short)active_edges(cs);
     for (int e = 0; e < 12; e++) t->edge[e] = mc_edge_desc(e);
     for (int ax = 0; ax < 3; ax++)
         for (int j = 0; j < 4; j++) t->axis_edges[4 * ax + j] = (unsigned char)mc_axis_edge(ax, j);
@@ -750,12 +823,16 @@ struct lenia_mesher {
     McGeom g;
     int device = 0;
     int grid = 0;
+    int list_grid = 0;
     std::string err;
     McTables *tab = nullptr;
     unsigned char *cases = nullptr;
     int *tri_base = nullptr, *vert_base = nullptr;
     unsigned long long *blk = nullptr;  // per chunk and channel: tri | vert << 32, then its exclusive scan
     long long *list = nullptr;          // chunk-channels with triangles, in order
+    long long *list_tmp = nullptr;      // the same per scan tile (at the tile's first slot)
+    unsigned long long *tile_tot = nullptr;  // per scan tile: its packed total
+    long long *tile_cnt = nullptr;           // per scan tile: its listed chunk-channels
     long long *totals = nullptr, *h_totals = nullptr;
     float *fn = nullptr, *pos = nullptr, *nrm = nullptr;
     int *vch = nullptr;
@@ -874,9 +951,13 @@ lenia_status lenia_mesher_create(const LeniaMeshDesc *desc, lenia_mesher **out)
     for (int f = 0; f < kMcMaxFields; f++)
         for (int a = 0; a < 3; a++) g.off[f][a] = f < g.F ? d.offset[f][a] : 0.0f;
     const long long nchunks = (long long)g.slabs * g.nblk;
-    // one chunk per block up to 32 blocks per SM (resident eight at a time)
-    m->grid = (int)(nchunks < 32LL * nsm ? nchunks : 32LL * nsm);
+    // one warp per chunk, up to six blocks of eight warps per SM
+    const long long count_blocks = (nchunks + kMcWarps - 1) / kMcWarps;
+    m->grid = (int)(count_blocks < 6LL * nsm ? count_blocks : 6LL * nsm);
     const long long M = nchunks * g.C;
+    // the output passes: blocks that walk the listed chunk-channels (and
+    // the vertices) with a stride, eight per SM
+    m->list_grid = (int)(M < 8LL * nsm ? M : 8LL * nsm);
     McTables host;
     build_tables(&host);
     cudaError_t e = cudaSuccess;
@@ -890,6 +971,10 @@ lenia_status lenia_mesher_create(const LeniaMeshDesc *desc, lenia_mesher **out)
     alloc(m->vert_base, sizeof(int) * cubes);
     alloc(m->blk, sizeof(unsigned long long) * (size_t)M);
     alloc(m->list, sizeof(long long) * (size_t)M);
+    alloc(m->list_tmp, sizeof(long long) * (size_t)M);
+    const size_t ntiles = (size_t)((M + kScanTile - 1) / kScanTile);
+    alloc(m->tile_tot, sizeof(unsigned long long) * ntiles);
+    alloc(m->tile_cnt, sizeof(long long) * ntiles);
     alloc(m->totals, 3 * sizeof(long long));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&m->h_totals, 3 * sizeof(long long));
     if (e == cudaSuccess) e = cudaMemcpy(m->tab, &host, sizeof(McTables), cudaMemcpyHostToDevice);
@@ -912,6 +997,9 @@ lenia_status lenia_mesher_destroy(lenia_mesher *m)
     dfree(m->vert_base);
     dfree(m->blk);
     dfree(m->list);
+    dfree(m->list_tmp);
+    dfree(m->tile_tot);
+    dfree(m->tile_cnt);
     dfree(m->totals);
     if (m->h_totals) cudaFreeHost(m->h_totals);
     delete m;
@@ -933,12 +1021,31 @@ lenia_status lenia_mesher_run(lenia_mesher *m, const float *const *fields, const
     m->have_mesh = false;
     const long long M = (long long)g.slabs * g.nblk * g.C;
     k_mc_count<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk);
-    k_mc_scan<<<1, kScanThreads, 0, st>>>(m->blk, M, m->totals, m->list);
+    const unsigned ntiles = (unsigned)((M + kScanTile - 1) / kScanTile);
+    k_mc_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(m->blk, M, m->tile_tot, m->tile_cnt, m->list_tmp);
+    k_mc_scan_add<<<ntiles, kScanThreads, 0, st>>>(m->blk, M, m->tile_tot, m->tile_cnt, m->list_tmp, m->list,
+                                                    m->totals);
     cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return mcuda(m, e, "mesher count");
+    // The output passes take their counts from the scan's totals on the
+    // device, so they follow it without a host round trip; they write only
+    // what fits the current buffers, and run again into larger ones when
+    // the totals read afterwards do not fit.
+    auto outputs = [&]() -> cudaError_t {
+        k_mc_emit<<<m->list_grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk, m->list, m->totals, m->tri_base,
+                                                       m->vert_base, m->fn, m->pos, m->vch, m->vsrc, m->cap_t,
+                                                       m->cap_v);
+        k_mc_index<<<m->list_grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vert_base, m->list,
+                                                        m->totals, m->idx, m->cap_t);
+        k_mc_normals<<<m->list_grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vsrc, m->fn, m->nrm,
+                                                          m->totals, m->cap_t, m->cap_v);
+        return cudaGetLastError();
+    };
+    e = outputs();
     if (e == cudaSuccess) e = cudaMemcpyAsync(m->h_totals, m->totals, 3 * sizeof(long long), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return mcuda(m, e, "mesher count");
-    const long long nt = m->h_totals[0], nv = m->h_totals[1], nlist = m->h_totals[2];
+    if (e != cudaSuccess) return mcuda(m, e, "mesher passes");
+    const long long nt = m->h_totals[0], nv = m->h_totals[1];
     if (3 * nt > 0xffffffffLL || nv > 0x7fffffffLL)
         return mfail(m, LENIA_ERR_UNSUPPORTED, "mesh of %lld triangles exceeds 32-bit indices", nt);
     if (nt > m->cap_t || nv > m->cap_v) {
@@ -957,17 +1064,8 @@ lenia_status lenia_mesher_run(lenia_mesher *m, const float *const *fields, const
         }
         m->cap_t = ct;
         m->cap_v = cv;
-    }
-    if (nt > 0) {
-        k_mc_emit<<<(unsigned)nlist, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk, m->list, m->tri_base,
-                                                  m->vert_base, m->fn, m->pos, m->vch, m->vsrc);
-        k_mc_index<<<(unsigned)nlist, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vert_base, m->list,
-                                                           m->idx);
-        const long long nb = (nv + kMcThreads - 1) / kMcThreads;
-        const int gn = (int)(nb < 64LL * m->grid ? (nb > 0 ? nb : 1) : 64LL * m->grid);
-        k_mc_normals<<<gn, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vsrc, m->fn, m->nrm, nv);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return mcuda(m, e, "mesher emit");
+        e = outputs();
+        if (e != cudaSuccess) return mcuda(m, e, "mesher passes");
     }
     m->n_t = nt;
     m->n_v = nv;

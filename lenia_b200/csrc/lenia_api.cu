@@ -118,6 +118,11 @@ struct lenia_world {
     float *A = nullptr, *A_next = nullptr, *V = nullptr, *GA = nullptr, *SUM = nullptr;
     float *H = nullptr, *H_RB = nullptr, *U_SUM = nullptr, *U_SUM_RB = nullptr, *BACK = nullptr;
     float *MU = nullptr, *F = nullptr, *ALPHA = nullptr, *U_S = nullptr, *SUM_S = nullptr, *RBB = nullptr;
+    // The grid buffer (A or A_next) whose contents RBB stands for while the
+    // snapshot copy is deferred (null: RBB holds the snapshot itself).  The
+    // copy is made only when RBB is read out, or before that buffer is
+    // written (the transport two steps later, lenia_set_field of A).
+    const float *rbb_src = nullptr;
     float *NA = nullptr, *NU = nullptr, *PREALPHA = nullptr, *TT = nullptr, *U = nullptr;
     float2 *XS = nullptr;   // (C+1) half spectra
     float2 *S = nullptr;    // max(K, C+1) half spectra
@@ -774,11 +779,15 @@ lenia_status stage_flow(lenia_world *w)
     return LENIA_OK;
 }
 
+cudaError_t rbb_materialize(lenia_world *w);
+
 lenia_status stage_transport(lenia_world *w)
 {
     const StepParams p = step_params(w);
     const TransportBuffers b = transport_buffers(w);
     cudaError_t e;
+    // the new grid overwrites A_next: a deferred snapshot of it is copied first
+    if (w->rbb_src == w->A_next && (e = rbb_materialize(w)) != cudaSuccess) return cuda_fail(w, e, "snapshot");
     {
         ProfScope ps(w, KID_TRANSPORT);
         e = launch_transport(p, b, w->stream);
@@ -800,13 +809,25 @@ lenia_status stage_transport(lenia_world *w)
     return LENIA_OK;
 }
 
+// RBB := the grid buffer it stands for, if the copy was deferred.
+cudaError_t rbb_materialize(lenia_world *w)
+{
+    if (!w->rbb_src || !w->RBB) return cudaSuccess;
+    const float *src = w->rbb_src;
+    w->rbb_src = nullptr;
+    return cudaMemcpyAsync(w->RBB, src, sizeof(float) * w->C * w->d.N, cudaMemcpyDeviceToDevice, w->stream);
+}
+
+// The snapshot of the grid the step produced (render.cpp's copy to RBB).
+// The copy itself is deferred: until RBB is read or the grid buffer is
+// written again, RBB's contents are that buffer's, which meshing reads in
+// place.
 lenia_status stage_snapshot(lenia_world *w)
 {
     lenia_status s = ensure_optional(w);
     if (s != LENIA_OK) return s;
     if (!w->RBB) return LENIA_OK;
-    cudaError_t e = cudaMemcpyAsync(w->RBB, w->A, sizeof(float) * w->C * w->d.N, cudaMemcpyDeviceToDevice, w->stream);
-    if (e != cudaSuccess) return cuda_fail(w, e, "snapshot");
+    w->rbb_src = w->A;
     return LENIA_OK;
 }
 
@@ -1048,7 +1069,11 @@ lenia_status lenia_set_field(lenia_world *w, int field, const float *src, size_t
     float *p = field_ptr(w, field, &n);
     if (!p) return fail(w, LENIA_ERR_INVALID_ARG, "field %d is not available (enable debug?)", field);
     if (count != n) return fail(w, LENIA_ERR_INVALID_ARG, "field %d holds %zu floats, got %zu", field, n, count);
-    cudaError_t e = cudaMemcpyAsync(p, src, count * sizeof(float),
+    cudaError_t e = cudaSuccess;
+    if (field == LENIA_FIELD_RBB) w->rbb_src = nullptr;  // replaced whole
+    else if (field == LENIA_FIELD_A && w->rbb_src == w->A) e = rbb_materialize(w);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(p, src, count * sizeof(float),
                                     on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, w->stream);
     if (e == cudaSuccess && !on_device) e = cudaStreamSynchronize(w->stream);
     if (e != cudaSuccess) return cuda_fail(w, e, "set_field");
@@ -1063,8 +1088,10 @@ lenia_status lenia_get_field(lenia_world *w, int field, float *dst, size_t count
     float *p = field_ptr(w, field, &n);
     if (!p) return fail(w, LENIA_ERR_INVALID_ARG, "field %d is not available (enable debug?)", field);
     if (count != n) return fail(w, LENIA_ERR_INVALID_ARG, "field %d holds %zu floats, got %zu", field, n, count);
-    cudaError_t e = cudaMemcpyAsync(dst, p, count * sizeof(float),
-                                    on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, w->stream);
+    cudaError_t e = field == LENIA_FIELD_RBB ? rbb_materialize(w) : cudaSuccess;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dst, p, count * sizeof(float), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                            w->stream);
     if (e == cudaSuccess && !on_device) e = cudaStreamSynchronize(w->stream);
     if (e != cudaSuccess) return cuda_fail(w, e, "get_field");
     return LENIA_OK;
@@ -1339,9 +1366,11 @@ lenia_status lenia_mesh_world(lenia_world *w, int view, lenia_mesher *m, long lo
                     mesher_fields(m));
     if (mesher_field_floats(m) != (long long)w->C * w->d.N)
         return fail(w, LENIA_ERR_INVALID_ARG, "mesher shape does not match the world");
-    // the snapshots, and the arrays their +1 faces copy (transposition.cpp:881-995)
-    const float *fields[3] = {w->RBB, w->U_SUM_RB, w->H_RB};
-    const float *halos[3] = {w->RBB, w->U_SUM, w->H};
+    // the snapshots, and the arrays their +1 faces copy (transposition.cpp:881-995);
+    // a deferred grid snapshot is read where it lies
+    const float *rbb = w->rbb_src ? w->rbb_src : w->RBB;
+    const float *fields[3] = {rbb, w->U_SUM_RB, w->H_RB};
+    const float *halos[3] = {rbb, w->U_SUM, w->H};
     const lenia_status s = lenia_mesher_run(m, fields, halos, w->stream, n_vertices, n_triangles);
     if (s != LENIA_OK) return fail(w, s, "mesh: %s", lenia_mesher_last_error(m));
     return LENIA_OK;

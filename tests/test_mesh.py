@@ -310,6 +310,41 @@ def test_gpu_mesh_of_world_views(view):
 
 
 @pytest.mark.gpu
+def test_gpu_snapshot_copy_deferred():
+    """The grid snapshot (RBB) is the grid at the end of the last step that
+    took one, however it is read: meshed in place, read out, after steps
+    without snapshots, and after the grid itself is overwritten."""
+    from lenia_b200.mesh import Mesher
+    wl = LC.four_channels()
+    w = _world_after(wl, 3)
+    ms = Mesher.for_view("NORMAL", 32, 32, 4, iso_value=wl.desc.iso_value)
+    ms.run_world(w, "NORMAL")                 # reads the grid buffer in place
+    lazy = ms.arrays(cases=True)
+    a3 = w.get("A")
+    assert np.array_equal(w.get("RBB").view(np.uint32), a3.view(np.uint32))
+    ms.run_world(w, "NORMAL")                 # reads the copy
+    copied = ms.arrays(cases=True)
+    for name in ("positions", "normals", "vertex_channel", "indices", "face_normals", "cases"):
+        a, b = getattr(copied, name), getattr(lazy, name)
+        assert a.shape == b.shape and np.array_equal(a.view(np.uint8), b.view(np.uint8)), name
+    # steps without snapshots leave the snapshot of step 3 (its buffer is
+    # overwritten two steps later)
+    w.step(1)
+    w.set_snapshots(False)
+    a4 = w.get("A")
+    w.step(3)
+    w.set_snapshots(True)
+    assert np.array_equal(w.get("RBB").view(np.uint32), a4.view(np.uint32))
+    # a snapshot, then the grid replaced: RBB keeps the stepped grid
+    w.step(1)
+    a5 = w.get("A")
+    w.set_state(np.zeros_like(a5))
+    assert np.array_equal(w.get("RBB").view(np.uint32), a5.view(np.uint32))
+    ms.close()
+    w.close()
+
+
+@pytest.mark.gpu
 def test_gpu_mesh_config1_size():
     """128^3 x 4 channels, the single-world size, after two steps."""
     from lenia_b200.mesh import Mesher
