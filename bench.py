@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--width", type=int, default=128)
     ap.add_argument("--mode", default="rt", choices=["rt", "adv"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--batch-worlds", type=int, default=512,
+    ap.add_argument("--jsonl", default=None, help="also append the result line to this JSONL file")
+    ap.add_argument("--batch-worlds", type=int, default=4096,
                     help="worlds of the batched measurement (config 3 mix; 0 = skip)")
     ap.add_argument("--conv-width", type=int, default=256,
                     help="side of the convolution-mode measurement (config 2 workload; 0 = skip)")
@@ -386,7 +387,7 @@ def run_reference(args):
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
+    emit(line, args)
     return 0
 
 
@@ -412,7 +413,7 @@ def run_reference_build(args, wl, path: str, n: int):
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 2, "kind": "reference", "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
+    emit(line, args)
     return 0
 
 
@@ -731,8 +732,19 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     if line is not None:
-        print(json.dumps(line), flush=True)
+        emit(line, args)
     return 0
+
+
+def emit(line: dict, args) -> None:
+    """Prints the result line; with --jsonl also appends it, time-stamped, to
+    that file (one JSON object per run)."""
+    print(json.dumps(line), flush=True)
+    if args.jsonl:
+        import datetime
+        rec = dict(line, time=datetime.datetime.now(datetime.timezone.utc).isoformat(timespec="seconds"))
+        with open(args.jsonl, "a") as f:
+            f.write(json.dumps(rec) + "\n")
 
 
 def main():

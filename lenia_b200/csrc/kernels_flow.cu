@@ -169,9 +169,18 @@ __device__ __forceinline__ void load_plane(const float *tile, int c, float (&v)[
 
 // The block (bx, by) of a world's flow launch: bx over the x-y tiles, by
 // over the z tiles (OWN_GRID: the launch's own blockIdx, read where used).
+// FULL: every cell of the block's tile is inside the grid (decided per
+// block), so no thread tests its cells' bounds.
 // tm_sum / tm_h: the world's tensor maps (kernel parameters, or a batch's
 // world table in global memory).
-template <bool OWN_GRID>
+// True when tile (bx, by) of a flow launch lies inside the grid.
+__device__ __forceinline__ bool flow_tile_full(const Dims &d, int bx, int by)
+{
+    const int tiles_x = (d.W + kFX - 1) / kFX;
+    return (bx % tiles_x) * kFX + kFX <= d.W && (bx / tiles_x) * kFY + kFY <= d.H && by * kFlowZ + kFlowZ <= d.D;
+}
+
+template <bool OWN_GRID, bool FULL>
 __device__ __forceinline__ void flow_body(const StepParams &p, const FlowBuffers &b, const CUtensorMap *tm_sum,
                                           const CUtensorMap *tm_h, int bx_arg, int by_arg)
 {
@@ -188,7 +197,7 @@ __device__ __forceinline__ void flow_body(const StepParams &p, const FlowBuffers
     const int y0 = (bx / tiles_x) * kFY;
     const int z0 = by * kFlowZ;
     const int x = x0 + tx, y = y0 + ty;
-    const bool col_in = x < d.W && y < d.H;
+    const bool col_in = FULL || (x < d.W && y < d.H);
     const float posx = (float)x + 0.5f, posy = (float)y + 0.5f, posz0 = (float)z0 + 0.5f;
     const int sobel = p.gradient_mode == kGradSobel;
     const float ta = p.theta_a;
@@ -271,7 +280,7 @@ __device__ __forceinline__ void flow_body(const StepParams &p, const FlowBuffers
         for (int lz = 0; lz < kFlowZ; lz++) {
             grad(flow_smem, literal, lz, win, na[lz]);
             const int z = z0 + lz;
-            if (b.NA && col_in && z < d.D) {
+            if (b.NA && col_in && (FULL || z < d.D)) {
                 const int i = x + y * d.W + z * d.W * d.H;
                 b.NA[i] = na[lz][0];
                 b.NA[N + i] = na[lz][1];
@@ -293,7 +302,7 @@ __device__ __forceinline__ void flow_body(const StepParams &p, const FlowBuffers
 #pragma unroll
             for (int lz = 0; lz < kFlowZ; lz++) {
                 const int z = z0 + lz;
-                if (z >= d.D) continue;
+                if (!FULL && z >= d.D) continue;
                 const int i = x + y * d.W + z * d.W * d.H;
                 const int ci = c * N + i;
 #pragma unroll
@@ -321,7 +330,7 @@ __device__ __forceinline__ void flow_body(const StepParams &p, const FlowBuffers
             float g[3];
             grad(tile, literal, lz, win, g);
             const int z = z0 + lz;
-            if (!col_in || z >= d.D) continue;
+            if (!FULL && (!col_in || z >= d.D)) continue;
             const int i = x + y * d.W + z * d.W * d.H;
             const int ci = c * N + i;
             float alpha;
@@ -394,7 +403,10 @@ __global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p
                                                    const __grid_constant__ CUtensorMap tm_sum,
                                                    const __grid_constant__ CUtensorMap tm_h)
 {
-    flow_body<true>(p, b, &tm_sum, &tm_h, 0, 0);
+    if (flow_tile_full(p.d, blockIdx.x, blockIdx.y))
+        flow_body<true, true>(p, b, &tm_sum, &tm_h, 0, 0);
+    else
+        flow_body<true, false>(p, b, &tm_sum, &tm_h, 0, 0);
 }
 
 // Copies a world's parameter block into shared memory (whole 4-byte words).
@@ -438,7 +450,11 @@ __global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow_multi(const 
     }
     const int gx = w->flow_gx;
     __syncthreads();
-    flow_body<false>(sp, sb, &w->tm_sum, &w->tm_h, it.block % gx, it.block / gx);
+    const int bx = it.block % gx, by = it.block / gx;
+    if (flow_tile_full(sp.d, bx, by))
+        flow_body<false, true>(sp, sb, &w->tm_sum, &w->tm_h, bx, by);
+    else
+        flow_body<false, false>(sp, sb, &w->tm_sum, &w->tm_h, bx, by);
 }
 
 namespace {

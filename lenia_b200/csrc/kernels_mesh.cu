@@ -36,6 +36,8 @@
 
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "lenia_internal.h"
 
 namespace {
@@ -887,6 +889,72 @@ long long mesher_field_floats(const lenia_mesher *m) { return m ? (long long)m->
 int mesher_fields(const lenia_mesher *m) { return m ? m->g.F : 0; }
 }  // namespace lenia
 
+namespace {
+
+// The six launches of one mesh and its one host synchronisation.
+lenia_status mesher_run(lenia_mesher *m, cudaStream_t st, long long *n_vertices, long long *n_triangles)
+{
+    McGeom &g = m->g;
+    m->stream = st;
+    m->have_mesh = false;
+    const long long M = (long long)g.slabs * g.nblk * g.C;
+    k_mc_count<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk);
+    const unsigned ntiles = (unsigned)((M + kScanTile - 1) / kScanTile);
+    k_mc_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(m->blk, M, m->tile_tot, m->tile_cnt, m->list_tmp);
+    k_mc_scan_add<<<ntiles, kScanThreads, 0, st>>>(m->blk, M, m->tile_tot, m->tile_cnt, m->list_tmp, m->list,
+                                                    m->totals);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return mcuda(m, e, "mesher count");
+    // The output passes take their counts from the scan's totals on the
+    // device, so they follow it without a host round trip; they write only
+    // what fits the current buffers, and run again into larger ones when
+    // the totals read afterwards do not fit.
+    auto outputs = [&]() -> cudaError_t {
+        k_mc_emit<<<m->list_grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk, m->list, m->totals, m->tri_base,
+                                                       m->vert_base, m->fn, m->pos, m->vch, m->vsrc, m->cap_t,
+                                                       m->cap_v);
+        k_mc_index<<<m->list_grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vert_base, m->list,
+                                                        m->totals, m->idx, m->cap_t);
+        k_mc_normals<<<m->list_grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vsrc, m->fn, m->nrm,
+                                                          m->totals, m->cap_t, m->cap_v);
+        return cudaGetLastError();
+    };
+    e = outputs();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m->h_totals, m->totals, 3 * sizeof(long long), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return mcuda(m, e, "mesher passes");
+    const long long nt = m->h_totals[0], nv = m->h_totals[1];
+    if (3 * nt > 0xffffffffLL || nv > 0x7fffffffLL)
+        return mfail(m, LENIA_ERR_UNSUPPORTED, "mesh of %lld triangles exceeds 32-bit indices", nt);
+    if (nt > m->cap_t || nv > m->cap_v) {
+        const long long ct = nt > m->cap_t ? nt + nt / 4 + 1024 : m->cap_t;
+        const long long cv = nv > m->cap_v ? nv + nv / 4 + 1024 : m->cap_v;
+        free_outputs(m);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&m->fn, sizeof(float) * 3 * ct);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&m->idx, sizeof(unsigned) * 3 * ct);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&m->pos, sizeof(float) * 3 * cv);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&m->nrm, sizeof(float) * 3 * cv);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&m->vch, sizeof(int) * cv);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&m->vsrc, sizeof(unsigned long long) * cv);
+        if (e != cudaSuccess) {
+            free_outputs(m);
+            return mcuda(m, e, "mesher buffers");
+        }
+        m->cap_t = ct;
+        m->cap_v = cv;
+        e = outputs();
+        if (e != cudaSuccess) return mcuda(m, e, "mesher passes");
+    }
+    m->n_t = nt;
+    m->n_v = nv;
+    m->have_mesh = true;
+    if (n_vertices) *n_vertices = nv;
+    if (n_triangles) *n_triangles = nt;
+    return LENIA_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int lenia_mc_triangle_table(int *table)
@@ -1017,62 +1085,10 @@ lenia_status lenia_mesher_run(lenia_mesher *m, const float *const *fields, const
         g.halo[f] = f < g.F ? (halos && halos[f] ? halos[f] : fields[f]) : nullptr;
     }
     cudaStream_t st = (cudaStream_t)stream;
-    m->stream = st;
-    m->have_mesh = false;
-    const long long M = (long long)g.slabs * g.nblk * g.C;
-    k_mc_count<<<m->grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk);
-    const unsigned ntiles = (unsigned)((M + kScanTile - 1) / kScanTile);
-    k_mc_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(m->blk, M, m->tile_tot, m->tile_cnt, m->list_tmp);
-    k_mc_scan_add<<<ntiles, kScanThreads, 0, st>>>(m->blk, M, m->tile_tot, m->tile_cnt, m->list_tmp, m->list,
-                                                    m->totals);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return mcuda(m, e, "mesher count");
-    // The output passes take their counts from the scan's totals on the
-    // device, so they follow it without a host round trip; they write only
-    // what fits the current buffers, and run again into larger ones when
-    // the totals read afterwards do not fit.
-    auto outputs = [&]() -> cudaError_t {
-        k_mc_emit<<<m->list_grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->blk, m->list, m->totals, m->tri_base,
-                                                       m->vert_base, m->fn, m->pos, m->vch, m->vsrc, m->cap_t,
-                                                       m->cap_v);
-        k_mc_index<<<m->list_grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vert_base, m->list,
-                                                        m->totals, m->idx, m->cap_t);
-        k_mc_normals<<<m->list_grid, kMcThreads, 0, st>>>(g, m->tab, m->cases, m->tri_base, m->vsrc, m->fn, m->nrm,
-                                                          m->totals, m->cap_t, m->cap_v);
-        return cudaGetLastError();
-    };
-    e = outputs();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(m->h_totals, m->totals, 3 * sizeof(long long), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return mcuda(m, e, "mesher passes");
-    const long long nt = m->h_totals[0], nv = m->h_totals[1];
-    if (3 * nt > 0xffffffffLL || nv > 0x7fffffffLL)
-        return mfail(m, LENIA_ERR_UNSUPPORTED, "mesh of %lld triangles exceeds 32-bit indices", nt);
-    if (nt > m->cap_t || nv > m->cap_v) {
-        const long long ct = nt > m->cap_t ? nt + nt / 4 + 1024 : m->cap_t;
-        const long long cv = nv > m->cap_v ? nv + nv / 4 + 1024 : m->cap_v;
-        free_outputs(m);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&m->fn, sizeof(float) * 3 * ct);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&m->idx, sizeof(unsigned) * 3 * ct);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&m->pos, sizeof(float) * 3 * cv);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&m->nrm, sizeof(float) * 3 * cv);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&m->vch, sizeof(int) * cv);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&m->vsrc, sizeof(unsigned long long) * cv);
-        if (e != cudaSuccess) {
-            free_outputs(m);
-            return mcuda(m, e, "mesher buffers");
-        }
-        m->cap_t = ct;
-        m->cap_v = cv;
-        e = outputs();
-        if (e != cudaSuccess) return mcuda(m, e, "mesher passes");
-    }
-    m->n_t = nt;
-    m->n_v = nv;
-    m->have_mesh = true;
-    if (n_vertices) *n_vertices = nv;
-    if (n_triangles) *n_triangles = nt;
-    return LENIA_OK;
+    nvtxRangePushA("lenia_mesher_run");
+    const lenia_status s = mesher_run(m, st, n_vertices, n_triangles);
+    nvtxRangePop();
+    return s;
 }
 
 lenia_status lenia_mesher_get(lenia_mesher *m, int which, void *dst, size_t count, int on_device)

@@ -19,6 +19,8 @@
 #include <utility>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "direct_conv.h"
 #include "lenia_internal.h"
 
@@ -166,11 +168,23 @@ cudaEvent_t prof_event(lenia_world *w)
 }
 
 // Brackets the launches issued between prof_begin and prof_end.
+// An NVTX range on the host timeline (header-only NVTX 3: a no-op unless a
+// profiler such as Nsight Systems injects itself).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+
+// One kernel launch of a step: an NVTX range named after the kernel and,
+// with profiling on, CUDA events around it on the world's stream.
 struct ProfScope {
     lenia_world *w;
     int kid;
     cudaEvent_t a = nullptr;
-    ProfScope(lenia_world *w_, int kid_) : w(w_), kid(kid_)
+    NvtxRange range;
+    ProfScope(lenia_world *w_, int kid_) : w(w_), kid(kid_), range(kKernelNames[kid_])
     {
         if (w->profile) {
             a = prof_event(w);
@@ -1113,6 +1127,7 @@ lenia_status lenia_step_stage(lenia_world *w, int stage)
 lenia_status lenia_step(lenia_world *w, int n_steps)
 {
     if (!w || n_steps < 0) return LENIA_ERR_INVALID_ARG;
+    NvtxRange range("lenia_step");
     lenia_status s = ensure_optional(w);
     if (s != LENIA_OK) return s;
     for (int i = 0; i < n_steps; i++) {
@@ -1960,6 +1975,7 @@ lenia_status lenia_batch_get_field(lenia_batch *b, int world, int field, float *
 lenia_status lenia_batch_step(lenia_batch *b, int n_steps)
 {
     if (!b || n_steps < 0) return LENIA_ERR_INVALID_ARG;
+    NvtxRange range("lenia_batch_step");
     for (int i = 0; i < n_steps; i++) {
         const cudaError_t e = cudaGraphLaunch(b->exec[b->parity], b->stream);
         if (e != cudaSuccess) return bfail(b, LENIA_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
