@@ -114,6 +114,11 @@ __device__ __forceinline__ bool tile_unsafe(const float *tile)
     return __syncthreads_or(bad) != 0;
 }
 
+// A / theta_A for a theta_A without an exact reciprocal: out of line, so
+// that the compiler does not evaluate the IEEE division alongside the
+// multiplication that the usual power-of-two theta_A takes.
+__device__ __noinline__ float div_theta(float a, float ta) { return a / ta; }
+
 __host__ __device__ constexpr float sob_w(int dd) { return dd == 0 ? 2.0f : 1.0f; }
 
 // The 27-tap gradient as the reference writes it, acc = acc + v * coef, in
@@ -312,9 +317,11 @@ __device__ __forceinline__ void flow_body(const StepParams &p, const FlowBuffers
                 int src_c = c, src_i = i;
                 bool valid = true;
                 if (!p.alpha_index_fix) {
-                    // ci < 4 N < 4 P, so the block index is 0..3
-                    src_c = (ci >= d.P) + (ci >= 2 * d.P) + (ci >= 3 * d.P);
-                    src_i = ci - src_c * d.P;
+                    // ci < 4 N < 4 P < 2^31 (sides <= 256), so the block
+                    // index is 0..3 and 32-bit arithmetic is exact
+                    const int P = (int)d.P;
+                    src_c = (ci >= P) + (ci >= 2 * P) + (ci >= 3 * P);
+                    src_i = ci - src_c * P;
                     valid = src_c < C && src_i < N;
                 }
                 gal[lz] = valid ? __ldg(b.A + src_c * N + src_i) : 0.0f;
@@ -339,7 +346,7 @@ __device__ __forceinline__ void flow_body(const StepParams &p, const FlowBuffers
                 if (!((gvalid >> lz) & 1u)) {
                     alpha = 0.0f;
                 } else {
-                    float pg = p.inv_theta_a != 0.0f ? gv * p.inv_theta_a : gv / ta;
+                    float pg = p.inv_theta_a != 0.0f ? gv * p.inv_theta_a : div_theta(gv, ta);
                     pg = pg * pg;
                     alpha = smin(smax(pg, 0.0f), 1.0f);
                 }

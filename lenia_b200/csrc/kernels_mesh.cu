@@ -34,6 +34,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <string>
 
 #include <nvtx3/nvToolsExt.h>
@@ -882,6 +883,26 @@ void free_outputs(lenia_mesher *m)
     m->cap_t = m->cap_v = 0;
 }
 
+// Output buffers for ct triangles and cv vertices (the old ones freed).
+cudaError_t alloc_outputs(lenia_mesher *m, long long ct, long long cv)
+{
+    free_outputs(m);
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = cudaMalloc((void **)&m->fn, sizeof(float) * 3 * ct);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&m->idx, sizeof(unsigned) * 3 * ct);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&m->pos, sizeof(float) * 3 * cv);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&m->nrm, sizeof(float) * 3 * cv);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&m->vch, sizeof(int) * cv);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&m->vsrc, sizeof(unsigned long long) * cv);
+    if (e != cudaSuccess) {
+        free_outputs(m);
+        return e;
+    }
+    m->cap_t = ct;
+    m->cap_v = cv;
+    return cudaSuccess;
+}
+
 }  // namespace
 
 namespace lenia {
@@ -929,19 +950,7 @@ lenia_status mesher_run(lenia_mesher *m, cudaStream_t st, long long *n_vertices,
     if (nt > m->cap_t || nv > m->cap_v) {
         const long long ct = nt > m->cap_t ? nt + nt / 4 + 1024 : m->cap_t;
         const long long cv = nv > m->cap_v ? nv + nv / 4 + 1024 : m->cap_v;
-        free_outputs(m);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&m->fn, sizeof(float) * 3 * ct);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&m->idx, sizeof(unsigned) * 3 * ct);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&m->pos, sizeof(float) * 3 * cv);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&m->nrm, sizeof(float) * 3 * cv);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&m->vch, sizeof(int) * cv);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&m->vsrc, sizeof(unsigned long long) * cv);
-        if (e != cudaSuccess) {
-            free_outputs(m);
-            return mcuda(m, e, "mesher buffers");
-        }
-        m->cap_t = ct;
-        m->cap_v = cv;
+        if ((e = alloc_outputs(m, ct, cv)) != cudaSuccess) return mcuda(m, e, "mesher buffers");
         e = outputs();
         if (e != cudaSuccess) return mcuda(m, e, "mesher passes");
     }
@@ -1046,6 +1055,13 @@ lenia_status lenia_mesher_create(const LeniaMeshDesc *desc, lenia_mesher **out)
     alloc(m->totals, 3 * sizeof(long long));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&m->h_totals, 3 * sizeof(long long));
     if (e == cudaSuccess) e = cudaMemcpy(m->tab, &host, sizeof(McTables), cudaMemcpyHostToDevice);
+    // first output buffers: one triangle and one vertex per 32 cube slots
+    // (at most 2^20 each, 60 MB), so that a first mesh rarely runs its
+    // output passes twice; a larger mesh grows them
+    if (e == cudaSuccess) {
+        const long long first = std::min<long long>(std::max<long long>(cubes / 32, 4096), 1LL << 20);
+        e = alloc_outputs(m, first, first);
+    }
     if (e != cudaSuccess) {
         lenia_mesher_destroy(m);
         return e == cudaErrorMemoryAllocation ? LENIA_ERR_OOM : LENIA_ERR_CUDA;

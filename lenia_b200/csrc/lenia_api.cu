@@ -874,6 +874,13 @@ float *field_ptr(lenia_world *w, int field, size_t *count)
     }
 }
 
+// The stream a world created for itself.
+void destroy_streams(lenia_world *w)
+{
+    if (w->own_stream) cudaStreamDestroy(w->own_stream);
+    w->own_stream = nullptr;
+}
+
 // A world; with `shared`, the per-step buffers are the lane's and the
 // kernels are built on `stream` (which the world then uses).
 lenia_status create_world(const LeniaWorldDesc *desc, const LeniaKernelParams *kernels, int n_kernels,
@@ -975,6 +982,7 @@ lenia_status create_world(const LeniaWorldDesc *desc, const LeniaKernelParams *k
         s = e == cudaErrorMemoryAllocation ? LENIA_ERR_OOM : LENIA_ERR_CUDA;
         fprintf(stderr, "lenia_create: %s\n", cudaGetErrorString(e));
         free_world(w);
+        destroy_streams(w);
         delete w;
         return s;
     }
@@ -983,6 +991,7 @@ lenia_status create_world(const LeniaWorldDesc *desc, const LeniaKernelParams *k
     if (s != LENIA_OK) {
         fprintf(stderr, "lenia_create: %s\n", w->err.c_str());
         free_world(w);
+        destroy_streams(w);
         delete w;
         return s;
     }
@@ -1012,7 +1021,7 @@ lenia_status lenia_destroy(lenia_world *w)
     }
     for (cudaEvent_t e : w->prof_free) cudaEventDestroy(e);
     free_world(w);
-    if (w->own_stream) cudaStreamDestroy(w->own_stream);
+    destroy_streams(w);
     delete w;
     return LENIA_OK;
 }
