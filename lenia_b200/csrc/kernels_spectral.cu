@@ -316,13 +316,15 @@ __global__ void k_kernel_values(Dims d, const LeniaKernelParams *__restrict__ kp
 }
 
 // Sum of the cell values in the reference's (r_x, r_y, r_z) loop order, in
-// float (lenia.cpp:215-243), then the normalisation (lenia.cpp:250-257).
+// float (lenia.cpp:215-243); the normalisation (lenia.cpp:250-257) follows.
 // Cells outside the box |r| <= bound hold +0 and leave the sum unchanged.
+// The block stages the box's values 256 at a time into one of two shared
+// buffers while thread 0 adds up the other one in order (one barrier per
+// chunk; four values per shared-memory load); k_kernel_scale then divides.
 __global__ void k_kernel_normalise(Dims d, const LeniaKernelParams *__restrict__ kps, float *grids,
                                    float *ksum, int blur)
 {
-    __shared__ float chunk[256];
-    __shared__ float total;
+    __shared__ __align__(16) float chunk[2][256];
     const int k = blockIdx.x;
     float *g = grids + (long long)k * d.N;
     int bx, by;
@@ -338,8 +340,8 @@ __global__ void k_kernel_normalise(Dims d, const LeniaKernelParams *__restrict__
     const int yl = by < oh ? -by : -oh, yh = by < oh ? by : oh - 1;
     const int nx = x1 - x0 + 1, ny = yh - yl + 1;
     const long long cnt = (long long)nx * ny * nx;
-    float s = 0.0f;
-    for (long long c0 = 0; c0 < cnt; c0 += 256) {
+    // value c of the box in the reference's (r_x, r_y, r_z) loop order
+    auto stage = [&](long long c0, float *dst) {
         const long long c = c0 + threadIdx.x;
         float v = 0.0f;
         if (c < cnt) {
@@ -349,21 +351,40 @@ __global__ void k_kernel_normalise(Dims d, const LeniaKernelParams *__restrict__
             const int gx = rx < 0 ? rx + d.W : rx, gy = ry < 0 ? ry + d.H : ry, gz = rz < 0 ? rz + d.D : rz;
             v = g[gx + (long long)gy * d.W + (long long)gz * d.W * d.H];
         }
-        chunk[threadIdx.x] = v;
-        __syncthreads();
+        dst[threadIdx.x] = v;
+    };
+    float s = 0.0f;
+    if (cnt > 0) stage(0, chunk[0]);
+    __syncthreads();
+    int it = 0;
+    for (long long c0 = 0; c0 < cnt; c0 += 256, it++) {
+        if (c0 + 256 < cnt) stage(c0 + 256, chunk[(it + 1) & 1]);
         if (threadIdx.x == 0) {
+            const float4 *q = reinterpret_cast<const float4 *>(chunk[it & 1]);
             const int lim = cnt - c0 < 256 ? (int)(cnt - c0) : 256;
-            for (int j = 0; j < lim; j++) s = s + chunk[j];
+            int j = 0;
+            for (; j + 4 <= lim; j += 4) {
+                const float4 v = q[j / 4];
+                s = s + v.x;
+                s = s + v.y;
+                s = s + v.z;
+                s = s + v.w;
+            }
+            for (; j < lim; j++) s = s + chunk[it & 1][j];
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        total = s;
-        ksum[k] = s;
-    }
-    __syncthreads();
-    const float t = total;
-    for (long long i = threadIdx.x; i < d.N; i += blockDim.x) g[i] = g[i] / t;
+    if (threadIdx.x == 0) ksum[k] = s;
+}
+
+// The normalisation itself (lenia.cpp:250-257): every cell of kernel grid
+// blockIdx.y divided by its sum, over a grid of blocks.
+__global__ void k_kernel_scale(Dims d, float *grids, const float *__restrict__ ksum)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.N) return;
+    float *g = grids + (long long)blockIdx.y * d.N;
+    g[i] = g[i] / ksum[blockIdx.y];
 }
 
 // precompute_blur_kernel (reintegration.cpp:37-73): 5^3 exp(-d^2/s^3), s = 1.5.
@@ -542,6 +563,7 @@ cudaError_t launch_kernel_grids(const Dims &d, const LeniaKernelParams *kp_dev, 
     dim3 grid((unsigned)((d.N + 255) / 256), K);
     k_kernel_values<<<grid, 256, 0, st>>>(d, kp_dev, grids);
     k_kernel_normalise<<<K, 256, 0, st>>>(d, kp_dev, grids, ksum, 0);
+    k_kernel_scale<<<dim3((unsigned)((d.N + 255) / 256), K), 256, 0, st>>>(d, grids, ksum);
     return cudaGetLastError();
 }
 
@@ -549,6 +571,7 @@ cudaError_t launch_blur_grid(const Dims &d, float *grid, float *ksum, cudaStream
 {
     k_blur_values<<<(unsigned)((d.N + 255) / 256), 256, 0, st>>>(d, grid);
     k_kernel_normalise<<<1, 256, 0, st>>>(d, nullptr, grid, ksum, 1);
+    k_kernel_scale<<<dim3((unsigned)((d.N + 255) / 256), 1), 256, 0, st>>>(d, grid, ksum);
     return cudaGetLastError();
 }
 
