@@ -285,7 +285,8 @@ lenia_status lenia_load(const char *path, lenia_world **out, unsigned long long 
  * batched launches: per stage one launch per grid size (the transforms) or
  * one launch for all of them (growth from u_k, flow, transport), whose
  * blocks each take one block of one world from a device work list, in waves
- * whose per-step buffers share one scratch pool of at most 12 GB.  One step
+ * whose per-step buffers share one scratch pool (at most 48 GB and a third of
+ * the device memory free when the step is captured).  One step
  * of every world is captured once into a CUDA graph and replayed, so a batch
  * step is one graph launch.  Every world computes exactly what a world of
  * lenia_create computes (bit-identical fields). */

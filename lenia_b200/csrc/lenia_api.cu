@@ -1560,7 +1560,22 @@ lenia_status step_once(lenia_world *w)
 // from u_k, flow, transport), each block working on one block of one world
 // through a device work list.
 
-constexpr size_t kWaveScratchBytes = 12ull << 30;  // per-step buffers of one wave
+// Per-step buffers of one wave: at most 48 GB, and at most a third of the
+// device memory that is free or already held by the batch's pool when the
+// plan is built (the pool is allocated once and reused by every wave).
+constexpr size_t kWaveScratchMax = 48ull << 30;
+
+size_t wave_scratch_budget(size_t held)
+{
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return held > (4ull << 30) ? held : (4ull << 30);
+    }
+    const size_t third = (free_b + held) / 3;
+    const size_t budget = third < kWaveScratchMax ? third : kWaveScratchMax;
+    return budget > held ? budget : held;
+}
 
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
@@ -1610,9 +1625,10 @@ lenia_status build_plan(lenia_batch *b, int which)
         if (group_eligible(b->worlds[i])) ids.push_back(i);
     std::stable_sort(ids.begin(), ids.end(), [&](int a, int c) { return b->worlds[a]->d.N > b->worlds[c]->d.N; });
     size_t used = 0, need = 0;
+    const size_t budget = wave_scratch_budget(b->pool_bytes);
     for (int i : ids) {
         const size_t sb = group_scratch_bytes(b->worlds[i]);
-        if (plan.waves.empty() || (used + sb > kWaveScratchBytes && !plan.waves.back().worlds.empty())) {
+        if (plan.waves.empty() || (used + sb > budget && !plan.waves.back().worlds.empty())) {
             plan.waves.emplace_back();
             used = 0;
         }
