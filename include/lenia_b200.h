@@ -194,7 +194,9 @@ lenia_status lenia_set_debug(lenia_world *w, int on);
  * usable.  polls < 0 restores the default (2^24 polls); 0 makes every such
  * wait give up at once (for tests of the timeout path). */
 lenia_status lenia_set_wait_limit(lenia_world *w, long long polls);
-/* 1: keep the mesh snapshots H_RB / U_SUM_RB / RBB every step. */
+/* 1: keep the mesh snapshots H_RB / U_SUM_RB / RBB every step.  RBB (the
+ * grid after the step) is copied only when it is read out or before the
+ * grid buffer it equals is overwritten; meshing reads that buffer in place. */
 lenia_status lenia_set_snapshots(lenia_world *w, int on);
 
 /* 1: bracket every kernel launch with CUDA events on the world's stream and

@@ -23,6 +23,7 @@ namespace {
 #define LENIA_GROWTH_ROWS 16
 #endif
 constexpr int kFastRowThreads = 256;
+constexpr int kMaxGridY = 65535;  // the largest grid.y of a launch
 constexpr int kFastPlaneThreads = LENIA_PLANE_THREADS;    // block of the plane transform
 constexpr int kGrowthThreads = LENIA_GROWTH_THREADS;      // block of the growth pass
 
@@ -841,8 +842,13 @@ cudaError_t fwd_rows_list_w(const float2 *tw, RowPairList jobs, cudaStream_t st)
     const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2);
     cudaError_t e = smem_attr((const void *)k_fwd_rows_s<W, RowPairList>, smem);
     if (e != cudaSuccess || jobs.n == 0) return e;
-    k_fwd_rows_s<W, RowPairList><<<dim3(W * (W / S::TY), jobs.n), kFastRowThreads, smem, st>>>(jobs, tw);
-    return cudaGetLastError();
+    // the jobs run as grid.y, at most kMaxGridY per launch
+    for (int j0 = 0; j0 < jobs.n && e == cudaSuccess; j0 += kMaxGridY) {
+        const RowPairList part{jobs.j + j0, std::min(jobs.n - j0, kMaxGridY)};
+        k_fwd_rows_s<W, RowPairList><<<dim3(W * (W / S::TY), part.n), kFastRowThreads, smem, st>>>(part, tw);
+        e = cudaGetLastError();
+    }
+    return e;
 }
 
 template <int W>
@@ -852,8 +858,12 @@ cudaError_t planes_list_w(const float2 *twy, const float2 *twz, PlaneJobList job
     const size_t smem = (size_t)(2 * W + PadMat<W>::size(W)) * sizeof(float2);
     cudaError_t e = smem_attr((const void *)k_planes_s<W, PlaneJobList>, smem);
     if (e != cudaSuccess || jobs.n == 0) return e;
-    k_planes_s<W, PlaneJobList><<<dim3(W / 2 + 1, jobs.n), kFastPlaneThreads, smem, st>>>(jobs, twy, twz, sign);
-    return cudaGetLastError();
+    for (int j0 = 0; j0 < jobs.n && e == cudaSuccess; j0 += kMaxGridY) {
+        const PlaneJobList part{jobs.j + j0, std::min(jobs.n - j0, kMaxGridY)};
+        k_planes_s<W, PlaneJobList><<<dim3(W / 2 + 1, part.n), kFastPlaneThreads, smem, st>>>(part, twy, twz, sign);
+        e = cudaGetLastError();
+    }
+    return e;
 }
 
 template <int W>
@@ -863,8 +873,12 @@ cudaError_t inv_rows_list_w(const float2 *tw, InvPairList jobs, cudaStream_t st)
     const size_t smem = (size_t)(W + S::PM::size(S::TY)) * sizeof(float2);
     cudaError_t e = smem_attr((const void *)k_blur_rows_s<W, InvPairList>, smem);
     if (e != cudaSuccess || jobs.n == 0) return e;
-    k_blur_rows_s<W, InvPairList><<<dim3(W * (W / S::TY), jobs.n), kFastRowThreads, smem, st>>>(jobs, tw);
-    return cudaGetLastError();
+    for (int j0 = 0; j0 < jobs.n && e == cudaSuccess; j0 += kMaxGridY) {
+        const InvPairList part{jobs.j + j0, std::min(jobs.n - j0, kMaxGridY)};
+        k_blur_rows_s<W, InvPairList><<<dim3(W * (W / S::TY), part.n), kFastRowThreads, smem, st>>>(part, tw);
+        e = cudaGetLastError();
+    }
+    return e;
 }
 
 }  // namespace

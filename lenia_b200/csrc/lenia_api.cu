@@ -1760,7 +1760,8 @@ lenia_status build_plan(lenia_batch *b, int which)
             g.n_planes_inv = (int)jobs[si].pi.size();
             g.inv = plan_copy(plan, jobs[si].inv, e);
             g.n_inv = (int)jobs[si].inv.size();
-            plan.launches += 4;
+            // each job list runs in launches of at most 65535 jobs (grid.y)
+            for (const int n : {g.n_fwd, g.n_planes_fwd, g.n_planes_inv, g.n_inv}) plan.launches += (n + 65534) / 65535;
         }
         if (e != cudaSuccess) break;
     }

@@ -110,6 +110,32 @@ def test_batch_matches_worlds_stepped_alone():
 
 
 @pytest.mark.gpu
+def test_batched_job_lists_beyond_one_launch():
+    """7,300 worlds of 24^3 with 9 kernels give 65,700 inverse-plane jobs of
+    one grid size, more than one launch's grid.y holds (65,535): the job list
+    runs as two launches, and worlds on both sides of the split step bit for
+    bit as stepped alone."""
+    from lenia_b200.batch import Batch
+    from lenia_b200.world import World
+    wls = P.config3(7300, seed=31, sizes=(24,))
+    b = Batch([wl.desc for wl in wls], [wl.kernels for wl in wls], lanes=4)
+    for i, wl in enumerate(wls):
+        b.set_state(i, wl.A0)
+    assert b.grouped_worlds() == len(wls)
+    b.step(1)
+    b.sync()
+    for i in (0, 7280, 7283, 7299):
+        w = World(wls[i].desc, wls[i].kernels)
+        w.set_state(wls[i].A0.ravel())
+        w.step(1)
+        for name in ("A", "V", "GA", "SUM"):
+            got, want = b.get(i, name), w.get(name)
+            assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (i, name)
+        w.close()
+    b.close()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("batched", [True, False])
 def test_config3_mix_matches_worlds_stepped_alone(batched):
     """Every config-3 size (24 .. 96), RT and advection, plus two worlds the
