@@ -596,7 +596,10 @@ __device__ __forceinline__ void growth_from_u_body(const Dims &d, const GrowthJo
     if (bad && err_flag) atomicOr(err_flag, 1);
 }
 
-__global__ void __launch_bounds__(256, 5)
+#ifndef LENIA_GROWTH_U_MINB
+#define LENIA_GROWTH_U_MINB 5
+#endif
+__global__ void __launch_bounds__(256, LENIA_GROWTH_U_MINB)
     k_growth_from_u(const __grid_constant__ Dims d, const __grid_constant__ GrowthJobs jobs,
                     const __grid_constant__ ChannelOrder ord, const float *__restrict__ lut_rows,
                     const float *__restrict__ U, const float *__restrict__ A, float *__restrict__ Hout,
