@@ -14,7 +14,7 @@
 // is compiled with -fmad=false), so outputs match the CPU restatement bit for
 // bit given the same inputs.
 //
-// A block owns a 32 x 8 x kFlowZ tile of cells; per field (SUM, then each H
+// A block owns a 32 x 8 x FZ tile of cells; per field (SUM, then each H
 // channel) one thread copies the field's tile with its halo into shared
 // memory with a TMA tensor load (zero outside the grid, which is the zero
 // border and the never-written halo edges), double buffered so that field
@@ -37,14 +37,26 @@ namespace lenia {
 #ifndef LENIA_FLOW_MINB
 #define LENIA_FLOW_MINB 4
 #endif
+// The batched form keeps four cells per thread: with the torus faces its
+// many small worlds patch, deeper tiles patch fewer cells per output
+// (23.7 vs 23.9 ms per step for 512 config-3 worlds).
+#ifndef LENIA_FLOW_MULTI_Z
+#define LENIA_FLOW_MULTI_Z 4
+#endif
 constexpr int kFX = 32, kFY = 8;          // output tile in x, y (one thread per column)
-constexpr int kFlowZ = LENIA_FLOW_Z;      // output cells per thread along z
+constexpr int kFlowZ = LENIA_FLOW_Z;      // output cells per thread along z (one world's launch)
+constexpr int kFlowMultiZ = LENIA_FLOW_MULTI_Z;  // the same in the batched launch
 constexpr int kTX = 40, kTY = kFY + 2;    // staged tile: x from x0 - 4 (TMA x must be 16-byte aligned), y halo
-constexpr int kTZ = kFlowZ + 2;
-constexpr int kTile = kTX * kTY * kTZ;    // floats per staged field
-// the second tile buffer starts kTile floats in: TMA tile destinations must
-// be 128-byte aligned
-static_assert((kTile * sizeof(float)) % 128 == 0, "a tile buffer must keep the next one 128-byte aligned");
+
+// Staged tile of a launch whose threads own FZ cells along z.
+template <int FZ>
+struct FlowShape {
+    static constexpr int TZ = FZ + 2;
+    static constexpr int TILE = kTX * kTY * TZ;  // floats per staged field
+    // the second tile buffer starts TILE floats in: TMA tile destinations
+    // must be 128-byte aligned
+    static_assert((TILE * sizeof(float)) % 128 == 0, "a tile buffer must keep the next one 128-byte aligned");
+};
 
 __device__ __forceinline__ float smax(float a, float b) { return a > b ? a : b; }
 __device__ __forceinline__ float smin(float a, float b) { return a < b ? a : b; }
@@ -71,15 +83,16 @@ __device__ __forceinline__ bool gb_source(const Dims &d, int border, int &x, int
 
 // Torus/wall halo faces of a staged tile (the TMA copy left zeros there).
 // Only the cells the gradients read are patched: x0-1..x0+32, y0-1..y0+8,
-// z0-1..z0+kFlowZ, with exactly one coordinate one step outside the grid.
+// z0-1..z0+FZ, with exactly one coordinate one step outside the grid.
 // Each grid face the staged box reaches is walked over its in-grid cells
 // (edges and corners keep the copy's zeros), so a block patches at most a
 // few hundred cells per field instead of testing its whole box.
+template <int FZ>
 __device__ void patch_faces(float *tile, const float *f, const Dims &d, int border, int x0, int y0, int z0)
 {
     const int tid = threadIdx.x + threadIdx.y * kFX;
     const int lo[3] = {x0 - 1, y0 - 1, z0 - 1};
-    const int hi[3] = {x0 + kFX, y0 + kFY, z0 + kFlowZ};  // inclusive
+    const int hi[3] = {x0 + kFX, y0 + kFY, z0 + FZ};  // inclusive
     const int ext[3] = {d.W, d.H, d.D};
 #pragma unroll
     for (int a = 0; a < 3; a++)
@@ -107,8 +120,10 @@ __device__ void patch_faces(float *tile, const float *f, const Dims &d, int bord
 // True when any staged value is infinite, NaN or so large that a Sobel
 // product could overflow (block-wide); such blocks take the literal 27-tap
 // multiply-then-add path.
+template <int FZ>
 __device__ __forceinline__ bool tile_unsafe(const float *tile)
 {
+    constexpr int kTile = FlowShape<FZ>::TILE;
     static_assert(kTile % 4 == 0 && (kTile * 4) % 16 == 0, "tiles are read as float4");
     const int tid = threadIdx.x + threadIdx.y * kFX;
     const float4 *t4 = reinterpret_cast<const float4 *>(tile);
@@ -185,17 +200,19 @@ __device__ __forceinline__ void load_plane(const float *tile, int c, float (&v)[
 // tm_sum / tm_h: the world's tensor maps (kernel parameters, or a batch's
 // world table in global memory).
 // True when tile (bx, by) of a flow launch lies inside the grid.
+template <int FZ>
 __device__ __forceinline__ bool flow_tile_full(const Dims &d, int bx, int by)
 {
     const int tiles_x = (d.W + kFX - 1) / kFX;
-    return (bx % tiles_x) * kFX + kFX <= d.W && (bx / tiles_x) * kFY + kFY <= d.H && by * kFlowZ + kFlowZ <= d.D;
+    return (bx % tiles_x) * kFX + kFX <= d.W && (bx / tiles_x) * kFY + kFY <= d.H && by * FZ + FZ <= d.D;
 }
 
-template <bool OWN_GRID, bool FULL>
+template <bool OWN_GRID, bool FULL, int FZ>
 __device__ __forceinline__ void flow_body(const StepParams &p, const FlowBuffers &b, const CUtensorMap *tm_sum,
                                           const CUtensorMap *tm_h, int bx_arg, int by_arg)
 {
     const int bx = OWN_GRID ? (int)blockIdx.x : bx_arg, by = OWN_GRID ? (int)blockIdx.y : by_arg;
+    constexpr int kTile = FlowShape<FZ>::TILE;
     extern __shared__ __align__(128) float flow_smem[];
     __shared__ __align__(8) uint64_t bars[2];
     const Dims &d = p.d;
@@ -206,14 +223,14 @@ __device__ __forceinline__ void flow_body(const StepParams &p, const FlowBuffers
     const int tiles_x = (d.W + kFX - 1) / kFX;
     const int x0 = (bx % tiles_x) * kFX;
     const int y0 = (bx / tiles_x) * kFY;
-    const int z0 = by * kFlowZ;
+    const int z0 = by * FZ;
     const int x = x0 + tx, y = y0 + ty;
     const bool col_in = FULL || (x < d.W && y < d.H);
     const float posx = (float)x + 0.5f, posy = (float)y + 0.5f, posz0 = (float)z0 + 0.5f;
     const int sobel = p.gradient_mode == kGradSobel;
     const float ta = p.theta_a;
     const bool patch = p.sobel_border != kBorderNone &&
-                       (x0 == 0 || x0 + kFX >= d.W || y0 == 0 || y0 + kFY >= d.H || z0 == 0 || z0 + kFlowZ >= d.D);
+                       (x0 == 0 || x0 + kFX >= d.W || y0 == 0 || y0 + kFY >= d.H || z0 == 0 || z0 + FZ >= d.D);
 
     if (leader) {
         mbar_init(&bars[0], 1);
@@ -246,10 +263,10 @@ __device__ __forceinline__ void flow_body(const StepParams &p, const FlowBuffers
             return -1;
         }
         if (patch) {
-            patch_faces(tile, f == 0 ? b.SUM : b.H + (f - 1) * N, d, p.sobel_border, x0, y0, z0);
+            patch_faces<FZ>(tile, f == 0 ? b.SUM : b.H + (f - 1) * N, d, p.sobel_border, x0, y0, z0);
             __syncthreads();
         }
-        return (sobel && tile_unsafe(tile)) ? 1 : 0;
+        return (sobel && tile_unsafe<FZ>(tile)) ? 1 : 0;
     };
     // the column: tile index of (x, y, z0 + lz) is col + (lz + 1) * plane
     const int col = (tx + 4) + (ty + 1) * kTX;
@@ -279,7 +296,7 @@ __device__ __forceinline__ void flow_body(const StepParams &p, const FlowBuffers
     };
 
     // field 0: the gradient of SUM (NA), kept in registers for every channel
-    float na[kFlowZ][3];
+    float na[FZ][3];
     issue(0);
     issue(1);
     {
@@ -288,7 +305,7 @@ __device__ __forceinline__ void flow_body(const StepParams &p, const FlowBuffers
         const bool literal = landed != 0;
         float win[3][9];
 #pragma unroll
-        for (int lz = 0; lz < kFlowZ; lz++) {
+        for (int lz = 0; lz < FZ; lz++) {
             grad(flow_smem, literal, lz, win, na[lz]);
             const int z = z0 + lz;
             if (b.NA && col_in && (FULL || z < d.D)) {
@@ -306,12 +323,12 @@ __device__ __forceinline__ void flow_body(const StepParams &p, const FlowBuffers
         float *tile = flow_smem + (f & 1) * kTile;
         if (f < C) issue(f + 1);
         // per-cell inputs of this channel, loaded while the tile lands
-        float v3[3][kFlowZ], gal[kFlowZ];
+        float v3[3][FZ], gal[FZ];
         unsigned gvalid = 0;  // bit lz: the alpha source of cell lz was written
         const int c = f - 1;
         if (col_in) {
 #pragma unroll
-            for (int lz = 0; lz < kFlowZ; lz++) {
+            for (int lz = 0; lz < FZ; lz++) {
                 const int z = z0 + lz;
                 if (!FULL && z >= d.D) continue;
                 const int i = x + y * d.W + z * d.W * d.H;
@@ -339,7 +356,7 @@ __device__ __forceinline__ void flow_body(const StepParams &p, const FlowBuffers
         const bool literal = landed != 0;
         float win[3][9];
 #pragma unroll
-        for (int lz = 0; lz < kFlowZ; lz++) {
+        for (int lz = 0; lz < FZ; lz++) {
             float g[3];
             grad(tile, literal, lz, win, g);
             const int z = z0 + lz;
@@ -416,10 +433,10 @@ __global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow(StepParams p
                                                    const __grid_constant__ CUtensorMap tm_sum,
                                                    const __grid_constant__ CUtensorMap tm_h)
 {
-    if (flow_tile_full(p.d, blockIdx.x, blockIdx.y))
-        flow_body<true, true>(p, b, &tm_sum, &tm_h, 0, 0);
+    if (flow_tile_full<kFlowZ>(p.d, blockIdx.x, blockIdx.y))
+        flow_body<true, true, kFlowZ>(p, b, &tm_sum, &tm_h, 0, 0);
     else
-        flow_body<true, false>(p, b, &tm_sum, &tm_h, 0, 0);
+        flow_body<true, false, kFlowZ>(p, b, &tm_sum, &tm_h, 0, 0);
 }
 
 // Copies a world's parameter block into shared memory (whole 4-byte words).
@@ -443,7 +460,11 @@ __device__ __forceinline__ void tensormap_acquire(const CUtensorMap *m)
 // The flow of a batch of worlds: block b is block items[b].block of world
 // items[b].world's own launch (x-y tile fastest); the world's parameters
 // are read into shared memory first.
-__global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow_multi(const BatchWorldDev *__restrict__ ws,
+#ifndef LENIA_FLOW_MULTI_MINB
+#define LENIA_FLOW_MULTI_MINB 3
+#endif
+// the batched form: four cells per thread, three blocks per SM
+__global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MULTI_MINB) k_flow_multi(const BatchWorldDev *__restrict__ ws,
                                                                          const WorkItem *__restrict__ items)
 {
     __shared__ StepParams sp;
@@ -464,10 +485,10 @@ __global__ void __launch_bounds__(kFX *kFY, LENIA_FLOW_MINB) k_flow_multi(const 
     const int gx = w->flow_gx;
     __syncthreads();
     const int bx = it.block % gx, by = it.block / gx;
-    if (flow_tile_full(sp.d, bx, by))
-        flow_body<false, true>(sp, sb, &w->tm_sum, &w->tm_h, bx, by);
+    if (flow_tile_full<kFlowMultiZ>(sp.d, bx, by))
+        flow_body<false, true, kFlowMultiZ>(sp, sb, &w->tm_sum, &w->tm_h, bx, by);
     else
-        flow_body<false, false>(sp, sb, &w->tm_sum, &w->tm_h, bx, by);
+        flow_body<false, false, kFlowMultiZ>(sp, sb, &w->tm_sum, &w->tm_h, bx, by);
 }
 
 namespace {
@@ -518,47 +539,54 @@ cudaError_t encode_tensor_map(CUtensorMap *map, const float *base, int rank, con
     return encode_tensor_map_typed(map, base, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (int)sizeof(float), rank, dims, box);
 }
 
+// Blocks of a world in the batched flow launch (gx: tiles per z layer).
 int flow_blocks(const Dims &d, int *gx)
 {
     const int tiles_x = (d.W + kFX - 1) / kFX, tiles_y = (d.H + kFY - 1) / kFY;
     if (gx) *gx = tiles_x * tiles_y;
-    return tiles_x * tiles_y * ((d.D + kFlowZ - 1) / kFlowZ);
+    return tiles_x * tiles_y * ((d.D + kFlowMultiZ - 1) / kFlowMultiZ);
 }
 
 cudaError_t launch_flow_multi(const BatchWorldDev *ws, const WorkItem *items, int n_items, cudaStream_t st)
 {
     if (n_items == 0) return cudaSuccess;
-    const size_t smem = 2 * kTile * sizeof(float);
+    const size_t smem = 2 * FlowShape<kFlowMultiZ>::TILE * sizeof(float);
     cudaError_t e = cudaFuncSetAttribute(k_flow_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k_flow_multi<<<(unsigned)n_items, dim3(kFX, kFY), smem, st>>>(ws, items);
     return cudaGetLastError();
 }
 
-// The flow launch's tensor maps: SUM (x, y, z) and H (x, y, z, channel),
-// tiles of 40 x 10 x (kFlowZ + 2).
-cudaError_t flow_tensor_maps(const StepParams &p, const FlowBuffers &b, CUtensorMap *tm_sum, CUtensorMap *tm_h)
+// A flow launch's tensor maps: SUM (x, y, z) and H (x, y, z, channel), tiles
+// of 40 x 10 x (fz + 2) for threads owning fz cells along z.
+cudaError_t flow_maps(const StepParams &p, const FlowBuffers &b, CUtensorMap *tm_sum, CUtensorMap *tm_h, int fz)
 {
     const Dims &d = p.d;
     const unsigned long long dsum[3] = {(unsigned long long)d.W, (unsigned long long)d.H, (unsigned long long)d.D};
     const unsigned long long dh[4] = {(unsigned long long)d.W, (unsigned long long)d.H, (unsigned long long)d.D,
                                       (unsigned long long)p.C};
-    const unsigned box[4] = {kTX, kTY, kTZ, 1};
+    const unsigned box[4] = {(unsigned)kTX, (unsigned)kTY, (unsigned)(fz + 2), 1u};
     cudaError_t e = encode_tensor_map(tm_sum, b.SUM, 3, dsum, box);
     if (e == cudaSuccess) e = encode_tensor_map(tm_h, b.H, 4, dh, box);
     return e;
+}
+
+// The batched flow launch's tensor maps of a world.
+cudaError_t flow_tensor_maps(const StepParams &p, const FlowBuffers &b, CUtensorMap *tm_sum, CUtensorMap *tm_h)
+{
+    return flow_maps(p, b, tm_sum, tm_h, kFlowMultiZ);
 }
 
 cudaError_t launch_flow(const StepParams &p, const FlowBuffers &b, cudaStream_t st)
 {
     const Dims &d = p.d;
     CUtensorMap tm_sum, tm_h;
-    cudaError_t e = flow_tensor_maps(p, b, &tm_sum, &tm_h);
+    cudaError_t e = flow_maps(p, b, &tm_sum, &tm_h, kFlowZ);
     if (e != cudaSuccess) return e;
     const int tiles_x = (d.W + kFX - 1) / kFX, tiles_y = (d.H + kFY - 1) / kFY;
     dim3 grid(tiles_x * tiles_y, (d.D + kFlowZ - 1) / kFlowZ);
     dim3 block(kFX, kFY);
-    const size_t smem = 2 * kTile * sizeof(float);
+    const size_t smem = 2 * FlowShape<kFlowZ>::TILE * sizeof(float);
     return launch_pdl(k_flow, grid, block, smem, st, p, b, tm_sum, tm_h);
 }
 
