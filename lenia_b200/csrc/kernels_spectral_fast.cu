@@ -26,6 +26,13 @@ constexpr int kFastRowThreads = 256;
 constexpr int kMaxGridY = 65535;  // the largest grid.y of a launch
 constexpr int kFastPlaneThreads = LENIA_PLANE_THREADS;    // block of the plane transform
 constexpr int kGrowthThreads = LENIA_GROWTH_THREADS;      // block of the growth pass
+#ifndef LENIA_PLANE_PAIRED
+#define LENIA_PLANE_PAIRED 1
+#endif
+// The plane passes (bound by instruction issue) take the paired butterflies;
+// the row passes keep the scalar ones, whose fewer registers keep more blocks
+// resident to cover their global-memory latency.
+constexpr bool kPlanePaired = LENIA_PLANE_PAIRED;
 
 // Rows per tile of the growth pass: at most 2048 cells, so that a thread's
 // cells (prefetched spectra and growth sums in registers) stay at 8.
@@ -159,7 +166,7 @@ __device__ __forceinline__ void plane_first_stage(float2 *buf, const float2 *__r
                     v[r] = t;
                 }
             }
-            dft_small<R>(v, sign, tw, H);
+            dft_small<R, kPlanePaired>(v, sign, tw, H);
 #pragma unroll
             for (int r = 0; r < R; r++) buf[PM::at(z, j * R + r)] = v[r];
         }
@@ -198,7 +205,7 @@ __device__ __forceinline__ void plane_last_stage(const float2 *buf, float2 *__re
 #pragma unroll
                 for (int r = 1; r < R; r++) v[i][r] = cmul(v[i][r], tw[r * jm * TSTEP]);
             }
-            dft_small<R>(v[i], sign, tw, D);
+            dft_small<R, kPlanePaired>(v[i], sign, tw, D);
             const int base = (j / NS) * NS * R + jm;
 #pragma unroll
             for (int r = 0; r < R; r++) dst[(base + r * NS) * H + l] = v[i][r];
@@ -248,8 +255,8 @@ __global__ void __launch_bounds__(kFastPlaneThreads) k_planes_s(J jobs, const fl
         }
     }
     __syncthreads();
-    static_fft<H, D, false, H, kFastPlaneThreads>(buf, twy, sign);
-    static_fft<D, H, true, H, kFastPlaneThreads>(buf, twz, sign);
+    static_fft<H, D, false, H, kFastPlaneThreads, kPlanePaired>(buf, twy, sign);
+    static_fft<D, H, true, H, kFastPlaneThreads, kPlanePaired>(buf, twz, sign);
     for (int e = threadIdx.x; e < D * H / 2; e += kFastPlaneThreads) {
         const int z = (2 * e) / H, y = (2 * e) % H;
         const float2 a = buf[PM::at(z, y)], b = buf[PM::at(z, y + 1)];
@@ -303,8 +310,9 @@ __global__ void __launch_bounds__(kFastPlaneThreads) k_planes_stream_s(PlaneJobs
         asm volatile("mov.u32 %0, %%tid.x;" : "=r"(tid));
         plane_first_stage<W>(buf, src, kp, twy, sign, tid);
         if (tid == 0 && u + stride < units) plane_unit_prefetch<W>(jobs, u + stride);
-        static_stages<H, 1, D, false, H, kFastPlaneThreads, false>(buf, twy, sign, tid);
-        static_stages<D, 0, H, true, H, kFastPlaneThreads, false, plan_count(D) - 1>(buf, twz, sign, tid);
+        static_stages<H, 1, D, false, H, kFastPlaneThreads, false, plan_count(H), kPlanePaired>(buf, twy, sign, tid);
+        static_stages<D, 0, H, true, H, kFastPlaneThreads, false, plan_count(D) - 1, kPlanePaired>(buf, twz, sign,
+                                                                                                   tid);
         plane_last_stage<W>(buf, dst, twz, sign, tid);
         __syncthreads();  // the next plane's first stage overwrites buf
     }
@@ -349,7 +357,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_plane_lines_y_s(PlaneJobs job
         buf[PM::at(t, y)] = v;
     }
     __syncthreads();
-    static_fft<H, TZ, false, H, kSplitThreads>(buf, twy, sign);
+    static_fft<H, TZ, false, H, kSplitThreads, kPlanePaired>(buf, twy, sign);
     for (int e = threadIdx.x; e < TZ * H; e += kSplitThreads) dst[e] = buf[PM::at(e / H, e % H)];
 }
 
@@ -372,7 +380,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_plane_lines_z_s(PlaneJobs job
         buf[PM::at(z, t)] = dst[(long long)z * H + t];
     }
     __syncthreads();
-    static_fft<D, TY, true, TY, kSplitThreads>(buf, twz, sign);
+    static_fft<D, TY, true, TY, kSplitThreads, kPlanePaired>(buf, twz, sign);
     for (int e = threadIdx.x; e < D * TY; e += kSplitThreads) {
         const int z = e / TY, t = e % TY;
         dst[(long long)z * H + t] = buf[PM::at(z, t)];

@@ -35,51 +35,86 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 w)
 {
     return make_float2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
 }
+
+// Paired forms (P = true): the same per-lane operations issued as paired FP32
+// instructions (two lanes per issue on sm_100), so the bits are those of the
+// scalar forms.  The difference is a + (-1) * b with one rounding, which is
+// a - b exactly (signed zeros included).  The product by a constant w takes
+// the four products as two paired multiplies, (a.x w.x, a.y w.x) and
+// (a.x w.y, a.y w.y), then (a.x w.x - a.y w.y, a.y w.x + a.x w.y): the
+// roundings of cmul.  They hold more registers, so only kernels bound by
+// instruction issue use them.
+template <bool P>
+__device__ __forceinline__ float2 cadd_t(float2 a, float2 b)
+{
+    if constexpr (P) return __fadd2_rn(a, b);
+    else return cadd(a, b);
+}
+template <bool P>
+__device__ __forceinline__ float2 csub_t(float2 a, float2 b)
+{
+    if constexpr (P) return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+    else return csub(a, b);
+}
+template <bool P>
+__device__ __forceinline__ float2 cmul_const(float2 a, float wx, float wy)
+{
+    if constexpr (P) {
+        const float2 p = __fmul2_rn(a, make_float2(wx, wx));
+        const float2 q = __fmul2_rn(a, make_float2(wy, wy));
+        return make_float2(p.x - q.y, p.y + q.x);
+    } else {
+        return cmul(a, make_float2(wx, wy));
+    }
+}
 // sign * i * a (exact)
 __device__ __forceinline__ float2 cmul_si(float2 a, int sign)
 {
     return sign > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
 }
 
+template <bool P = false>
 __device__ __forceinline__ void dft2(float2 *v)
 {
     float2 a = v[0], b = v[1];
-    v[0] = cadd(a, b);
-    v[1] = csub(a, b);
+    v[0] = cadd_t<P>(a, b);
+    v[1] = csub_t<P>(a, b);
 }
 
+template <bool P = false>
 __device__ __forceinline__ void dft4(float2 *v, int sign)
 {
-    float2 t0 = cadd(v[0], v[2]);
-    float2 t1 = csub(v[0], v[2]);
-    float2 t2 = cadd(v[1], v[3]);
-    float2 t3 = csub(v[1], v[3]);
+    float2 t0 = cadd_t<P>(v[0], v[2]);
+    float2 t1 = csub_t<P>(v[0], v[2]);
+    float2 t2 = cadd_t<P>(v[1], v[3]);
+    float2 t3 = csub_t<P>(v[1], v[3]);
     float2 u = cmul_si(t3, sign);
-    v[0] = cadd(t0, t2);
-    v[1] = cadd(t1, u);
-    v[2] = csub(t0, t2);
+    v[0] = cadd_t<P>(t0, t2);
+    v[1] = cadd(t1, u);  // lanes cross: scalar
+    v[2] = csub_t<P>(t0, t2);
     v[3] = csub(t1, u);
 }
 
+template <bool P = false>
 __device__ __forceinline__ void dft8(float2 *v, int sign)
 {
     float2 e[4] = {v[0], v[2], v[4], v[6]};
     float2 o[4] = {v[1], v[3], v[5], v[7]};
-    dft4(e, sign);
-    dft4(o, sign);
+    dft4<P>(e, sign);
+    dft4<P>(o, sign);
     const float h = 0x1.6a09e6p-1f;
     const float sh = (float)sign * h;
-    float2 o1 = cmul(o[1], make_float2(h, sh));
+    float2 o1 = cmul_const<P>(o[1], h, sh);
     float2 o2 = cmul_si(o[2], sign);
-    float2 o3 = cmul(o[3], make_float2(-h, sh));
-    v[0] = cadd(e[0], o[0]);
-    v[4] = csub(e[0], o[0]);
-    v[1] = cadd(e[1], o1);
-    v[5] = csub(e[1], o1);
-    v[2] = cadd(e[2], o2);
+    float2 o3 = cmul_const<P>(o[3], -h, sh);
+    v[0] = cadd_t<P>(e[0], o[0]);
+    v[4] = csub_t<P>(e[0], o[0]);
+    v[1] = cadd_t<P>(e[1], o1);
+    v[5] = csub_t<P>(e[1], o1);
+    v[2] = cadd(e[2], o2);  // lanes cross: scalar
     v[6] = csub(e[2], o2);
-    v[3] = cadd(e[3], o3);
-    v[7] = csub(e[3], o3);
+    v[3] = cadd_t<P>(e[3], o3);
+    v[7] = csub_t<P>(e[3], o3);
 }
 
 __device__ __forceinline__ void dft3(float2 *v, int sign)
@@ -114,13 +149,13 @@ __device__ __forceinline__ void dft_generic(float2 *v, const float2 *tw, int n)
     for (int k = 0; k < R; k++) v[k] = y[k];
 }
 
-template <int R>
+template <int R, bool P = false>
 __device__ __forceinline__ void dft_small(float2 *v, int sign, const float2 *tw, int n)
 {
-    if constexpr (R == 2) dft2(v);
+    if constexpr (R == 2) dft2<P>(v);
     else if constexpr (R == 3) dft3(v, sign);
-    else if constexpr (R == 4) dft4(v, sign);
-    else if constexpr (R == 8) dft8(v, sign);
+    else if constexpr (R == 4) dft4<P>(v, sign);
+    else if constexpr (R == 8) dft8<P>(v, sign);
     else dft_generic<R>(v, tw, n);
 }
 

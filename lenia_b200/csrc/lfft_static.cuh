@@ -55,8 +55,9 @@ struct PadMat {
 // One Stockham stage.  COLS = false: NLINES rows of length N along the
 // matrix columns (contiguous); COLS = true: NLINES matrix columns of length N
 // along the rows.  THREADS threads with indices `tid` take part; WARP selects
-// a warp-scope barrier (the lines belong to one warp) instead of the block's.
-template <int N, int S, int NLINES, bool COLS, int NC, int THREADS, bool WARP>
+// a warp-scope barrier (the lines belong to one warp) instead of the block's;
+// P selects the paired butterflies of lfft_device.cuh (same bits).
+template <int N, int S, int NLINES, bool COLS, int NC, int THREADS, bool WARP, bool P = false>
 __device__ __forceinline__ void static_stage(float2 *buf, const float2 *tw, int sign, int tid)
 {
     constexpr int R = plan_radix(N, S);
@@ -92,7 +93,7 @@ __device__ __forceinline__ void static_stage(float2 *buf, const float2 *tw, int 
 #pragma unroll
                 for (int r = 1; r < R; r++) v[i][r] = cmul(v[i][r], tw[r * jm * TSTEP]);
             }
-            dft_small<R>(v[i], sign, tw, N);
+            dft_small<R, P>(v[i], sign, tw, N);
             const int base = (j / NS) * NS * R + jm;
 #pragma unroll
             for (int r = 0; r < R; r++) {
@@ -106,21 +107,22 @@ __device__ __forceinline__ void static_stage(float2 *buf, const float2 *tw, int 
 }
 
 // Stages S .. END-1 of the plan (END defaults to the whole plan).
-template <int N, int S, int NLINES, bool COLS, int NC, int THREADS, bool WARP, int END = plan_count(N)>
+template <int N, int S, int NLINES, bool COLS, int NC, int THREADS, bool WARP, int END = plan_count(N),
+          bool P = false>
 __device__ __forceinline__ void static_stages(float2 *buf, const float2 *tw, int sign, int tid)
 {
     if constexpr (S < END) {
-        static_stage<N, S, NLINES, COLS, NC, THREADS, WARP>(buf, tw, sign, tid);
-        static_stages<N, S + 1, NLINES, COLS, NC, THREADS, WARP, END>(buf, tw, sign, tid);
+        static_stage<N, S, NLINES, COLS, NC, THREADS, WARP, P>(buf, tw, sign, tid);
+        static_stages<N, S + 1, NLINES, COLS, NC, THREADS, WARP, END, P>(buf, tw, sign, tid);
     }
 }
 
 // Whole transform of NLINES lines held in a PadMat<NC>, by the whole block.
-template <int N, int NLINES, bool COLS, int NC, int THREADS>
+template <int N, int NLINES, bool COLS, int NC, int THREADS, bool P = false>
 __device__ __forceinline__ void static_fft(float2 *buf, const float2 *tw, int sign)
 {
     static_assert(plan_count(N) > 0, "unsupported transform length");
-    static_stages<N, 0, NLINES, COLS, NC, THREADS, false>(buf, tw, sign, threadIdx.x);
+    static_stages<N, 0, NLINES, COLS, NC, THREADS, false, plan_count(N), P>(buf, tw, sign, threadIdx.x);
 }
 
 // Whole transform of NLINES rows owned by one warp (lane = threadIdx.x & 31).
