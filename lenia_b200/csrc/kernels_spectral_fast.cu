@@ -308,6 +308,10 @@ __global__ void __launch_bounds__(kFastPlaneThreads) k_planes_stream_s(PlaneJobs
         // across it
         int tid;
         asm volatile("mov.u32 %0, %%tid.x;" : "=r"(tid));
+        // its range, which the asm read hides: the stages' divisions and
+        // remainders by constants then take their unsigned forms
+        __builtin_assume(tid >= 0);
+        __builtin_assume(tid < kFastPlaneThreads);
         plane_first_stage<W>(buf, src, kp, twy, sign, tid);
         if (tid == 0 && u + stride < units) plane_unit_prefetch<W>(jobs, u + stride);
         static_stages<H, 1, D, false, H, kFastPlaneThreads, false, plan_count(H), kPlanePaired>(buf, twy, sign, tid);
