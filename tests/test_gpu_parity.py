@@ -105,6 +105,15 @@ def test_stages_bit_exact_mixed_radix(cuda_lib, oracle_built, width):
     assert not problems, "\n".join(problems[:12])
 
 
+@pytest.mark.parametrize("width", [64, 96])
+def test_stages_bit_exact_paired_plane_sizes(cuda_lib, oracle_built, width):
+    """One-plane-per-block plane passes at 64 (radix 8 only) and 96 (8, 4, 3),
+    whose butterflies run as paired FP32 instructions, against the scalar C
+    restatement."""
+    problems = run_staged(variant("sobel_torus", seed=width + 1, width=width), steps=1)
+    assert not problems, "\n".join(problems[:12])
+
+
 @pytest.mark.parametrize("shape", [(32, 24), (24, 40)])
 def test_stages_bit_exact_non_cubic(cuda_lib, oracle_built, shape):
     """Width != height runs the runtime-sized kernels (the size-specialised
