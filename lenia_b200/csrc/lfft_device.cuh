@@ -44,6 +44,12 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 w)
 // (a.x w.y, a.y w.y), then (a.x w.x - a.y w.y, a.y w.x + a.x w.y): the
 // roundings of cmul.  They hold more registers, so only kernels bound by
 // instruction issue use them.
+// A paired product that feeds a paired sum directly is contracted into one
+// paired fma even under -fmad=false and the _rn forms (measured on sm_100a:
+// __fadd2_rn(c, __fmul2_rn(a, b)) gave the fused result wherever one and two
+// roundings differ).  So no paired sum here takes a paired product: the
+// products of cmul_const meet scalar sums, and csub_t's fma multiplies by -1
+// exactly.
 template <bool P>
 __device__ __forceinline__ float2 cadd_t(float2 a, float2 b)
 {
